@@ -1,0 +1,341 @@
+"""Throughput of the grid-embedded D3Q19 channel step on B200 (MLUPS).
+
+One "step" is one coarse time step of the channel: the coarse stream-collide,
+GR fine substeps on both near-wall blocks with their coarse-to-fine interface
+transfers, the fine-to-coarse injection and the flow-rate reduction.  Its work
+is U = xdv ydv zdc + 2 GR (GR xdv)(GR ydv) zds node updates.
+
+Default workload: the production channel, coarse grid 256 x 96 x 128 (stream,
+wall-normal, span) with a 2:1 fine level over the 8 coarse cells next to each
+wall (fine blocks 512 x 16 x 256), i.e. reference macros xdv=256, ydv=128,
+zdv=83, zds=16, gratio=2; constant flow rate at Re_tau ~ 180; FP64 plain form;
+seeded synthetic initial state.  The state (2.1 GB) is far larger than L2.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+N > 1 runs under torchrun: every rank advances its own independent channel
+(replicas, weak scaling); the reported value is the whole job's updates over
+the slowest rank's device time.  ``--impl reference`` times the reference's own
+CPU routines (compiled from its sources, oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    # name: (macros, description)
+    "c2": (dict(xdv=256, ydv=128, zdv=83, zds=16, gratio=2, Rebs=5533.0, ub=0.0866034, CFL=0.1, pattern=None),
+           "channel 256x96x128 coarse, 2:1 fine blocks 512x16x256 per wall (xdv256 ydv128 zdv83 zds16 GR2), "
+           "CFR Re_tau~180"),
+    "c1": (dict(xdv=64, ydv=64, zdv=27, zds=8, gratio=2, Rebs=150.0 * 0.0866034 * 63, ub=0.0866034, CFL=0.1,
+                pattern=None),
+           "channel 64x32x64 coarse, 2:1 fine blocks 128x8x128 per wall (xdv64 ydv64 zdv27 zds8 GR2)"),
+    "c3r": (dict(xdv=384, ydv=192, zdv=115, zds=16, gratio=2, Rebs=13585.0, ub=0.0866034, CFL=0.1, pattern="RSLIP",
+                 gyplussize=24, wyplussize=24),
+            "SHS channel 384x128x192 coarse, streamwise ridges pitch 48 GF 0.5, Re_tau~395"),
+}
+METRIC = "MLUPS (coarse-step node updates, FP64 plain form)"
+
+
+def measured_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel: str, config: str):
+    """dram bytes per launch from a committed ncu summary, if one exists."""
+    f = ROOT / "profiles" / f"traffic_{config}.txt"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,power.draw")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.thread = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        reasons = sorted({names[q] for r in self.rows for q in range(4) if r[2 + q].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def reference_cpu(config: str, steps: int, processes: int, timeout: float = 900.0):
+    """Time the reference's own routines (oracle/_ref/<config>/ref_harness, one
+    rank per process, from rest, constant-force mode with zero force) on the host.
+    Returns (aggregate MLUPS, seconds per step per process, processes)."""
+    exe = ROOT / "oracle" / "_ref" / config / "ref_harness"
+    if not exe.exists():
+        return None
+    with tempfile.TemporaryDirectory() as d:
+        procs = []
+        for q in range(processes):
+            od = Path(d) / f"p{q}"
+            od.mkdir()
+            procs.append(subprocess.Popen([str(exe), "-", "0", str(od), "-1", str(steps), "const", "0"],
+                                          stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
+        secs = []
+        for pr in procs:
+            out, _ = pr.communicate(timeout=timeout)
+            for line in out.splitlines():
+                if line.startswith("harness_seconds"):
+                    secs.append(float(line.split()[1]))
+    if len(secs) != processes:
+        return None
+    return secs
+
+
+def host_parallelism(per_process_bytes: float):
+    ncpu = os.cpu_count() or 1
+    try:
+        import psutil
+
+        avail = psutil.virtual_memory().available
+    except Exception:
+        avail = 16e9
+    return max(1, min(ncpu, int(avail * 0.6 // per_process_bytes), 64))
+
+
+def updates_per_step(m):
+    gr = m["gratio"]
+    return m["xdv"] * m["ydv"] * m["zdv"] + 2 * gr * (gr * m["xdv"]) * (gr * m["ydv"]) * m["zds"]
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    m, desc = CONFIGS[args.config]
+    U = updates_per_step(m)
+    # about 2.3 GB of AoS arrays per process at the default config
+    per_proc = 19 * 8 * 2.2 * (U + 2 * (m["gratio"] * m["xdv"]) * (m["gratio"] * m["ydv"]))
+    nproc = host_parallelism(per_proc)
+    steps = max(1, min(args.steps, args.ref_steps))
+    secs = reference_cpu(args.config, steps, nproc)
+    line = {"impl": "reference", "metric": METRIC, "unit": "MLUPS", "n_gpus": world, "steps": steps,
+            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference cold start from rest)",
+            "config": {"workload": args.config, "description": desc}}
+    if secs is None:
+        line["unavailable"] = "compiled reference binary missing (oracle/_ref not built)"
+        print(json.dumps(line), flush=True)
+        return 0
+    mlups = U * steps * len(secs) / max(secs) / 1e6
+    line.update({"value": mlups, "ms_per_step": 1e3 * max(secs) / steps})
+    line["cpu_baseline"] = {"value": mlups, "unit": "MLUPS", "cores": len(secs), "kind": "reference",
+                            "sample": f"{len(secs)} concurrent single-rank reference processes x {steps} coarse "
+                                      f"steps of {args.config} (own step-loop clock, main's t2-t4)"}
+    line["e2e"] = {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    import importlib
+
+    pkg = importlib.import_module("dns-solvers-with-grid-embedding_b200")
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist_mod
+        from datetime import timedelta
+
+        dist = dist_mod
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    m, desc = CONFIGS[args.config]
+    p = pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank)
+    geom = pkg.geometry(p)
+    U = geom.updates_per_step
+    ch = pkg.Channel(p)
+    stream = torch.cuda.Stream()
+    ch.set_stream(stream.cuda_stream)
+    ch.init_seeded(42 + rank, 0.05, 0.005)
+    ch.step(args.warmup, log=False)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # ---- timed region: K coarse steps, state resident in HBM
+    ch.set_profiling(True)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local_rank) as clk:
+        barrier()
+        start.record(stream)
+        log = ch.step(args.steps, log=True)
+        end.record(stream)
+        barrier()
+    ms = start.elapsed_time(end)
+    kt = ch.kernel_times()
+    ch.set_profiling(False)
+    ms_max = ms
+    if dist:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    value = U * args.steps * world / (ms_max * 1e-3) / 1e6
+
+    # ---- end to end through the C ABI with pinned host buffers: import the
+    # state, K steps with the per-step log read back, export the state
+    shapes = [(geom.nx, geom.ny, geom.nzc, 19), (geom.nxf, geom.nyf, geom.zdf, 19), (geom.nxf, geom.nyf, geom.zdf, 19)]
+    host = [torch.empty(s, dtype=torch.float64, pin_memory=True).numpy() for s in shapes]
+    for lv in range(3):
+        host[lv][...] = ch.export_state(lv)
+    state_bytes = sum(h.nbytes for h in host)
+    barrier()
+    t0 = time.perf_counter()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for lv in range(3):
+        ch.import_state(lv, host[lv])
+    ch.step(args.steps, log=True)
+    for lv in range(3):
+        lib_out = host[lv]
+        pkg.lib().dns_export_state(ch.h, lv, lib_out.ctypes.data)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_e2e = time.perf_counter() - t0
+    e2e_ms = max(e0.elapsed_time(e1), 1e3 * t_e2e)
+    if dist:
+        t = torch.tensor([e2e_ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = U * args.steps * world / (e2e_ms * 1e-3) / 1e6
+
+    if rank != 0:
+        if dist:
+            dist.barrier()
+            dist.destroy_process_group()
+        return 0
+
+    # ---- roofline of the dominant kernel (fine stream-collide, both blocks)
+    fine_ms, fine_n = kt["fine"]
+    fine_nodes = 2 * geom.nxf * geom.nyf * p.zds
+    bytes_per_launch = fine_nodes * 2 * 19 * 8
+    achieved = bytes_per_launch / (fine_ms / fine_n * 1e-3) / 1e9 if fine_n else None
+    peak, peak_kind = measured_peak()
+    launches = sum(n for _, n in kt.values())
+    line = {
+        "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded laminar profile + noise)",
+        "config": {"workload": args.config, "description": desc, "updates_per_step": U,
+                   "l2": "state 2.1 GB >> 126 MB L2 (no flush needed)" if args.config != "c1"
+                   else "state smaller than needed to defeat L2", "parallelism": f"replicas x{world}"},
+        "roofline": {"bound": "hbm", "kernel": "fine_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": bytes_per_launch,
+                     "traffic": traffic_from_profiles("fine_kernel", args.config)},
+        "kernel_ms_per_step": {k: (v[0] / args.steps) for k, v in kt.items()},
+        "whole_step_hbm_frac": (U * args.steps * 304 / (ms_max * 1e-3) / 1e9) / peak,
+        "e2e": {"value": e2e, "unit": "MLUPS", "h2d_bytes_per_step": state_bytes / args.steps,
+                "d2h_bytes_per_step": (state_bytes + 72 * args.steps) / args.steps,
+                "note": "import state from pinned host, K steps with per-step log read-back, export state"},
+        "gpu_launches": launches,
+        "clocks": clk.summary(),
+        "log_tail": {"force": float(log[-1, 1]), "flowrate": float(log[-1, 4]), "stress": float(log[-1, 7])},
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        m_ = CONFIGS[args.config][0]
+        secs = reference_cpu(args.config, args.cpu_steps, 1)
+        if secs:
+            line["cpu_baseline"] = {"value": U * args.cpu_steps / secs[0] / 1e6, "unit": "MLUPS", "cores": 1,
+                                    "kind": "reference",
+                                    "sample": f"{args.cpu_steps} coarse steps of {args.config}, one single-rank "
+                                              "reference process (its own routines, own step-loop clock)"}
+        else:
+            line["cpu_baseline"] = None
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
+    ap.add_argument("--cpu-steps", type=int, default=4)
+    ap.add_argument("--ref-steps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    return run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,252 @@
+"""Python host side of the B200 grid-embedded D3Q19 channel solver.
+
+A thin ctypes layer over the C ABI of ``libdnsembed.so`` (``include/dns_embed.h``).
+It mirrors the reference solver's interface for the time-step path: the
+parameters of ``src/definitions.h`` (:class:`Params`, same names), the restart
+files read in mode ``-p`` and written every 50 unit times, the per-step log
+values of ``encalc2``/``wshearstr`` and the plane statistics of
+``statistics``.  Errors raise :class:`DnsError` carrying the C status code.
+
+The CUDA library is required: if ``libdnsembed.so`` is missing or cannot be
+loaded, :func:`lib` raises instead of falling back to any CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIBPATH = HERE / "libdnsembed.so"
+
+DNS_OK, DNS_EINVAL, DNS_ENOMEM, DNS_EIO, DNS_ENAN, DNS_ETIMEOUT, DNS_ECUDA = 0, -1, -2, -3, -4, -5, -6
+PATTERN_NONE, PATTERN_RSLIP, PATTERN_PSLIP, PATTERN_SSLIP = 0, 1, 2, 3
+FORCING_CFR, FORCING_CONST = 0, 1
+FP64, FP32 = 0, 1
+NSTAT = 14
+STAT_NAMES = ("z", "U", "V", "W", "rho", "uu", "vv", "ww", "uw", "rr", "uu_t", "vv_t", "ww_t", "uw_t")
+NKERNEL = 7
+KERNEL_NAMES = ("coarse", "extract", "fine", "interface", "inject", "finalize", "stats")
+PLANE_STAT_NAMES = ("UAVG", "VAVG", "WAVG", "UTIN", "VTIN", "WTIN", "REYS", "DAVG", "DTIN")
+
+
+class DnsError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (status {code})")
+        self.code = code
+
+
+class Params(C.Structure):
+    """``dns_params``: the reference's definitions.h macros plus run-time options."""
+
+    _fields_ = [
+        ("Rebs", C.c_double), ("ub", C.c_double), ("zdv", C.c_int), ("ydv", C.c_int), ("xdv", C.c_int),
+        ("TSTR", C.c_int), ("TEND", C.c_int), ("CFL", C.c_double), ("gratio", C.c_int), ("zds", C.c_int),
+        ("gyplussize", C.c_int), ("wyplussize", C.c_int), ("gxplussize", C.c_int), ("wxplussize", C.c_int),
+        ("pattern", C.c_int), ("XDIM", C.c_int), ("YDIM", C.c_int), ("ITER", C.c_long),
+        ("forcing", C.c_int), ("force_const", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+    ]
+
+
+class Geometry(C.Structure):
+    _fields_ = [
+        ("nx", C.c_int), ("ny", C.c_int), ("nzc", C.c_int), ("nxf", C.c_int), ("nyf", C.c_int), ("zdf", C.c_int),
+        ("gr", C.c_int), ("nzs", C.c_int), ("nz_profile", C.c_int), ("utime", C.c_int),
+        ("omega_c", C.c_double), ("omega_f", C.c_double), ("updates_per_step", C.c_longlong),
+        ("device_bytes", C.c_longlong),
+    ]
+
+
+class StepLog(C.Structure):
+    _fields_ = [(n, C.c_double) for n in
+                ("time", "force", "momentum", "denst", "flowrate", "stup", "stdown", "stress", "pgrad")]
+
+
+LOG_FIELDS = tuple(n for n, _ in StepLog._fields_)
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load ``libdnsembed.so``; raise if it is absent (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIBPATH.exists():
+        raise DnsError(DNS_ECUDA, f"{LIBPATH.name} is not built; run build.py")
+    L = C.CDLL(str(LIBPATH))
+    P, I, D = C.c_void_p, C.c_int, C.c_double
+    sig = {
+        "dns_params_default": (I, [C.POINTER(Params)]),
+        "dns_params_from_definitions": (I, [C.c_char_p, C.POINTER(Params)]),
+        "dns_geometry_of": (I, [C.POINTER(Params), C.POINTER(Geometry)]),
+        "dns_create": (I, [C.POINTER(Params), C.POINTER(P)]),
+        "dns_destroy": (None, [P]),
+        "dns_set_stream": (I, [P, P]),
+        "dns_get_geometry": (I, [P, C.POINTER(Geometry)]),
+        "dns_load_restart": (I, [P, C.c_char_p, I]),
+        "dns_write_restart": (I, [P, C.c_char_p, I]),
+        "dns_init_seeded": (I, [P, C.c_uint64, D, D]),
+        "dns_export_state": (I, [P, I, P]),
+        "dns_import_state": (I, [P, I, P]),
+        "dns_export_history": (I, [P, P]),
+        "dns_get_force": (I, [P, C.POINTER(D)]),
+        "dns_step": (I, [P, C.c_long, P]),
+        "dns_set_sampling": (I, [P, C.c_long]),
+        "dns_stats_reset": (I, [P]),
+        "dns_stats": (I, [P, P, C.POINTER(C.c_long)]),
+        "dns_plane_stats": (I, [P, P]),
+        "dns_set_profiling": (I, [P, I]),
+        "dns_kernel_times": (I, [P, P, P]),
+        "dns_error_string": (C.c_char_p, [I]),
+        "dns_last_error": (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(rc: int, what: str):
+    if rc != DNS_OK:
+        msg = lib().dns_last_error().decode(errors="replace")
+        raise DnsError(rc, f"{what}: {msg or lib().dns_error_string(rc).decode()}")
+
+
+def default_params() -> Params:
+    p = Params()
+    _check(lib().dns_params_default(C.byref(p)), "dns_params_default")
+    return p
+
+
+def params_from_definitions(path) -> Params:
+    """Read a reference-style ``definitions.h``."""
+    p = Params()
+    _check(lib().dns_params_from_definitions(str(path).encode(), C.byref(p)), "dns_params_from_definitions")
+    return p
+
+
+def make_params(**kw) -> Params:
+    """Defaults of the reference, overridden by keyword (macro names, e.g. xdv=64)."""
+    p = default_params()
+    for k, v in kw.items():
+        if k == "pattern" and isinstance(v, str):
+            v = {"RSLIP": PATTERN_RSLIP, "PSLIP": PATTERN_PSLIP, "SSLIP": PATTERN_SSLIP}[v]
+        if k == "pattern" and v is None:
+            v = PATTERN_NONE
+        setattr(p, k, v)
+    return p
+
+
+def geometry(p: Params) -> Geometry:
+    g = Geometry()
+    _check(lib().dns_geometry_of(C.byref(p), C.byref(g)), "dns_geometry_of")
+    return g
+
+
+class Channel:
+    """One grid-embedded channel resident on a GPU (a ``dns_handle``)."""
+
+    def __init__(self, params: Params):
+        self.params = params
+        h = C.c_void_p()
+        _check(lib().dns_create(C.byref(params), C.byref(h)), "dns_create")
+        self.h = h
+        self.geom = Geometry()
+        _check(lib().dns_get_geometry(self.h, C.byref(self.geom)), "dns_get_geometry")
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dns_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # ---- state
+    def set_stream(self, stream_handle: int | None):
+        _check(lib().dns_set_stream(self.h, C.c_void_p(stream_handle or 0)), "dns_set_stream")
+
+    def init_seeded(self, seed: int = 42, uc: float = 0.05, amp: float = 0.005):
+        _check(lib().dns_init_seeded(self.h, seed, uc, amp), "dns_init_seeded")
+
+    def load_restart(self, directory, cntr: int):
+        _check(lib().dns_load_restart(self.h, str(directory).encode(), cntr), "dns_load_restart")
+
+    def write_restart(self, directory, cntr: int):
+        _check(lib().dns_write_restart(self.h, str(directory).encode(), cntr), "dns_write_restart")
+
+    def _level_shape(self, level: int):
+        g = self.geom
+        return (g.nx, g.ny, g.nzc, 19) if level == 0 else (g.nxf, g.nyf, g.zdf, 19)
+
+    def export_state(self, level: int) -> np.ndarray:
+        out = np.empty(self._level_shape(level), dtype=np.float64)
+        _check(lib().dns_export_state(self.h, level, out.ctypes.data), "dns_export_state")
+        return out
+
+    def import_state(self, level: int, arr: np.ndarray):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != self._level_shape(level):
+            raise DnsError(DNS_EINVAL, f"state shape {a.shape} != {self._level_shape(level)}")
+        _check(lib().dns_import_state(self.h, level, a.ctypes.data), "dns_import_state")
+
+    def export_history(self) -> np.ndarray:
+        g = self.geom
+        out = np.empty((3, 2, g.nx, g.ny, 23), dtype=np.float64)
+        _check(lib().dns_export_history(self.h, out.ctypes.data), "dns_export_history")
+        return out
+
+    def force(self) -> float:
+        f = C.c_double()
+        _check(lib().dns_get_force(self.h, C.byref(f)), "dns_get_force")
+        return f.value
+
+    # ---- hot path
+    def step(self, n: int = 1, log: bool = True) -> np.ndarray | None:
+        """Advance n coarse steps; returns the per-step log (n x 9) when asked."""
+        if log:
+            buf = (StepLog * max(n, 1))()
+            _check(lib().dns_step(self.h, n, buf), "dns_step")
+            return np.frombuffer(buf, dtype=np.float64).reshape(-1, len(LOG_FIELDS))[:n].copy()
+        _check(lib().dns_step(self.h, n, None), "dns_step")
+        return None
+
+    # ---- statistics
+    def set_sampling(self, every: int):
+        _check(lib().dns_set_sampling(self.h, every), "dns_set_sampling")
+
+    def stats_reset(self):
+        _check(lib().dns_stats_reset(self.h), "dns_stats_reset")
+
+    def stats(self):
+        nz = self.geom.nz_profile
+        out = np.zeros((NSTAT, nz))
+        ns = C.c_long()
+        _check(lib().dns_stats(self.h, out.ctypes.data, C.byref(ns)), "dns_stats")
+        return out, ns.value
+
+    # ---- measurement
+    def set_profiling(self, on: bool):
+        _check(lib().dns_set_profiling(self.h, 1 if on else 0), "dns_set_profiling")
+
+    def kernel_times(self):
+        """{kernel class: (total ms, launches)} since profiling was switched on."""
+        ms = np.zeros(NKERNEL)
+        n = np.zeros(NKERNEL, dtype=np.int64)
+        _check(lib().dns_kernel_times(self.h, ms.ctypes.data, n.ctypes.data), "dns_kernel_times")
+        return {k: (float(ms[i]), int(n[i])) for i, k in enumerate(KERNEL_NAMES)}
+
+    def plane_stats(self) -> np.ndarray:
+        out = np.zeros((9, self.geom.nz_profile))
+        _check(lib().dns_plane_stats(self.h, out.ctypes.data), "dns_plane_stats")
+        return out

@@ -1,0 +1,837 @@
+// Host driver and C ABI of the grid-embedded channel solver (include/dns_embed.h).
+//
+// Replaces the reference main program's set-up, file I/O and step loop
+// (DNS-solver-with-grid-embedding/src/dns-q-mgrd-all-patterns-xyc.c) for one
+// GPU-resident domain.  All device memory is allocated in dns_create; a coarse
+// step issues the kernels of kernels_f64.cu on the handle's stream.
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/dns_embed.h"
+#include "kernels.h"
+
+using namespace dns;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CUDA_TRY(expr)                                                                      \
+  do {                                                                                      \
+    cudaError_t e_ = (expr);                                                                \
+    if (e_ != cudaSuccess)                                                                  \
+      return fail(DNS_ECUDA, std::string(#expr) + ": " + cudaGetErrorString(e_));           \
+  } while (0)
+
+constexpr int kLogCap = 1024;
+constexpr int kProfSteps = 32;  // steps per chunk while profiling (bounds the event pool)
+
+// CUDA-event timing of every launch (dns_set_profiling)
+struct Profiler {
+  bool on = false;
+  std::vector<cudaEvent_t> ev;  // pairs
+  std::vector<int> cls;
+  size_t used = 0;
+  double ms[DNS_NKERNEL] = {0};
+  long cnt[DNS_NKERNEL] = {0};
+};
+
+}  // namespace
+
+struct dns_handle {
+  dns_params p{};
+  dns_geometry g{};
+  Dims d{};
+  LaunchShape shape{};
+  PartialLayout pl{};
+  StepParams sp{};
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double *fc[2] = {nullptr, nullptr};  // coarse SoA, [cur] holds S
+  double *ff[2] = {nullptr, nullptr};  // fine SoA (both blocks)
+  double *hist = nullptr;              // [3 slots][2 walls][23][ny][nx]
+  int hn = 0, hp = 1, hpp = 2;         // ring slots of levels n, p, pp
+  int8_t *wflag = nullptr;             // [nyf][nxf]
+  double *partials = nullptr;
+  DevState *state = nullptr;
+  DevLog *dlog = nullptr;              // kLogCap rows
+  DevLog *hlog = nullptr;              // pinned mirror
+  double *stats_acc = nullptr;         // [nz_profile][16]
+  int cur_c = 0, cur_f = 0;
+  long ss = 0;                         // coarse steps since load / seed
+  int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
+  long sample_every = 0;
+  std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
+  Profiler prof;
+};
+
+// Bracket one launch with events when profiling; returns the pair index or -1.
+static int prof_begin(dns_handle *h, int cls) {
+  Profiler &P = h->prof;
+  if (!P.on) return -1;
+  if (P.used * 2 + 2 > P.ev.size()) {
+    cudaEvent_t a, b;
+    cudaEventCreate(&a);
+    cudaEventCreate(&b);
+    P.ev.push_back(a);
+    P.ev.push_back(b);
+    P.cls.push_back(0);
+  }
+  const int q = (int)P.used++;
+  P.cls[q] = cls;
+  cudaEventRecord(P.ev[2 * q], h->stream);
+  return q;
+}
+static void prof_end(dns_handle *h, int q) {
+  if (q >= 0) cudaEventRecord(h->prof.ev[2 * q + 1], h->stream);
+}
+// after a stream synchronize: fold the recorded pairs into the totals
+static void prof_collect(dns_handle *h) {
+  Profiler &P = h->prof;
+  for (size_t q = 0; q < P.used; q++) {
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, P.ev[2 * q], P.ev[2 * q + 1]) == cudaSuccess) {
+      P.ms[P.cls[q]] += t;
+      P.cnt[P.cls[q]] += 1;
+    }
+  }
+  P.used = 0;
+}
+#define PROFILED(h, cls, launch)      \
+  do {                                \
+    const int pq_ = prof_begin(h, cls); \
+    launch;                           \
+    prof_end(h, pq_);                 \
+  } while (0)
+
+// ---------------------------------------------------------------- parameters
+extern "C" int dns_params_default(dns_params *p) {
+  if (!p) return fail(DNS_EINVAL, "null params");
+  std::memset(p, 0, sizeof(*p));
+  // reference src/definitions.h:34-119
+  p->Rebs = 7200.0;
+  p->ub = 0.0866034;
+  p->zdv = 220;
+  p->ydv = 256;
+  p->xdv = 512;
+  p->TSTR = 400;
+  p->TEND = 800;
+  p->CFL = 0.1;
+  p->gratio = 4;
+  p->zds = 10;
+  p->gyplussize = 56;
+  p->wyplussize = 8;
+  p->gxplussize = 4;
+  p->wxplussize = 4;
+  p->pattern = DNS_PATTERN_RSLIP;
+  p->XDIM = 1;
+  p->YDIM = 1;
+  p->ITER = -1;
+  p->forcing = DNS_FORCING_CFR;
+  p->force_const = 0.0;
+  p->precision = DNS_FP64;
+  p->device = 0;
+  return DNS_OK;
+}
+
+extern "C" int dns_params_from_definitions(const char *path, dns_params *p) {
+  if (!path || !p) return fail(DNS_EINVAL, "null argument");
+  FILE *fp = std::fopen(path, "r");
+  if (!fp) return fail(DNS_EIO, std::string("cannot open ") + path);
+  dns_params_default(p);
+  p->pattern = DNS_PATTERN_NONE;
+  char line[1024];
+  while (std::fgets(line, sizeof line, fp)) {
+    const char *s = line;
+    while (*s == ' ' || *s == '\t') s++;
+    if (std::strncmp(s, "#define", 7) != 0) continue;  // commented-out switches start with //
+    s += 7;
+    char name[128] = {0}, val[256] = {0};
+    if (std::sscanf(s, "%127s %255s", name, val) < 1) continue;
+    const std::string n(name);
+    auto num = [&](double &dst) { if (val[0]) dst = std::strtod(val, nullptr); };
+    auto inum = [&](int &dst) { if (val[0]) dst = (int)std::strtol(val, nullptr, 10); };
+    if (n == "Rebs") num(p->Rebs);
+    else if (n == "ub") num(p->ub);
+    else if (n == "zdv") inum(p->zdv);
+    else if (n == "ydv") inum(p->ydv);
+    else if (n == "xdv") inum(p->xdv);
+    else if (n == "TSTR") inum(p->TSTR);
+    else if (n == "TEND") inum(p->TEND);
+    else if (n == "CFL") num(p->CFL);
+    else if (n == "gratio") inum(p->gratio);
+    else if (n == "zds") inum(p->zds);
+    else if (n == "gyplussize") inum(p->gyplussize);
+    else if (n == "wyplussize") inum(p->wyplussize);
+    else if (n == "gxplussize") inum(p->gxplussize);
+    else if (n == "wxplussize") inum(p->wxplussize);
+    else if (n == "XDIM") inum(p->XDIM);
+    else if (n == "YDIM") inum(p->YDIM);
+    else if (n == "ITER") p->ITER = val[0] ? std::strtol(val, nullptr, 10) : 1;
+    else if (n == "RSLIP") p->pattern = DNS_PATTERN_RSLIP;
+    else if (n == "PSLIP") p->pattern = DNS_PATTERN_PSLIP;
+    else if (n == "SSLIP") p->pattern = DNS_PATTERN_SSLIP;
+  }
+  std::fclose(fp);
+  return DNS_OK;
+}
+
+extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
+  if (!p || !g) return fail(DNS_EINVAL, "null argument");
+  if (p->gratio < 2 || p->gratio > 4) return fail(DNS_EINVAL, "gratio must be 2, 3 or 4");
+  if (p->xdv < 4 || p->ydv < 4) return fail(DNS_EINVAL, "xdv and ydv must be >= 4");
+  if (p->zdv < 5) return fail(DNS_EINVAL, "zdv (coarse wall-normal nodes) must be >= 5");
+  if (p->zds < p->gratio + 2 || p->zds < 4)
+    return fail(DNS_EINVAL, "zds must be >= max(4, gratio + 2) (transfer planes inside the fine block)");
+  if (p->pattern < DNS_PATTERN_NONE || p->pattern > DNS_PATTERN_SSLIP) return fail(DNS_EINVAL, "bad pattern");
+  if (p->Rebs <= 0 || p->ub <= 0 || p->CFL <= 0) return fail(DNS_EINVAL, "Rebs, ub and CFL must be positive");
+  if (p->precision != DNS_FP64) return fail(DNS_EINVAL, "only DNS_FP64 is available in this build");
+  std::memset(g, 0, sizeof(*g));
+  const int GR = p->gratio;
+  g->gr = GR;
+  g->nx = p->xdv;
+  g->ny = p->ydv;
+  g->nzc = p->zdv;
+  g->nxf = GR * p->xdv;
+  g->nyf = GR * p->ydv;
+  g->zdf = p->zds + 1;
+  // dns-q-mgrd-all-patterns-xyc.c:155
+  g->nzs = 2 * g->zdf + GR * (g->nzc - 4) + GR - 1;
+  g->nz_profile = 2 * g->zdf + g->nzc - 4;
+  // :439-451, evaluated in the same order
+  double utime = ((double)(0.5 * (g->nzs - 2.) / p->CFL)) / ((double)(GR));
+  g->utime = (int)utime;
+  double tauf = (3. / p->Rebs) * p->ub * (g->nzs - 2.) + 0.5;
+  double tauc = (1. / ((double)GR)) * (3. / p->Rebs) * p->ub * (g->nzs - 2.) + 0.5;
+  g->omega_f = 1. / tauf;
+  g->omega_c = 1. / tauc;
+  g->updates_per_step = (long long)p->xdv * p->ydv * p->zdv +
+                        2LL * GR * ((long long)GR * p->xdv) * ((long long)GR * p->ydv) * p->zds;
+  Dims d{g->nx, g->ny, g->nzc, g->nxf, g->nyf, g->zdf, p->zds, GR, g->nzs};
+  LaunchShape s = make_shape(d);
+  PartialLayout pl = partial_layout(d, s);
+  const long long nc = 19LL * g->nzc * g->ny * g->nx, nf = 19LL * 2 * p->zds * g->nyf * g->nxf;
+  g->device_bytes = 8 * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + pl.total + 16LL * g->nz_profile) +
+                    (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
+  return DNS_OK;
+}
+
+// wall flags: solid_init.c:46-69, slip_ridges_init.c:35-66, slip_posts_init.c:45-117,
+// slip_spanwise_init.c:34-66 (global index; writes past the span are dropped)
+static std::vector<int8_t> wall_flags(const dns_params &p, const dns_geometry &g) {
+  std::vector<int8_t> sx(g.nxf, -1), sy(g.nyf, -1), w((size_t)g.nyf * g.nxf, -1);
+  const bool ys = p.pattern == DNS_PATTERN_RSLIP || p.pattern == DNS_PATTERN_PSLIP;
+  const bool xs = p.pattern == DNS_PATTERN_SSLIP || p.pattern == DNS_PATTERN_PSLIP;
+  if (ys)
+    for (int j = p.wyplussize / 2; j < g.nyf; j += p.gyplussize + p.wyplussize)
+      for (int a = 0; a < p.gyplussize && j + a < g.nyf; a++) sy[j + a] = -2;
+  if (xs)
+    for (int i = p.wxplussize / 2; i < g.nxf; i += p.gxplussize + p.wxplussize)
+      for (int a = 0; a < p.gxplussize && i + a < g.nxf; a++) sx[i + a] = -2;
+  for (int j = 0; j < g.nyf; j++)
+    for (int i = 0; i < g.nxf; i++) {
+      int8_t f = -1;
+      if (p.pattern == DNS_PATTERN_RSLIP) f = sy[j];
+      else if (p.pattern == DNS_PATTERN_SSLIP) f = sx[i];
+      else if (p.pattern == DNS_PATTERN_PSLIP) f = (sx[i] == -2 || sy[j] == -2) ? -2 : -1;
+      w[(size_t)j * g.nxf + i] = f;
+    }
+  return w;
+}
+
+// ---------------------------------------------------------------- lifecycle
+extern "C" void dns_destroy(dns_handle *h) {
+  if (!h) return;
+  cudaSetDevice(h->p.device);
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int q = 0; q < 2; q++) {
+    cudaFree(h->fc[q]);
+    cudaFree(h->ff[q]);
+  }
+  cudaFree(h->hist);
+  cudaFree(h->wflag);
+  cudaFree(h->partials);
+  cudaFree(h->state);
+  cudaFree(h->dlog);
+  cudaFree(h->stats_acc);
+  if (h->hlog) cudaFreeHost(h->hlog);
+  for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+}
+
+extern "C" int dns_create(const dns_params *p, dns_handle **out) {
+  if (!p || !out) return fail(DNS_EINVAL, "null argument");
+  *out = nullptr;
+  dns_geometry g;
+  int rc = dns_geometry_of(p, &g);
+  if (rc) return rc;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(DNS_ECUDA, "no CUDA device");
+  if (p->device < 0 || p->device >= ndev) return fail(DNS_EINVAL, "device ordinal out of range");
+  size_t freeb = 0, totalb = 0;
+  CUDA_TRY(cudaSetDevice(p->device));
+  CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
+  if ((long long)freeb < g.device_bytes) return fail(DNS_ENOMEM, "not enough free device memory for this channel");
+  dns_handle *h = new dns_handle();
+  h->p = *p;
+  h->g = g;
+  h->d = Dims{g.nx, g.ny, g.nzc, g.nxf, g.nyf, g.zdf, p->zds, g.gr, g.nzs};
+  h->shape = make_shape(h->d);
+  h->pl = partial_layout(h->d, h->shape);
+  h->sp = StepParams{g.omega_c, g.omega_f, p->ub, p->force_const, p->forcing == DNS_FORCING_CFR ? 1 : 0};
+  h->tm = p->TSTR;
+  const size_t nc = 19ull * g.nzc * g.ny * g.nx, nf = 19ull * 2 * p->zds * g.nyf * g.nxf;
+  auto alloc = [&](void **ptr, size_t bytes) -> int {
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) {
+      dns_destroy(h);
+      return fail(DNS_ENOMEM, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+    }
+    return DNS_OK;
+  };
+  for (int q = 0; q < 2; q++) {
+    if ((rc = alloc((void **)&h->fc[q], nc * 8))) return rc;
+    if ((rc = alloc((void **)&h->ff[q], nf * 8))) return rc;
+  }
+  if ((rc = alloc((void **)&h->hist, 3ull * 2 * 23 * g.ny * g.nx * 8))) return rc;
+  if ((rc = alloc((void **)&h->wflag, (size_t)g.nyf * g.nxf))) return rc;
+  if ((rc = alloc((void **)&h->partials, (size_t)h->pl.total * 8))) return rc;
+  if ((rc = alloc((void **)&h->state, sizeof(DevState)))) return rc;
+  if ((rc = alloc((void **)&h->dlog, kLogCap * sizeof(DevLog)))) return rc;
+  if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * 16 * 8))) return rc;
+  if (cudaMallocHost((void **)&h->hlog, kLogCap * sizeof(DevLog)) != cudaSuccess) {
+    dns_destroy(h);
+    return fail(DNS_ENOMEM, "cudaMallocHost failed");
+  }
+  if (cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    dns_destroy(h);
+    return fail(DNS_ECUDA, "cudaStreamCreate failed");
+  }
+  h->own_stream = true;
+  std::vector<int8_t> wf = wall_flags(*p, g);
+  cudaMemcpy(h->wflag, wf.data(), wf.size(), cudaMemcpyHostToDevice);
+  cudaMemset(h->partials, 0, (size_t)h->pl.total * 8);
+  cudaMemset(h->stats_acc, 0, (size_t)g.nz_profile * 16 * 8);
+  cudaMemset(h->state, 0, sizeof(DevState));
+  h->wall_lo.assign((size_t)g.nxf * g.nyf * 19, 0.0);
+  h->wall_hi.assign((size_t)g.nxf * g.nyf * 19, 0.0);
+  cudaError_t e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    dns_destroy(h);
+    return fail(DNS_ECUDA, cudaGetErrorString(e));
+  }
+  *out = h;
+  return DNS_OK;
+}
+
+extern "C" int dns_set_stream(dns_handle *h, void *cuda_stream) {
+  if (!h) return fail(DNS_EINVAL, "null handle");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (cuda_stream) {
+    if (h->own_stream) cudaStreamDestroy(h->stream);
+    h->stream = (cudaStream_t)cuda_stream;
+    h->own_stream = false;
+  } else if (!h->own_stream) {
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return DNS_OK;
+}
+
+extern "C" int dns_get_geometry(const dns_handle *h, dns_geometry *g) {
+  if (!h || !g) return fail(DNS_EINVAL, "null argument");
+  *g = h->g;
+  return DNS_OK;
+}
+
+// ---------------------------------------------------------------- state transfer
+// device SoA <-> reference AoS of one level, staged through the idle ping-pong buffer
+static int export_level(dns_handle *h, int level, double *out) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  if (level == 0) {
+    double *stage = h->fc[1 - h->cur_c];
+    launch_soa_to_aos(h->fc[h->cur_c], stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, stage, 19ull * g.nzc * g.ny * g.nx * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DNS_OK;
+  }
+  double *stage = h->ff[1 - h->cur_f];
+  const size_t n = 19ull * g.zdf * g.nyf * g.nxf;
+  // lower block: device planes 0..zds-1 are k = 1..zdf-1; upper: zds.. are k = 0..zdf-2
+  if (level == 1)
+    launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
+  else
+    launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaMemcpyAsync(out, stage, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+  const int kw = level == 1 ? 0 : g.zdf - 1;
+  for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
+    std::memcpy(out + (c * g.zdf + kw) * 19, wall.data() + c * 19, 19 * 8);
+  return DNS_OK;
+}
+
+static int import_level(dns_handle *h, int level, const double *in) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  if (level == 0) {
+    double *stage = h->fc[1 - h->cur_c];
+    CUDA_TRY(cudaMemcpyAsync(stage, in, 19ull * g.nzc * g.ny * g.nx * 8, cudaMemcpyHostToDevice, h->stream));
+    launch_aos_to_soa(stage, h->fc[h->cur_c], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return DNS_OK;
+  }
+  double *stage = h->ff[1 - h->cur_f];
+  const size_t n = 19ull * g.zdf * g.nyf * g.nxf;
+  CUDA_TRY(cudaMemcpyAsync(stage, in, n * 8, cudaMemcpyHostToDevice, h->stream));
+  if (level == 1)
+    launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
+  else
+    launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+  const int kw = level == 1 ? 0 : g.zdf - 1;
+  for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
+    std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
+  return DNS_OK;
+}
+
+// history: device [slot][wall][23][ny][nx] <-> file order [level][wall][nx][ny][23]
+static int export_history(dns_handle *h, double *out) {
+  const dns_geometry &g = h->g;
+  const size_t plane = (size_t)g.ny * g.nx, per = 2 * 23 * plane;
+  std::vector<double> tmp(3 * per);
+  CUDA_TRY(cudaMemcpyAsync(tmp.data(), h->hist, 3 * per * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  const int slots[3] = {h->hn, h->hp, h->hpp};
+  for (int l = 0; l < 3; l++)
+    for (int w = 0; w < 2; w++)
+      for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+          for (int b = 0; b < 23; b++)
+            out[((((size_t)l * 2 + w) * g.nx + i) * g.ny + j) * 23 + b] =
+                tmp[(((size_t)slots[l] * 2 + w) * 23 + b) * plane + (size_t)j * g.nx + i];
+  return DNS_OK;
+}
+
+static int import_history(dns_handle *h, const double *in) {
+  const dns_geometry &g = h->g;
+  const size_t plane = (size_t)g.ny * g.nx, per = 2 * 23 * plane;
+  std::vector<double> tmp(3 * per);
+  for (int l = 0; l < 3; l++)
+    for (int w = 0; w < 2; w++)
+      for (int i = 0; i < g.nx; i++)
+        for (int j = 0; j < g.ny; j++)
+          for (int b = 0; b < 23; b++)
+            tmp[(((size_t)l * 2 + w) * 23 + b) * plane + (size_t)j * g.nx + i] =
+                in[((((size_t)l * 2 + w) * g.nx + i) * g.ny + j) * 23 + b];
+  CUDA_TRY(cudaMemcpyAsync(h->hist, tmp.data(), 3 * per * 8, cudaMemcpyHostToDevice, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->hn = 0;
+  h->hp = 1;
+  h->hpp = 2;
+  return DNS_OK;
+}
+
+// encalc2 of the stored state -> device scalars (force for the next step)
+static int refresh_flow(dns_handle *h, double force_file) {
+  DevState st{force_file, 0., 0., 0.};
+  CUDA_TRY(cudaMemcpyAsync(h->state, &st, sizeof st, cudaMemcpyHostToDevice, h->stream));
+  launch_flow_sums_f64(h->fc[h->cur_c], h->ff[h->cur_f], h->state, h->partials, h->pl, h->d, h->shape, h->sp,
+                       h->stream);
+  CUDA_TRY(cudaGetLastError());
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DNS_OK;
+}
+
+extern "C" int dns_export_state(dns_handle *h, int level, double *aos_out) {
+  if (!h || !aos_out || level < 0 || level > 2) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  return export_level(h, level, aos_out);
+}
+
+extern "C" int dns_import_state(dns_handle *h, int level, const double *aos_in) {
+  if (!h || !aos_in || level < 0 || level > 2) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  int rc = import_level(h, level, aos_in);
+  if (rc) return rc;
+  return refresh_flow(h, h->p.force_const);
+}
+
+extern "C" int dns_export_history(dns_handle *h, double *out) {
+  if (!h || !out) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  return export_history(h, out);
+}
+
+extern "C" int dns_get_force(dns_handle *h, double *force) {
+  if (!h || !force) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  DevState st;
+  CUDA_TRY(cudaMemcpyAsync(&st, h->state, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  *force = st.force;
+  return DNS_OK;
+}
+
+extern "C" int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double amp) {
+  if (!h) return fail(DNS_EINVAL, "null handle");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  h->cur_c = 0;
+  h->cur_f = 0;
+  h->hn = 0;
+  h->hp = 1;
+  h->hpp = 2;
+  launch_seed_f64(h->fc[0], h->ff[0], h->hist, h->d, seed, uc, amp, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  std::fill(h->wall_lo.begin(), h->wall_lo.end(), 0.0);
+  std::fill(h->wall_hi.begin(), h->wall_hi.end(), 0.0);
+  h->ss = 0;
+  h->tm = h->p.TSTR;
+  return refresh_flow(h, h->p.forcing == DNS_FORCING_CFR ? 0.0 : h->p.force_const);
+}
+
+// ---------------------------------------------------------------- restart files
+static int read_file(const std::string &fn, double *dst, size_t n, size_t skip = 0) {
+  FILE *fp = std::fopen(fn.c_str(), "rb");
+  if (!fp) return fail(DNS_EIO, "cannot open " + fn);
+  if (skip && std::fseek(fp, (long)(skip * 8), SEEK_SET) != 0) {
+    std::fclose(fp);
+    return fail(DNS_EIO, "seek failed in " + fn);
+  }
+  size_t got = std::fread(dst, 8, n, fp);
+  std::fclose(fp);
+  if (got != n) return fail(DNS_EIO, "short read in " + fn);
+  return DNS_OK;
+}
+
+static std::string cname(const char *dir, const char *base, int cntr) {
+  char buf[64];
+  std::snprintf(buf, sizeof buf, "%s.%.4d", base, cntr);
+  return std::string(dir) + "/" + buf;
+}
+
+extern "C" int dns_load_restart(dns_handle *h, const char *dir, int cntr) {
+  if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const dns_geometry &g = h->g;
+  std::vector<double> buf(19ull * std::max((size_t)g.nzc * g.ny * g.nx, (size_t)g.zdf * g.nyf * g.nxf));
+  int rc;
+  // lbf-c: [ftemp | f]; the post-stream state is the first half (:1006-1016)
+  if ((rc = read_file(cname(dir, "lbf-c", cntr), buf.data(), 19ull * g.nzc * g.ny * g.nx))) return rc;
+  if ((rc = import_level(h, 0, buf.data()))) return rc;
+  if ((rc = read_file(cname(dir, "lbf-slf", cntr), buf.data(), 19ull * g.zdf * g.nyf * g.nxf))) return rc;
+  if ((rc = import_level(h, 1, buf.data()))) return rc;
+  if ((rc = read_file(cname(dir, "lbf-suf", cntr), buf.data(), 19ull * g.zdf * g.nyf * g.nxf))) return rc;
+  if ((rc = import_level(h, 2, buf.data()))) return rc;
+  double force = 0.;
+  if ((rc = read_file(cname(dir, "force", cntr), &force, 1))) return rc;
+  const size_t per = (size_t)g.nx * g.ny * 23;
+  std::vector<double> hist(3 * 2 * per), one(3 * per);
+  const char *hn[2] = {"lbf-lin", "lbf-uin"};
+  for (int w = 0; w < 2; w++) {
+    if ((rc = read_file(cname(dir, hn[w], cntr), one.data(), 3 * per))) return rc;
+    for (int l = 0; l < 3; l++) std::memcpy(hist.data() + ((size_t)l * 2 + w) * per, one.data() + l * per, per * 8);
+  }
+  if ((rc = import_history(h, hist.data()))) return rc;
+  h->ss = 0;
+  h->tm = cntr;
+  return refresh_flow(h, h->p.forcing == DNS_FORCING_CFR ? force : h->p.force_const);
+}
+
+static int write_file(const std::string &fn, const double *a, size_t n, int copies) {
+  FILE *fp = std::fopen(fn.c_str(), "wb");
+  if (!fp) return fail(DNS_EIO, "cannot create " + fn);
+  bool ok = true;
+  for (int c = 0; c < copies; c++) ok = ok && std::fwrite(a, 8, n, fp) == n;
+  ok = (std::fclose(fp) == 0) && ok;
+  return ok ? DNS_OK : fail(DNS_EIO, "short write in " + fn);
+}
+
+extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
+  if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const dns_geometry &g = h->g;
+  std::vector<double> buf(19ull * std::max((size_t)g.nzc * g.ny * g.nx, (size_t)g.zdf * g.nyf * g.nxf));
+  int rc;
+  // [ftemp | f]: the second half is the reference's scratch lattice, which its
+  // step overwrites before reading; the post-stream state fills both halves
+  const char *names[3] = {"lbf-c", "lbf-slf", "lbf-suf"};
+  for (int lv = 0; lv < 3; lv++) {
+    if ((rc = export_level(h, lv, buf.data()))) return rc;
+    const size_t n = lv == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
+    if ((rc = write_file(cname(dir, names[lv], cntr), buf.data(), n, 2))) return rc;
+  }
+  double force;
+  if ((rc = dns_get_force(h, &force))) return rc;
+  if ((rc = write_file(cname(dir, "force", cntr), &force, 1, 1))) return rc;
+  const size_t per = (size_t)g.nx * g.ny * 23;
+  std::vector<double> hist(3 * 2 * per), one(3 * per);
+  if ((rc = export_history(h, hist.data()))) return rc;
+  const char *hn[2] = {"lbf-lin", "lbf-uin"};
+  for (int w = 0; w < 2; w++) {
+    for (int l = 0; l < 3; l++) std::memcpy(one.data() + l * per, hist.data() + ((size_t)l * 2 + w) * per, per * 8);
+    if ((rc = write_file(cname(dir, hn[w], cntr), one.data(), 3 * per, 1))) return rc;
+  }
+  return DNS_OK;
+}
+
+// ---------------------------------------------------------------- stepping
+static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
+  const Dims &d = h->d;
+  const LaunchShape &s = h->shape;
+  const int nc = 1 - h->cur_c;
+  PROFILED(h, 0, launch_coarse_f64(h->fc[h->cur_c], h->fc[nc], d, s, h->g.omega_c, h->state, h->partials, h->pl,
+                                   sample, h->stream));
+  // rotate history: the new level n takes the slot of pp (xcomputations.c:548-556)
+  const int t = h->hpp;
+  h->hpp = h->hp;
+  h->hp = h->hn;
+  h->hn = t;
+  const size_t hslot = 2ull * 23 * d.ny * d.nx;
+  PROFILED(h, 1, launch_extract_f64(h->fc[nc], h->hist + h->hn * hslot, d, s, h->stream));
+  for (int it = 1; it <= d.gr; it++) {
+    const int nf = 1 - h->cur_f;
+    PROFILED(h, 2, launch_fine_f64(h->ff[h->cur_f], h->ff[nf], h->wflag, d, s, h->g.omega_f, h->state,
+                                   h->partials, h->pl, it == 1, it == d.gr, sample && it == 1, h->stream));
+    PROFILED(h, 3, launch_interface_f64(h->hist + h->hn * hslot, h->hist + h->hp * hslot, h->hist + h->hpp * hslot,
+                                        h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, h->stream));
+    h->cur_f = nf;
+  }
+  PROFILED(h, 4, launch_inject_f64(h->ff[h->cur_f], h->fc[nc], d, s, h->g.omega_c, h->g.omega_f, h->partials,
+                                   h->pl, h->stream));
+  PROFILED(h, 5, launch_finalize(h->state, log_row, h->partials, h->pl, d, s, h->sp, h->stream));
+  if (sample) PROFILED(h, 6, launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, s, h->stream));
+  h->cur_c = nc;
+}
+
+extern "C" int dns_step(dns_handle *h, long ncoarse, dns_step_log *log) {
+  if (!h || ncoarse < 0) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const double dt = h->g.gr * 1. / ((double)(0.5 * (h->g.nzs - 2.) / h->p.CFL));
+  long done = 0;
+  int status = DNS_OK;
+  while (done < ncoarse) {
+    const long n = std::min<long>(h->prof.on ? kProfSteps : kLogCap, ncoarse - done);
+    const long ss0 = h->ss;
+    for (long q = 0; q < n; q++) {
+      const bool sample = h->sample_every > 0 && (h->ss % h->sample_every) == 0;
+      issue_step(h, h->dlog + q, sample);
+      h->ss++;
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(h->hlog, h->dlog, n * sizeof(DevLog), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    prof_collect(h);
+    for (long q = 0; q < n; q++) {
+      const DevLog &r = h->hlog[q];
+      if (log) {
+        dns_step_log &o = log[done + q];
+        o.time = (double)h->tm + dt * (double)(ss0 + q);
+        o.force = r.force;
+        o.momentum = r.momentum;
+        o.denst = r.denst;
+        o.flowrate = r.flowrate;
+        o.stup = r.stup;
+        o.stdown = r.stdown;
+        o.stress = r.stress;
+        o.pgrad = r.pgrad;
+      }
+      if (status == DNS_OK && !std::isfinite(r.stress)) {
+        status = fail(DNS_ENAN, "non-finite wall shear stress at step " + std::to_string(ss0 + q));
+      }
+    }
+    done += n;
+    if (status != DNS_OK) break;
+  }
+  return status;
+}
+
+// ---------------------------------------------------------------- statistics
+extern "C" int dns_set_sampling(dns_handle *h, long every) {
+  if (!h || every < 0) return fail(DNS_EINVAL, "bad argument");
+  h->sample_every = every;
+  return DNS_OK;
+}
+
+extern "C" int dns_stats_reset(dns_handle *h) {
+  if (!h) return fail(DNS_EINVAL, "null handle");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  CUDA_TRY(cudaMemsetAsync(h->stats_acc, 0, (size_t)h->g.nz_profile * 16 * 8, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  return DNS_OK;
+}
+
+// z/H of the composite profile points (statistics.c:319-329)
+static void profile_z(const dns_geometry &g, std::vector<double> &z) {
+  const int NZ = g.nz_profile, zdf = g.zdf, zdc = g.nzc, GR = g.gr;
+  z.assign(NZ, 0.0);
+  for (int k = 1; k < zdf; k++) z[k] = k - 0.5;
+  for (int k = 2; k < zdc - 2; k++) z[zdf - 2 + k] = GR * (k - 1) + (zdf - 1 - 0.5);
+  for (int k = 0; k < zdf - 1; k++) z[zdf + zdc - 4 + k] = k + GR * (zdc - 3) + zdf - 1. - 0.5;
+  z[2 * zdf + zdc - 5] = 2 * zdf + GR * (zdc - 4) + GR - 3;
+  for (int k = 0; k < NZ; k++) z[k] /= ((double)(g.nzs - 2.));
+}
+
+extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
+  if (!h || !out) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const int NZ = h->g.nz_profile;
+  std::vector<double> acc((size_t)NZ * 16);
+  CUDA_TRY(cudaMemcpyAsync(acc.data(), h->stats_acc, acc.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  std::vector<double> z;
+  profile_z(h->g, z);
+  long ns = 0;
+  for (int p = 0; p < NZ; p++) ns = std::max(ns, (long)acc[(size_t)p * 16 + 15]);
+  if (nsamples) *nsamples = ns;
+  std::memset(out, 0, sizeof(double) * DNS_NSTAT * NZ);
+  for (int p = 0; p < NZ; p++) {
+    const double *a = acc.data() + (size_t)p * 16;
+    out[0 * NZ + p] = z[p];
+    const double S = a[15], N = a[14];
+    if (S <= 0 || N <= 0) continue;
+    const double T = S * N;  // samples x nodes
+    out[1 * NZ + p] = a[0] / T;
+    out[2 * NZ + p] = a[1] / T;
+    out[3 * NZ + p] = a[2] / T;
+    out[4 * NZ + p] = a[3] / T;
+    for (int c = 0; c < 5; c++) out[(5 + c) * NZ + p] = a[9 + c] / S;
+    const double mu = a[0] / T, mv = a[1] / T, mw = a[2] / T;
+    out[10 * NZ + p] = a[4] / T - mu * mu;
+    out[11 * NZ + p] = a[5] / T - mv * mv;
+    out[12 * NZ + p] = a[6] / T - mw * mw;
+    out[13 * NZ + p] = a[7] / T - mu * mw;
+  }
+  return DNS_OK;
+}
+
+// instantaneous plane statistics exactly as statistics.c:48-300 (two passes over
+// the exported state, same summation order)
+extern "C" int dns_plane_stats(dns_handle *h, double *out) {
+  if (!h || !out) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const dns_geometry &g = h->g;
+  const int zdf = g.zdf, zdc = g.nzc, NZ = g.nz_profile;
+  std::vector<double> lv[3];
+  lv[0].resize(19ull * g.nzc * g.ny * g.nx);
+  lv[1].resize(19ull * g.zdf * g.nyf * g.nxf);
+  lv[2].resize(19ull * g.zdf * g.nyf * g.nxf);
+  int rc;
+  for (int l = 0; l < 3; l++)
+    if ((rc = export_level(h, l, lv[l].data()))) return rc;
+  static const int EX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0};
+  static const int EY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+  static const int EZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+  double *U = out, *V = out + NZ, *W = out + 2 * NZ, *UT = out + 3 * NZ, *VT = out + 4 * NZ, *WT = out + 5 * NZ,
+         *RE = out + 6 * NZ, *DA = out + 7 * NZ, *DT = out + 8 * NZ;
+  std::memset(out, 0, sizeof(double) * 9 * NZ);
+  struct Seg { int lvl, k0, k1, off, ex, ey, nz, d0, d1; } segs[3] = {
+      {1, 1, zdf, 0, g.nxf, g.nyf, zdf, 0, zdf},
+      {0, 2, zdc - 2, zdf - 2, g.nx, g.ny, zdc, zdf, zdf + zdc - 4},
+      {2, 0, zdf - 1, zdf + zdc - 4, g.nxf, g.nyf, zdf, zdf + zdc - 4, 2 * zdf + zdc - 4}};
+  for (int pass = 0; pass < 2; pass++)
+    for (const Seg &sg : segs) {
+      const double *a = lv[sg.lvl].data();
+      for (int i = 0; i < sg.ex; i++)
+        for (int j = 0; j < sg.ey; j++)
+          for (int k = sg.k0; k < sg.k1; k++) {
+            const double *f = a + (((size_t)i * sg.ey + j) * sg.nz + k) * 19;
+            double u = 0., v = 0., w = 0., dens = 0.;
+            for (int q = 0; q < 19; q++) {
+              dens += f[q];
+              u += (double)EX[q] * f[q];
+              v += (double)EY[q] * f[q];
+              w += (double)EZ[q] * f[q];
+            }
+            const int p = sg.off + k;
+            if (pass == 0) {
+              U[p] += (u / dens);
+              V[p] += (v / dens);
+              W[p] += (w / dens);
+              DA[p] += dens;
+            } else {
+              const double uf = (u / dens) - U[p], vf = (v / dens) - V[p], wf = (w / dens) - W[p],
+                           df = dens - DA[p];
+              UT[p] += uf * uf;
+              VT[p] += vf * vf;
+              WT[p] += wf * wf;
+              RE[p] += uf * wf;
+              DT[p] += df * df;
+            }
+          }
+      const double norm = (double)(sg.ex * sg.ey * 1 * 1);
+      for (int p = sg.d0; p < sg.d1; p++) {
+        if (pass == 0) {
+          U[p] /= norm; V[p] /= norm; W[p] /= norm; DA[p] /= norm;
+        } else {
+          UT[p] /= norm; VT[p] /= norm; WT[p] /= norm; RE[p] /= norm; DT[p] /= norm;
+        }
+      }
+    }
+  for (int p = 0; p < NZ; p++) {
+    UT[p] = std::sqrt(UT[p]);
+    VT[p] = std::sqrt(VT[p]);
+    WT[p] = std::sqrt(WT[p]);
+    DT[p] = std::sqrt(DT[p]);
+  }
+  return DNS_OK;
+}
+
+// ---------------------------------------------------------------- measurement
+extern "C" int dns_set_profiling(dns_handle *h, int on) {
+  if (!h) return fail(DNS_EINVAL, "null handle");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  prof_collect(h);
+  h->prof.on = on != 0;
+  if (h->prof.on)
+    for (int c = 0; c < DNS_NKERNEL; c++) {
+      h->prof.ms[c] = 0.;
+      h->prof.cnt[c] = 0;
+    }
+  return DNS_OK;
+}
+
+extern "C" int dns_kernel_times(dns_handle *h, double *ms, long *launches) {
+  if (!h) return fail(DNS_EINVAL, "null handle");
+  for (int c = 0; c < DNS_NKERNEL; c++) {
+    if (ms) ms[c] = h->prof.ms[c];
+    if (launches) launches[c] = h->prof.cnt[c];
+  }
+  return DNS_OK;
+}
+
+// ---------------------------------------------------------------- errors
+extern "C" const char *dns_error_string(int code) {
+  switch (code) {
+    case DNS_OK: return "ok";
+    case DNS_EINVAL: return "invalid argument";
+    case DNS_ENOMEM: return "out of memory";
+    case DNS_EIO: return "i/o error";
+    case DNS_ENAN: return "non-finite wall shear stress";
+    case DNS_ETIMEOUT: return "device wait timed out";
+    case DNS_ECUDA: return "CUDA error";
+    default: return "unknown error";
+  }
+}
+
+extern "C" const char *dns_last_error(void) { return g_last_error.c_str(); }

@@ -1,0 +1,88 @@
+// Host-side launchers of the device kernels (internal to libdnsembed).
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+namespace dns {
+
+// Device-side scalar state carried between steps (one instance per handle).
+struct DevState {
+  double force;     // force[0] of the next step
+  double momentum;  // encalc2 momentum of the current state
+  double denst;     // encalc2 mass of the current state
+  double pad;
+};
+
+// One row of the per-step log, filled on the device (time is added on the host).
+struct DevLog {
+  double force, momentum, denst, flowrate, stup, stdown, stress, pgrad;
+};
+
+struct Dims {
+  int nx, ny, nzc;        // coarse
+  int nxf, nyf, zdf, zds; // fine block; zds planes stored per block
+  int gr, nzs;
+};
+
+// Launch geometry shared by the kernels and the reductions.
+struct LaunchShape {
+  int bx;          // threads per block along x
+  int jb;          // rows (y) per block
+  int cgx, cgy;    // coarse grid x/y blocks (z = nzc planes)
+  int fgx, fgy;    // fine grid x/y blocks (z = 2 zds planes)
+  int igx, igy;    // interface tile grid
+  int jgx, jgy;    // injection / extraction grid (x, y) per wall
+  long n_coarse_blocks() const { return (long)cgx * cgy; }  // per plane
+  long n_fine_blocks() const { return (long)fgx * fgy; }    // per plane
+};
+
+LaunchShape make_shape(const Dims &d);
+
+// Reduction scratch sizes (doubles) for a given shape.
+struct PartialLayout {
+  long coarse, fine, inject, wall, stats_c, stats_f, flow;  // offsets into one buffer
+  long total;
+};
+PartialLayout partial_layout(const Dims &d, const LaunchShape &s);
+
+struct StepParams {
+  double omega_c, omega_f;
+  double ub;        // bulk velocity (constant flow rate target)
+  double gconst;    // constant body force
+  int cfr;          // 1: force = ub - momentum
+};
+
+// --- FP64 kernels (kernels_f64.cu) ---
+void launch_coarse_f64(const double *src, double *dst, const Dims &d, const LaunchShape &s, double om,
+                       const DevState *st, double *partials, const PartialLayout &pl, bool stats,
+                       cudaStream_t stream);
+void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s,
+                        cudaStream_t stream);
+void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
+                     double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
+                     bool last, bool stats, cudaStream_t stream);
+void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *fdst, const Dims &d,
+                          const LaunchShape &s, int substep, double omega_c, double omega_f,
+                          cudaStream_t stream);
+void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
+                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
+void launch_finalize(DevState *st, DevLog *log_row, const double *partials, const PartialLayout &pl,
+                     const Dims &d, const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
+void launch_stats_finalize(double *acc, const double *partials, const PartialLayout &pl, const Dims &d,
+                           const LaunchShape &s, cudaStream_t stream);
+// direct encalc2 reduction of the stored state into st (momentum, denst, force)
+void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,
+                          const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
+                          cudaStream_t stream);
+void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
+                     cudaStream_t stream);
+// layout transposes between the device SoA state and the reference AoS order
+void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream);
+void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream);
+
+}  // namespace dns

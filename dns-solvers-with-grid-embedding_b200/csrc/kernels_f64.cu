@@ -1,0 +1,806 @@
+// FP64 plain-form kernels of the grid-embedded D3Q19 channel step.
+//
+// Built with -fmad=false: together with the operation order of lattice.cuh the
+// per-node arithmetic is bit-identical to the reference compiled without fused
+// multiply-add.  Only the constant-flow-rate reduction (a sum over the whole
+// domain) is associated differently from the reference's sequential loop.
+//
+// Device layout (structure of arrays, x fastest, one array per population):
+//   coarse  fc[a][k][j][i]   k = 0..zdc-1, j < ydv, i < xdv
+//   fine    ff[a][p][j][i]   p = 0..zds-1 : lower block k = p + 1 (1..zdf-1)
+//                            p = zds..2zds-1 : upper block k = p - zds (0..zdf-2)
+//   wall flags wf[j][i] (-1 no-slip, -2 slip), identical on both walls
+//   interface history h[wall][field][j][i], fields [rho, ux, uy, uz, fneq_0..18]
+// The state between coarse steps is the post-stream state S (the reference's
+// ftemp arrays after exchange); kernels read S from one buffer, collide, and
+// push into the other (ping-pong), with the periodic wrap in x and y replacing
+// the reference's ghost column/row and halo exchange.
+#include "bicubic_gen.cuh"
+#include "kernels.h"
+#include "lattice.cuh"
+
+namespace dns {
+
+namespace {
+
+constexpr int kMaxThreads = 128;
+
+__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+
+// Fixed-order block reduction of N doubles; thread 0 returns the sums.
+template <int N>
+__device__ __forceinline__ void block_reduce(double (&v)[N], double *out) {
+  __shared__ double red[N][kMaxThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+      double s = red[q][0];
+      for (int w = 1; w < nw; w++) s += red[q][w];
+      out[q] = s;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void load19(const double *__restrict__ src, size_t idx, size_t stride, double (&f)[19]) {
+#pragma unroll
+  for (int a = 0; a < 19; a++) f[a] = __ldg(src + idx + (size_t)a * stride);
+}
+
+// ------------------------------------------------------------------ coarse
+// Collide every coarse plane (xcomputations.c:49-86, 291-342) and push into
+// planes 1..zdc-2 (:135-204, 353-420).  Planes 0 and zdc-1 of dst are
+// rewritten by the fine-to-coarse injection, so pushes into them are dropped.
+// Partials: constant-flow-rate momentum/mass of what lands in dst (all weight
+// GR^3 in encalc2.c:57-84); with STATS the pre-collision plane moments.
+template <bool STATS>
+__global__ void __launch_bounds__(kMaxThreads) coarse_kernel(const double *__restrict__ src, double *__restrict__ dst,
+                                                            Dims d, int jb, double om, const DevState *st,
+                                                            double *__restrict__ part, double *__restrict__ spart) {
+  const int nx = d.nx, ny = d.ny, nzc = d.nzc;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.z;
+  const size_t pstride = (size_t)nzc * ny * nx;
+  const double G = st->force;
+  double acc[2] = {0., 0.};
+  double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+  for (int r = 0; r < jb; r++) {
+    const int j = blockIdx.y * jb + r;
+    if (i >= nx || j >= ny) continue;
+    double f[19];
+    load19(src, ((size_t)k * ny + j) * nx + i, pstride, f);
+    double dens, u0, u1, u2;
+    collide_f64(f, om, G, dens, u0, u1, u2);
+    if (STATS) {
+      sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += dens;
+      sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += dens * dens;
+    }
+    const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      const int k2 = k + ez_of(a);
+      if (k2 < 1 || k2 > nzc - 2) continue;
+      const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
+      const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
+      dst[(size_t)a * pstride + ((size_t)k2 * ny + j2) * nx + i2] = f[a];
+      acc[1] += f[a];
+      if (ex_of(a) > 0) acc[0] += f[a];
+      if (ex_of(a) < 0) acc[0] -= f[a];
+    }
+  }
+  const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  block_reduce<2>(acc, part + blk * 2);
+  if (STATS) block_reduce<9>(sacc, spart + blk * 9);
+}
+
+// Interface planes of the new coarse state into history level n
+// (xcomputations.c:558-625): [rho, u, f - feq] at k = 1 (lower) and zdc-2.
+__global__ void __launch_bounds__(kMaxThreads) extract_kernel(const double *__restrict__ fc, double *__restrict__ hn,
+                                                             Dims d) {
+  const int nx = d.nx, ny = d.ny, nzc = d.nzc;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, w = blockIdx.z;
+  if (i >= nx) return;
+  const int k = w == 0 ? 1 : nzc - 2;
+  const size_t pstride = (size_t)nzc * ny * nx, plane = (size_t)ny * nx;
+  double f[19];
+  load19(fc, ((size_t)k * ny + j) * nx + i, pstride, f);
+  double dens, mx, my, mz;
+  moments_f64(f, dens, mx, my, mz);
+  const double u0 = mx / dens, u1 = my / dens, u2 = mz / dens;
+  const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+  const Weighted wr = weighted_rho(dens);
+  double *o = hn + (size_t)w * 23 * plane + (size_t)j * nx + i;
+  o[0] = dens;
+  o[plane] = u0;
+  o[2 * plane] = u1;
+  o[3 * plane] = u2;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int c = wclass_of(a);
+    const double feq = feq_f64(c == 0 ? wr.w0 : (c == 1 ? wr.w1 : wr.w2), proj_f64(a, u0, u1, u2), t15v);
+    o[(size_t)(4 + a) * plane] = f[a] - feq;
+  }
+}
+
+// ------------------------------------------------------------------ fine
+// Both near-wall blocks in one launch (xfcomputations.c:43-214, 599-712
+// collision with force G/GR; :215-442, 724-897 streaming).  At a wall plane
+// destination d = x + e_a with flags sld = flag(d), sld1 = flag(column of x):
+//   sld = -1 and sld1 = -1 : half-way bounce-back into f(x, opposite a)
+//   otherwise (slip involved): specular reflection into f(d_i, d_j, x_k, mirror a)
+// Pushes into the interface planes are dropped (the coarse-to-fine transfer
+// rewrites them).  MODE bits: 1 constant-flow-rate partials of dst (last
+// substep; encalc2.c:33-53, 86-107 weights), 2 wall-shear plane sums of the
+// pre-collision state (first substep; wshearstr.c:37-134), 4 plane statistics.
+template <int MODE>
+__global__ void __launch_bounds__(kMaxThreads) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
+                                                          const int8_t *__restrict__ wf, Dims d, int jb, double om,
+                                                          const DevState *st, double *__restrict__ part,
+                                                          double *__restrict__ wpart, double *__restrict__ spart) {
+  const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
+  const int P = 2 * zds;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int p = blockIdx.z;
+  const bool upper = p >= zds;
+  const int k = upper ? p - zds : p + 1;  // reference k inside the block
+  const int kwall = upper ? zdf - 1 : 0;
+  const size_t pstride = (size_t)P * ny * nx;
+  const double Gf = (1. / ((double)gr)) * st->force;
+  // encalc2 weight of a destination plane (block-uniform)
+  auto weight = [&](int kd) -> double {
+    if (!upper) return (kd >= 1 && kd < zdf - gr) ? 1.0 : 0.0;
+    return (kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5 : 1.0) : 0.0;
+  };
+  const bool wall_sum_plane =
+      upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
+  const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
+  double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
+  double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+  for (int r = 0; r < jb; r++) {
+    const int j = blockIdx.y * jb + r;
+    if (i >= nx || j >= ny) continue;
+    double f[19];
+    load19(src, ((size_t)p * ny + j) * nx + i, pstride, f);
+    double dens, u0, u1, u2;
+    collide_f64(f, om, Gf, dens, u0, u1, u2);
+    if (MODE & 2) {
+      if (wall_sum_plane) wacc[0] += u0;
+      if (wall_rho_plane) wacc[1] += dens;
+    }
+    if (MODE & 4) {
+      sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += dens;
+      sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += dens * dens;
+    }
+    const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+    const int8_t own = wf[(size_t)j * nx + i];
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      const int k2 = k + ez_of(a);
+      const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
+      const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
+      int pd, id, jd, ad, kd, exd;
+      if (k2 == kwall) {
+        const int8_t sld = wf[(size_t)j2 * nx + i2];
+        if (sld == -1 && own == -1) {
+          pd = p; id = i; jd = j; ad = opp_of(a); exd = -ex_of(a);
+        } else {
+          pd = p; id = i2; jd = j2; ad = mir_of(a); exd = ex_of(a);
+        }
+        kd = k;
+      } else {
+        if (!upper && k2 >= zdf - 1) continue;
+        if (upper && k2 <= 0) continue;
+        pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
+      }
+      dst[(size_t)ad * pstride + ((size_t)pd * ny + jd) * nx + id] = f[a];
+      if (MODE & 1) {
+        const double wgt = weight(kd);
+        acc[1] += wgt * f[a];
+        if (exd > 0) acc[0] += wgt * f[a];
+        if (exd < 0) acc[0] -= wgt * f[a];
+      }
+    }
+  }
+  const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (MODE & 1) block_reduce<2>(acc, part + blk * 2);
+  if ((MODE & 2) && wall_sum_plane) block_reduce<2>(wacc, wpart + blk * 2);
+  if (MODE & 4) block_reduce<9>(sacc, spart + blk * 9);
+}
+
+// ------------------------------------------------------------------ interface
+// Coarse-to-fine transfer for one substep, both walls (tinterpolate_hrmt.c,
+// derivative.c, bcucof_opt.c, ctfdtransfer_opt.c): Hermite interpolation in
+// time of the three history levels, 4th-order central derivatives d/dx, d/dy,
+// d2/dxdy, bicubic coefficients per coarse cell, Horner evaluation at the
+// GR x GR fine nodes and f = feq + omega_c/(GR omega_f) fneq.  A tile of
+// ITX x ITY coarse cells stages the (ITX+5) x (ITY+5) periodic patch of one
+// field at a time in shared memory; one thread owns one coarse cell.
+constexpr int ITX = 16, ITY = 8;
+constexpr int PX = ITX + 5, PY = ITY + 5;
+
+struct IfaceArgs {
+  double h1, h2, h3, h4, fac;
+};
+
+template <int GR>
+__global__ void __launch_bounds__(ITX *ITY) interface_kernel(const double *__restrict__ hn,
+                                                             const double *__restrict__ hp,
+                                                             const double *__restrict__ hpp,
+                                                             double *__restrict__ fdst, Dims d, IfaceArgs ia) {
+  __shared__ double V[PY][PX];
+  __shared__ double Dy[ITY + 1][PX];
+  __shared__ double Dx[ITY + 1][ITX + 1];
+  __shared__ double Dxy[ITY + 1][ITX + 1];
+  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf, zds = d.zds;
+  const int w = blockIdx.z;
+  const int i0 = blockIdx.x * ITX, j0 = blockIdx.y * ITY;
+  const int tx = threadIdx.x % ITX, ty = threadIdx.x / ITX;
+  const int ic = i0 + tx, jc = j0 + ty;
+  const bool valid = ic < nx && jc < ny;
+  const size_t plane = (size_t)ny * nx;
+  const int pf = w == 0 ? zds - 1 : zds;  // interface plane of the fine block
+  const size_t fstride = (size_t)2 * zds * nyf * nxf;
+  constexpr int NN = GR * GR;
+  double rho[NN], ua[NN], ub[NN], uc[NN], t15v[NN];
+  const double c2o3 = 2. / 3., c1o12 = 1. / 12.;
+  for (int b = 0; b < 23; b++) {
+    const size_t fo = ((size_t)w * 23 + b) * plane;
+    for (int q = threadIdx.x; q < PX * PY; q += blockDim.x) {
+      const int pi = q % PX, pj = q / PX;
+      const int gi = wrapi(i0 - 2 + pi, nx), gj = wrapi(j0 - 2 + pj, ny);
+      const size_t g = fo + (size_t)gj * nx + gi;
+      const double n = hn[g], pv = hp[g], pp = hpp[g];
+      const double c1 = pv;
+      const double c2 = (n - pp) * 0.5;
+      const double c3 = n;
+      const double c4 = (3. * n - 4. * pv + pp) * 0.5;
+      V[pj][pi] = ia.h1 * c1 + ia.h2 * c2 + ia.h3 * c3 + ia.h4 * c4;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < PX * (ITY + 1); q += blockDim.x) {
+      const int pi = q % PX, r = q / PX, pj = r + 2;
+      Dy[r][pi] = c2o3 * (V[pj + 1][pi] - V[pj - 1][pi]) - c1o12 * (V[pj + 2][pi] - V[pj - 2][pi]);
+      if (pi >= 2 && pi < ITX + 3)
+        Dx[r][pi - 2] = c2o3 * (V[pj][pi + 1] - V[pj][pi - 1]) - c1o12 * (V[pj][pi + 2] - V[pj][pi - 2]);
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < (ITX + 1) * (ITY + 1); q += blockDim.x) {
+      const int c = q % (ITX + 1), r = q / (ITX + 1), pi = c + 2;
+      Dxy[r][c] = c2o3 * (Dy[r][pi + 1] - Dy[r][pi - 1]) - c1o12 * (Dy[r][pi + 2] - Dy[r][pi - 2]);
+    }
+    __syncthreads();
+    if (valid) {
+      double x[16], cf[16];
+      const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 0, 1, 1};
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int c = tx + ci[q], r = ty + cj[q];
+        x[q] = V[r + 2][c + 2];
+        x[4 + q] = Dx[r][c];
+        x[8 + q] = Dy[r][c + 2];
+        x[12 + q] = Dxy[r][c];
+      }
+      DNS_BICUBIC_COEFFS(cf, x);
+#pragma unroll
+      for (int ii = 0; ii < GR; ii++)
+#pragma unroll
+        for (int jj = 0; jj < GR; jj++) {
+          const double tt = ((double)ii) / ((double)GR);
+          const double uu = ((double)jj) / ((double)GR);
+          double val = 0.;
+#pragma unroll
+          for (int nn = 3; nn > -1; nn--)
+            val = tt * val + ((cf[nn * 4 + 3] * uu + cf[nn * 4 + 2]) * uu + cf[nn * 4 + 1]) * uu + cf[nn * 4 + 0];
+          const int node = ii * GR + jj;
+          if (b == 0) rho[node] = val;
+          else if (b == 1) ua[node] = val;
+          else if (b == 2) ub[node] = val;
+          else if (b == 3) {
+            uc[node] = val;
+            t15v[node] = 1.5 * (ua[node] * ua[node] + ub[node] * ub[node] + uc[node] * uc[node]);
+          } else {
+            const int a = b - 4;
+            const int cls = a == 0 ? 0 : (a <= 6 ? 1 : 2);
+            const double wra = (cls == 0 ? 1. / 3. : (cls == 1 ? 1. / 18. : 1. / 36.)) * rho[node];
+            const double feq = feq_f64(wra, proj_f64(a, ua[node], ub[node], uc[node]), t15v[node]);
+            const int fi = ic * GR + ii, fj = jc * GR + jj;
+            fdst[(size_t)a * fstride + ((size_t)pf * nyf + fj) * nxf + fi] = feq + ia.fac * val;
+          }
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ injection
+// Fine-to-coarse transfer (ftcdtransfer.c:28-115): the fine node on the coarse
+// vertex at lower k = zdf-1-GR / upper k = GR gives the coarse planes 0 and
+// zdc-1 as feq + GR omega_f/omega_c (f - feq).  Partials: what this writes into
+// the state weighs GR^3 / 2 in encalc2.
+__global__ void __launch_bounds__(kMaxThreads) inject_kernel(const double *__restrict__ fsrc,
+                                                            double *__restrict__ cdst, Dims d, double fac,
+                                                            double *__restrict__ part) {
+  const int nx = d.nx, ny = d.ny, nzc = d.nzc, gr = d.gr, zdf = d.zdf, zds = d.zds;
+  const int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y, w = blockIdx.z;
+  double acc[2] = {0., 0.};
+  if (ic < nx) {
+    const int ps = w == 0 ? (zdf - 1 - gr) - 1 : zds + gr;  // lower k = zdf-1-GR, upper k = GR
+    const size_t fstride = (size_t)2 * zds * d.nyf * d.nxf;
+    double f[19];
+    load19(fsrc, ((size_t)ps * d.nyf + (size_t)jc * gr) * d.nxf + (size_t)ic * gr, fstride, f);
+    double dens, mx, my, mz;
+    moments_f64(f, dens, mx, my, mz);
+    const double u0 = mx / dens, u1 = my / dens, u2 = mz / dens;
+    const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+    const Weighted wr = weighted_rho(dens);
+    const int kc = w == 0 ? 0 : nzc - 1;
+    const size_t cstride = (size_t)nzc * ny * nx;
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      const int c = wclass_of(a);
+      const double feq = feq_f64(c == 0 ? wr.w0 : (c == 1 ? wr.w1 : wr.w2), proj_f64(a, u0, u1, u2), t15v);
+      const double fn = feq + fac * (f[a] - feq);
+      cdst[(size_t)a * cstride + ((size_t)kc * ny + jc) * nx + ic] = fn;
+      acc[1] += fn;
+      if (ex_of(a) > 0) acc[0] += fn;
+      if (ex_of(a) < 0) acc[0] -= fn;
+    }
+  }
+  const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  block_reduce<2>(acc, part + blk * 2);
+}
+
+// ------------------------------------------------------------------ direct encalc2
+// encalc2 sums of a stored state (used after a load / seed and by dns_get_force):
+// one block partial per (plane, row-block) of each level.
+__global__ void __launch_bounds__(kMaxThreads) flow_sums_kernel(const double *__restrict__ fc,
+                                                               const double *__restrict__ ff, Dims d, int jb,
+                                                               int ncoarse_planes, double *__restrict__ part) {
+  const int z = blockIdx.z;
+  const bool coarse = z < ncoarse_planes;
+  const int nx = coarse ? d.nx : d.nxf, ny = coarse ? d.ny : d.nyf;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  double acc[2] = {0., 0.};
+  double wgt;
+  const double *base;
+  size_t pstride;
+  int p;
+  const double g3 = (double)d.gr * d.gr * d.gr;
+  if (coarse) {
+    p = z;
+    wgt = (p == 0 || p == d.nzc - 1) ? 0.5 * g3 : g3;
+    base = fc;
+    pstride = (size_t)d.nzc * d.ny * d.nx;
+  } else {
+    p = z - ncoarse_planes;
+    const bool upper = p >= d.zds;
+    const int k = upper ? p - d.zds : p + 1;
+    if (!upper) wgt = (k >= 1 && k < d.zdf - d.gr) ? 1.0 : 0.0;
+    else wgt = (k >= d.gr && k < d.zdf - 1) ? (k == d.gr ? 0.5 : 1.0) : 0.0;
+    base = ff;
+    pstride = (size_t)2 * d.zds * d.nyf * d.nxf;
+  }
+  if (i < nx && blockIdx.x * blockDim.x < nx) {
+    for (int r = 0; r < jb; r++) {
+      const int j = blockIdx.y * jb + r;
+      if (j >= ny) break;
+      double f[19];
+      load19(base, ((size_t)p * ny + j) * nx + i, pstride, f);
+      double dens, mx, my, mz;
+      moments_f64(f, dens, mx, my, mz);
+      acc[0] += wgt * mx;
+      acc[1] += wgt * dens;
+    }
+  }
+  const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  block_reduce<2>(acc, part + blk * 2);
+}
+
+// ------------------------------------------------------------------ finalize
+// Deterministic reduction of the block partials (fixed order, one block) into
+// the next step's encalc2 values and force, plus this step's log row.
+constexpr int kFinThreads = 1024;
+
+__device__ double fixed_sum(const double *p, long n, int stride, int comp) {
+  __shared__ double sh[kFinThreads];
+  double s = 0.;
+  for (long q = threadIdx.x; q < n; q += blockDim.x) s += p[q * stride + comp];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+struct FinArgs {
+  long nc, nf, ni;             // partial counts (pairs)
+  long wb[6];                  // wall-shear plane block offsets (pairs), lower k=1,2,3 then upper zdf-2,-3,-4
+  long wn;                     // blocks per plane
+  double g3, norm, norm2, mu, ub, gconst, pgrad_scale, flow_scale;
+  int cfr, with_log;
+};
+
+__global__ void __launch_bounds__(kFinThreads) finalize_kernel(DevState *st, DevLog *lg, const double *part_c,
+                                                              const double *part_f, const double *part_i,
+                                                              const double *part_w, FinArgs a) {
+  double momc = fixed_sum(part_c, a.nc, 2, 0), denc = fixed_sum(part_c, a.nc, 2, 1);
+  double momf = fixed_sum(part_f, a.nf, 2, 0), denf = fixed_sum(part_f, a.nf, 2, 1);
+  double momi = fixed_sum(part_i, a.ni, 2, 0), deni = fixed_sum(part_i, a.ni, 2, 1);
+  double U[6], D[6];
+  if (a.with_log) {
+    for (int q = 0; q < 6; q++) {
+      U[q] = fixed_sum(part_w + a.wb[q] * 2, a.wn, 2, 0);
+      D[q] = fixed_sum(part_w + a.wb[q] * 2, a.wn, 2, 1);
+    }
+  }
+  if (threadIdx.x == 0) {
+    if (a.with_log) {
+      DevLog r;
+      r.force = st->force;
+      r.momentum = st->momentum;
+      r.denst = st->denst;
+      r.flowrate = st->momentum * a.flow_scale / st->denst;
+      const double stdown = ((-2. * U[0] + 3. * U[1] - U[2]) / a.norm2) * (a.mu * (D[0] / a.norm2));
+      const double stup = (-(2. * U[3] - 3. * U[4] + U[5]) / a.norm2) * (a.mu * (D[5] / a.norm2));
+      r.stup = stup;
+      r.stdown = stdown;
+      r.stress = 0.5 * (stup + stdown);
+      r.pgrad = st->force * a.pgrad_scale;
+      *lg = r;
+    }
+    const double mom = (a.g3 * momc + 0.5 * a.g3 * momi + momf) / a.norm;
+    const double den = (a.g3 * denc + 0.5 * a.g3 * deni + denf) / a.norm;
+    st->momentum = mom;
+    st->denst = den;
+    st->force = a.cfr ? a.ub - mom : a.gconst;
+  }
+}
+
+// per-plane statistics of one sample, accumulated over samples
+// acc[NZ][16]: 0..8 sums over samples of plane sums (u v w rho uu vv ww uw rr),
+// 9..13 sums over samples of per-sample plane variances, 14 nodes per plane, 15 samples
+struct StatsArgs {
+  int nzp;          // composite profile length
+  int zdf, nzc, zds;
+  long bc, bf;      // blocks per plane (coarse, fine)
+  double nc, nf;    // nodes per plane (coarse, fine)
+};
+
+__global__ void __launch_bounds__(256) stats_finalize_kernel(double *acc, const double *spc, const double *spf,
+                                                            StatsArgs a) {
+  __shared__ double sh[256];
+  const int idx = blockIdx.x;
+  const double *src = nullptr;
+  long nb = 0;
+  double nn = 0.;
+  const int zdf = a.zdf, nzc = a.nzc;
+  if (idx >= 1 && idx <= zdf - 1) {  // lower fine k = idx
+    src = spf + (size_t)(idx - 1) * a.bf * 9; nb = a.bf; nn = a.nf;
+  } else if (idx >= zdf && idx <= zdf + nzc - 5) {  // coarse k = idx - zdf + 2
+    src = spc + (size_t)(idx - zdf + 2) * a.bc * 9; nb = a.bc; nn = a.nc;
+  } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {  // upper fine k
+    const int k = idx - (zdf + nzc - 4);
+    src = spf + (size_t)(a.zds + k) * a.bf * 9; nb = a.bf; nn = a.nf;
+  }
+  if (!src) return;
+  double s9[9];
+  for (int c = 0; c < 9; c++) {
+    double s = 0.;
+    for (long q = threadIdx.x; q < nb; q += blockDim.x) s += src[q * 9 + c];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    s9[c] = sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double *o = acc + (size_t)idx * 16;
+    for (int c = 0; c < 9; c++) o[c] += s9[c];
+    const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
+    o[9] += s9[4] / nn - mu * mu;
+    o[10] += s9[5] / nn - mv * mv;
+    o[11] += s9[6] / nn - mw * mw;
+    o[12] += s9[7] / nn - mu * mw;
+    o[13] += s9[8] / nn - mr * mr;
+    o[14] = nn;
+    o[15] += 1.0;
+  }
+}
+
+// ------------------------------------------------------------------ seeded state
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, uint32_t k0,
+                                              uint32_t k1, uint32_t (&out)[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; r++) {
+    if (r > 0) {
+      k0 += 0x9E3779B9u;
+      k1 += 0xBB67AE85u;
+    }
+    const uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    const uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    const uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0; c1 = lo1; c2 = n2; c3 = lo0;
+  }
+  out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+__device__ __forceinline__ void seeded_node(double *dst, size_t stride, uint64_t seed, double uc, double amp,
+                                            double H, double z, uint32_t i, uint32_t j, uint32_t k, uint32_t lvl,
+                                            double *u_out) {
+  uint32_t r[4];
+  philox4x32_10(i, j, k, lvl, (uint32_t)seed, (uint32_t)(seed >> 32), r);
+  const double zeta = z / H;
+  const double prof = 4.0 * uc * zeta * (1.0 - zeta);
+  double u[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const double x = ((double)r[c] + 0.5) * (1.0 / 4294967296.0);
+    u[c] = amp * (2.0 * x - 1.0);
+  }
+  u[0] = prof + u[0];
+  const double t15v = 1.5 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int c = wclass_of(a);
+    const double wr = (c == 0 ? 1. / 3. : (c == 1 ? 1. / 18. : 1. / 36.)) * 1.0;
+    dst[(size_t)a * stride] = feq_f64(wr, proj_f64(a, u[0], u[1], u[2]), t15v);
+  }
+  if (u_out) {
+    u_out[0] = u[0];
+    u_out[1] = u[1];
+    u_out[2] = u[2];
+  }
+}
+
+__global__ void __launch_bounds__(kMaxThreads) seed_kernel(double *fc, double *ff, double *hist3, Dims d,
+                                                          uint64_t seed, double uc, double amp) {
+  const int z = blockIdx.z, j = blockIdx.y;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const double H = d.nzs - 2.0;
+  if (z < d.nzc) {
+    const int k = z;
+    if (i >= d.nx || j >= d.ny) return;
+    const size_t stride = (size_t)d.nzc * d.ny * d.nx;
+    const double zpos = (d.zdf - 1.5) + d.gr * (k - 1.0);
+    double u[3];
+    seeded_node(fc + ((size_t)k * d.ny + j) * d.nx + i, stride, seed, uc, amp, H, zpos, i, j, k, 0, u);
+    if (k == 1 || k == d.nzc - 2) {
+      const size_t plane = (size_t)d.ny * d.nx;
+      const int w = k == 1 ? 0 : 1;
+      for (int l = 0; l < 3; l++) {
+        double *o = hist3 + ((size_t)l * 2 + w) * 23 * plane + (size_t)j * d.nx + i;
+        o[0] = 1.0;
+        o[plane] = u[0];
+        o[2 * plane] = u[1];
+        o[3 * plane] = u[2];
+        for (int b = 4; b < 23; b++) o[(size_t)b * plane] = 0.0;
+      }
+    }
+  } else {
+    const int p = z - d.nzc;
+    if (i >= d.nxf || j >= d.nyf) return;
+    const bool upper = p >= d.zds;
+    const int k = upper ? p - d.zds : p + 1;
+    const double zpos = upper ? (d.zdf - 1.5) + d.gr * (d.nzc - 3.0) + k : k - 0.5;
+    const size_t stride = (size_t)2 * d.zds * d.nyf * d.nxf;
+    seeded_node(ff + ((size_t)p * d.nyf + j) * d.nxf + i, stride, seed, uc, amp, H, zpos, i, j, k,
+                upper ? 2 : 1, nullptr);
+  }
+}
+
+// ------------------------------------------------------------------ transposes
+__global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__restrict__ aos, int nx, int ny, int P,
+                                  int p0, int nz_aos, int k0_aos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= nx) return;
+  const size_t stride = (size_t)P * ny * nx;
+  const size_t s = ((size_t)(p0 + q) * ny + j) * nx + i;
+  double *o = aos + (((size_t)i * ny + j) * nz_aos + k0_aos + q) * 19;
+  for (int a = 0; a < 19; a++) o[a] = soa[s + (size_t)a * stride];
+}
+
+__global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__restrict__ soa, int nx, int ny, int P,
+                                  int p0, int nz_aos, int k0_aos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= nx) return;
+  const size_t stride = (size_t)P * ny * nx;
+  const size_t s = ((size_t)(p0 + q) * ny + j) * nx + i;
+  const double *o = aos + (((size_t)i * ny + j) * nz_aos + k0_aos + q) * 19;
+  for (int a = 0; a < 19; a++) soa[s + (size_t)a * stride] = o[a];
+}
+
+}  // namespace
+
+// ====================================================================== host
+LaunchShape make_shape(const Dims &d) {
+  LaunchShape s;
+  s.bx = 128;
+  s.jb = 2;
+  s.cgx = (d.nx + s.bx - 1) / s.bx;
+  s.cgy = (d.ny + s.jb - 1) / s.jb;
+  s.fgx = (d.nxf + s.bx - 1) / s.bx;
+  s.fgy = (d.nyf + s.jb - 1) / s.jb;
+  s.igx = (d.nx + ITX - 1) / ITX;
+  s.igy = (d.ny + ITY - 1) / ITY;
+  s.jgx = (d.nx + s.bx - 1) / s.bx;
+  s.jgy = d.ny;
+  return s;
+}
+
+PartialLayout partial_layout(const Dims &d, const LaunchShape &s) {
+  PartialLayout pl;
+  const long nbc = s.n_coarse_blocks() * d.nzc, nbf = s.n_fine_blocks() * 2 * d.zds;
+  const long nbi = (long)s.jgx * s.jgy * 2;
+  long o = 0;
+  pl.coarse = o; o += nbc * 2;
+  pl.fine = o; o += nbf * 2;
+  pl.inject = o; o += nbi * 2;
+  pl.wall = o; o += nbf * 2;
+  pl.stats_c = o; o += nbc * 9;
+  pl.stats_f = o; o += nbf * 9;
+  const long gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
+  pl.flow = o; o += gx * gy * (d.nzc + 2 * d.zds) * 2;
+  pl.total = o;
+  return pl;
+}
+
+void launch_coarse_f64(const double *src, double *dst, const Dims &d, const LaunchShape &s, double om,
+                       const DevState *st, double *partials, const PartialLayout &pl, bool stats,
+                       cudaStream_t stream) {
+  dim3 grid(s.cgx, s.cgy, d.nzc), block(s.bx);
+  if (stats)
+    coarse_kernel<true><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
+                                                    partials + pl.stats_c);
+  else
+    coarse_kernel<false><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
+                                                     partials + pl.stats_c);
+}
+
+void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream) {
+  dim3 grid(s.jgx, d.ny, 2), block(s.bx);
+  extract_kernel<<<grid, block, 0, stream>>>(fc, hist_n, d);
+}
+
+void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
+                     double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
+                     bool last, bool stats, cudaStream_t stream) {
+  dim3 grid(s.fgx, s.fgy, 2 * d.zds), block(s.bx);
+  const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
+  double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
+#define FINE_CASE(M) \
+  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps); break;
+  switch (mode) {
+    FINE_CASE(0) FINE_CASE(1) FINE_CASE(2) FINE_CASE(3) FINE_CASE(4) FINE_CASE(5) FINE_CASE(6) FINE_CASE(7)
+  }
+#undef FINE_CASE
+}
+
+void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *fdst, const Dims &d,
+                          const LaunchShape &s, int substep, double omega_c, double omega_f, cudaStream_t stream) {
+  // Hermite basis at tau = substep / GR, evaluated as the reference writes it
+  // (tinterpolate_hrmt.c:34); rescaling factor of ctfdtransfer_opt.c:101.
+  const double tmp = (((double)substep) / ((double)d.gr));
+  IfaceArgs ia;
+  ia.h1 = 2. * tmp * tmp * tmp - 3. * tmp * tmp + 1.;
+  ia.h2 = tmp * tmp * tmp - 2. * tmp * tmp + tmp;
+  ia.h3 = -2. * tmp * tmp * tmp + 3. * tmp * tmp;
+  ia.h4 = tmp * tmp * tmp - tmp * tmp;
+  ia.fac = omega_c / ((double)d.gr * omega_f);
+  dim3 grid(s.igx, s.igy, 2), block(ITX * ITY);
+  if (d.gr == 2)
+    interface_kernel<2><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
+  else if (d.gr == 3)
+    interface_kernel<3><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
+  else
+    interface_kernel<4><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
+}
+
+void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
+                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream) {
+  const double fac = d.gr * (omega_f / omega_c);
+  dim3 grid(s.jgx, s.jgy, 2), block(s.bx);
+  inject_kernel<<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
+}
+
+static FinArgs fin_args(const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp) {
+  FinArgs a;
+  a.nc = s.n_coarse_blocks() * d.nzc;
+  a.nf = s.n_fine_blocks() * 2 * d.zds;
+  a.ni = (long)s.jgx * s.jgy * 2;
+  a.wn = s.n_fine_blocks();
+  const int zds = d.zds, zdf = d.zdf;
+  const int planes[6] = {0, 1, 2, zds + zdf - 2, zds + zdf - 3, zds + zdf - 4};
+  for (int q = 0; q < 6; q++) a.wb[q] = (long)planes[q] * s.n_fine_blocks();
+  a.g3 = (double)d.gr * d.gr * d.gr;
+  a.norm = (double)((double)d.nxf * (double)d.nyf * (d.nzs - 2.));
+  a.norm2 = (double)d.nxf * (double)d.nyf;
+  a.mu = (1. / 6.) * (2. / sp.omega_f - 1);
+  a.ub = sp.ub;
+  a.gconst = sp.gconst;
+  a.pgrad_scale = (d.nzs - 2.) / (2. * d.gr);
+  a.flow_scale = (double)((long)d.nyf * (d.nzs - 2));
+  a.cfr = sp.cfr;
+  a.with_log = 1;
+  (void)pl;
+  return a;
+}
+
+void launch_finalize(DevState *st, DevLog *log_row, const double *partials, const PartialLayout &pl, const Dims &d,
+                     const LaunchShape &s, const StepParams &sp, cudaStream_t stream) {
+  FinArgs a = fin_args(pl, d, s, sp);
+  finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, log_row, partials + pl.coarse, partials + pl.fine,
+                                                 partials + pl.inject, partials + pl.wall, a);
+}
+
+void launch_stats_finalize(double *acc, const double *partials, const PartialLayout &pl, const Dims &d,
+                           const LaunchShape &s, cudaStream_t stream) {
+  StatsArgs a;
+  a.nzp = 2 * d.zdf + d.nzc - 4;
+  a.zdf = d.zdf;
+  a.nzc = d.nzc;
+  a.zds = d.zds;
+  a.bc = s.n_coarse_blocks();
+  a.bf = s.n_fine_blocks();
+  a.nc = (double)d.nx * d.ny;
+  a.nf = (double)d.nxf * d.nyf;
+  stats_finalize_kernel<<<a.nzp, 256, 0, stream>>>(acc, partials + pl.stats_c, partials + pl.stats_f, a);
+}
+
+void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,
+                          const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
+                          cudaStream_t stream) {
+  // coarse planes then fine planes; one pair per block into the coarse+fine partial areas
+  const int gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
+  const int nz = d.nzc + 2 * d.zds;
+  const long nblocks = (long)gx * gy * nz;
+  double *scratch = partials + pl.flow;
+  dim3 grid(gx, gy, nz), block(s.bx);
+  flow_sums_kernel<<<grid, block, 0, stream>>>(fc, ff, d, s.jb, d.nzc, scratch);
+  FinArgs a = fin_args(pl, d, s, sp);
+  a.nc = 0;
+  a.ni = 0;
+  a.nf = nblocks;
+  a.with_log = 0;
+  // the fine path of finalize sums with weight 1: the kernel already applied
+  // every encalc2 weight, so feed everything through the fine slot
+  finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, nullptr, scratch, scratch, scratch, scratch, a);
+}
+
+void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
+                     cudaStream_t stream) {
+  const int nxm = d.nxf > d.nx ? d.nxf : d.nx, nym = d.nyf > d.ny ? d.nyf : d.ny;
+  dim3 grid((nxm + 127) / 128, nym, d.nzc + 2 * d.zds), block(128);
+  seed_kernel<<<grid, block, 0, stream>>>(fc, ff, hist3, d, seed, uc, amp);
+}
+
+void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos, int k0_aos,
+                       cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  soa_to_aos_kernel<<<grid, block, 0, stream>>>(soa, aos, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, int p0, int np, int nz_aos, int k0_aos,
+                       cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  aos_to_soa_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+}  // namespace dns

@@ -1,0 +1,181 @@
+/*
+ * dns_embed.h — C ABI of the B200 grid-embedded D3Q19 channel solver.
+ *
+ * Drop-in for the time-step path of the reference solver
+ * (arstgr/DNS-solvers-with-grid-embedding, DNS-solver-with-grid-embedding/src/).
+ * The reference is one monolithic C/MPI program with no library API; its
+ * boundaries are the compile-time macros in src/definitions.h, the restart and
+ * output files, and the routines called by main's loop.  Each entry point below
+ * names the reference code it replaces.
+ *
+ * Conventions
+ *   - Every call returns an int status: DNS_OK (0) or a negative DNS_E* code.
+ *     Nothing crosses the ABI as an exception.  dns_error_string() describes a
+ *     code; dns_last_error() gives the message of the last failure on the
+ *     calling thread.
+ *   - A handle owns all device memory of one channel.  Caller buffers are only
+ *     borrowed for the duration of a call.  One host thread per handle.
+ *   - Populations use the reference's D3Q19 order (src/globals.c:6-8) and the
+ *     reference axes: x streamwise (i), y spanwise (j), z wall-normal (k).
+ *   - The reference stores the relaxation RATE in variables named tau*; here
+ *     omega_c / omega_f are rates (1 / relaxation time).
+ */
+#ifndef DNS_EMBED_H
+#define DNS_EMBED_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DNS_OK 0
+#define DNS_EINVAL (-1)   /* bad argument or unsupported parameter combination */
+#define DNS_ENOMEM (-2)   /* device or host allocation failed / over budget */
+#define DNS_EIO (-3)      /* restart or output file missing, short or unwritable */
+#define DNS_ENAN (-4)     /* non-finite wall shear stress (reference aborts) */
+#define DNS_ETIMEOUT (-5) /* a bounded device wait gave up */
+#define DNS_ECUDA (-6)    /* CUDA runtime error */
+
+enum dns_pattern { DNS_PATTERN_NONE = 0, DNS_PATTERN_RSLIP = 1, DNS_PATTERN_PSLIP = 2, DNS_PATTERN_SSLIP = 3 };
+enum dns_forcing { DNS_FORCING_CFR = 0, DNS_FORCING_CONST = 1 };
+enum dns_precision { DNS_FP64 = 0, DNS_FP32 = 1 };
+
+/* Solver parameters.  The first block mirrors the macros of the reference's
+   src/definitions.h:34-119 (same names, same meaning); XDIM/YDIM are accepted
+   and ignored because one GPU holds the whole domain.  The second block holds
+   run-time options that the reference sets by editing source. */
+typedef struct dns_params {
+  double Rebs;      /* bulk Reynolds number on the full height (definitions.h:34) */
+  double ub;        /* bulk velocity, lattice units (definitions.h:35) */
+  int zdv;          /* coarse wall-normal nodes incl. the two overlap planes (zdc) */
+  int ydv;          /* spanwise coarse nodes */
+  int xdv;          /* streamwise coarse nodes */
+  int TSTR, TEND;   /* start / end in unit times (log time stamps, file counters) */
+  double CFL;       /* sets utime, the number of coarse steps per unit time */
+  int gratio;       /* coarse / fine grid ratio GR (>= 2) */
+  int zds;          /* fine wall-normal nodes per block (zdf = zds + 1 incl. wall) */
+  int gyplussize, wyplussize, gxplussize, wxplussize; /* wall pattern, fine cells */
+  int pattern;      /* enum dns_pattern: RSLIP / PSLIP / SSLIP / none (definitions.h:69-71) */
+  int XDIM, YDIM;   /* reference rank grid; ignored */
+  long ITER;        /* fixed iteration count, < 0 when undefined (definitions.h:98) */
+  /* run-time options */
+  int forcing;          /* enum dns_forcing: constant flow rate (encalc2) or constant force */
+  double force_const;   /* coarse-unit body force g when forcing == DNS_FORCING_CONST */
+  int precision;        /* enum dns_precision */
+  int device;           /* CUDA device ordinal */
+} dns_params;
+
+/* Derived sizes; computed on the host, no GPU needed. */
+typedef struct dns_geometry {
+  int nx, ny, nzc;          /* coarse nodes (xdv, ydv, zdc) */
+  int nxf, nyf, zdf;        /* fine nodes per block: GR xdv, GR ydv, zds + 1 (wall incl.) */
+  int gr;                   /* grid ratio */
+  int nzs;                  /* NZs: wall-normal fine extent incl. the 2 wall nodes */
+  int nz_profile;           /* NZ of the composite statistics profile: 2 zdf + zdc - 4 */
+  int utime;                /* coarse steps per unit time */
+  double omega_c, omega_f;  /* relaxation rates as the reference computes them */
+  long long updates_per_step; /* xdv ydv zdc + 2 GR (GR xdv)(GR ydv) zds */
+  long long device_bytes;   /* HBM the handle allocates */
+} dns_geometry;
+
+/* One coarse step's log values, computed on the pre-step state S_n exactly as
+   the reference's encalc2.c:109-144 and wshearstr.c:67-166 define them. */
+typedef struct dns_step_log {
+  double time;      /* TM + dt * step, the reference's log time stamp */
+  double force;     /* force[0] used by this step */
+  double momentum;  /* normalised streamwise momentum (encalc2) */
+  double denst;     /* normalised mass (density.txt) */
+  double flowrate;  /* momentum (ydf-1)(NZs-2) / denst (flowrate.txt) */
+  double stup, stdown, stress, pgrad; /* str-up / str-do / w-str / p-grad */
+} dns_step_log;
+
+typedef struct dns_handle dns_handle;
+
+/* ---- parameters (host only) ------------------------------------------- */
+/* Reference defaults: src/definitions.h with XDIM = YDIM = 1, CFR forcing, FP64. */
+int dns_params_default(dns_params *p);
+/* Parse a reference-style definitions.h ("#define NAME value" lines and the
+   RSLIP/PSLIP/SSLIP/ITER switches), replacing src/definitions.h:34-119. */
+int dns_params_from_definitions(const char *path, dns_params *p);
+/* Sizes and rates of dns-q-mgrd-all-patterns-xyc.c:139-155,439-451. */
+int dns_geometry_of(const dns_params *p, dns_geometry *g);
+
+/* ---- lifecycle ------------------------------------------------------------ */
+/* Allocate one channel on p->device (replaces main's calloc block :473-883 and
+   the wall flags of solid_init.c + slip_*_init.c). */
+int dns_create(const dns_params *p, dns_handle **out);
+void dns_destroy(dns_handle *h);
+/* Launch subsequent work on this CUDA stream (cudaStream_t passed as void*);
+   NULL selects the handle's own stream. */
+int dns_set_stream(dns_handle *h, void *cuda_stream);
+int dns_get_geometry(const dns_handle *h, dns_geometry *g);
+
+/* ---- state ------------------------------------------------------------------ */
+/* Mode -p restart read: lbf-c, lbf-slf, lbf-suf, force, lbf-uin, lbf-lin with
+   counter cntr (dns-q-mgrd-all-patterns-xyc.c:999-1163). */
+int dns_load_restart(dns_handle *h, const char *dir, int cntr);
+/* Restart write in the same layout (:1262-1341). */
+int dns_write_restart(dns_handle *h, const char *dir, int cntr);
+/* Seeded start: rho = 1, laminar profile 4 uc zeta (1 - zeta) plus Philox4x32-10
+   uniform perturbations in [-amp, amp] per component, f = feq; interface
+   history [rho, u, 0...] on all three levels (the state inter_init.c builds).
+   Replaces mode -s (init.c), which starts from rest. */
+int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double amp);
+/* Post-stream state S in reference AoS order f[i][j][k][a] of the global domain:
+   level 0 coarse (xdv, ydv, zdc, 19), 1 lower fine, 2 upper fine
+   ((GR xdv), (GR ydv), zdf, 19).  out must hold that many doubles. */
+int dns_export_state(dns_handle *h, int level, double *aos_out);
+int dns_import_state(dns_handle *h, int level, const double *aos_in);
+/* Interface history [3 levels n,p,pp][2 walls lower,upper][xdv][ydv][23]. */
+int dns_export_history(dns_handle *h, double *out);
+/* Force the next step will use (encalc2 of the current state in CFR mode). */
+int dns_get_force(dns_handle *h, double *force);
+
+/* ---- the hot path ---------------------------------------------------------- */
+/* Advance ncoarse coarse steps: the body of main's loop
+   (dns-q-mgrd-all-patterns-xyc.c:1254-1375): encalc2, wshearstr, xcomputations,
+   GR x (xfcomputations, tinterpolate_hrmt, derivative, ctfdtransfer_opt),
+   ftcdtransfer, exchange/fexchange.  log (may be NULL) receives ncoarse rows.
+   Returns DNS_ENAN if a wall shear stress is not finite (the reference calls
+   MPI_Abort, wshearstr.c:139-143); the state is then left as computed. */
+int dns_step(dns_handle *h, long ncoarse, dns_step_log *log);
+
+/* ---- statistics ---------------------------------------------------------- */
+/* Every `every` coarse steps (0 = off) the pre-step state is sampled on the
+   device: per plane of the composite profile (statistics.c:48-146 plane order)
+   FP64 sums of u, v, w, rho and their second moments are accumulated. */
+int dns_set_sampling(dns_handle *h, long every);
+int dns_stats_reset(dns_handle *h);
+/* Accumulated profiles, out[DNS_NSTAT][nz_profile], samples in *nsamples:
+   0 z/H  1 <U>  2 <V>  3 <W>  4 <rho>   (time mean of plane means)
+   5 <u'u'>  6 <v'v'>  7 <w'w'>  8 <u'w'>  9 <rho'rho'>  (time mean of the
+     per-sample plane variances: the reference definition, statistics.c:147-292
+     with time_stat.c:161-200 averaging)
+   10 <u'u'>_t  11 <v'v'>_t  12 <w'w'>_t  13 <u'w'>_t  (fluctuations about the
+     time-and-plane mean). */
+#define DNS_NSTAT 14
+int dns_stats(dns_handle *h, double *out, long *nsamples);
+/* Instantaneous plane statistics of the current state, the 9 x NZ record of
+   turb-fld.000.TTT (statistics.c:303-316). */
+int dns_plane_stats(dns_handle *h, double *out9xnz);
+
+/* ---- measurement ----------------------------------------------------------- */
+/* Per-kernel device time, measured with CUDA events recorded on the handle's
+   stream around every launch while profiling is on (no reference counterpart;
+   the reference times only the whole loop, main :1252/:1377).  Classes:
+   0 coarse stream-collide, 1 interface extraction, 2 fine stream-collide,
+   3 coarse-to-fine interface, 4 fine-to-coarse injection, 5 reduction finalize,
+   6 statistics finalize.  Times accumulate until profiling is switched on again. */
+#define DNS_NKERNEL 7
+int dns_set_profiling(dns_handle *h, int on);
+int dns_kernel_times(dns_handle *h, double *ms, long *launches);
+
+/* ---- errors -------------------------------------------------------------- */
+const char *dns_error_string(int code);
+const char *dns_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DNS_EMBED_H */

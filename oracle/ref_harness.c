@@ -23,6 +23,8 @@
  * [n | p | pp] interface history (i, j, 23); force holds force[0].
  *
  * usage: ref_harness INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY]
+ * (INDIR "-" starts from rest instead of reading restart files; CNTR_OUT < 0
+ *  skips the restart output, for timing)
  * The step loop time (MPI_Wtime, as main's t2-t4) is printed as
  *   "harness_seconds <s>".
  */
@@ -219,6 +221,8 @@ int main(int argc, char **argv) {
            V.sudwbufr, V.suupbufr, V.suurbufs, V.sudlbufr, V.sudlbufs, V.suurbufr, ydf, xdf, zdf)
 
   char fn[4096];
+  int cold = strcmp(indir, "-") == 0;
+  if (cold) goto cold_start;
   snprintf(fn, sizeof fn, "%s/lbf-c.%.4d", indir, cin);
   read_lattice(fn, V.ftemp, V.f, xdc - 1, ydc - 1, zdc);
   snprintf(fn, sizeof fn, "%s/lbf-slf.%.4d", indir, cin);
@@ -236,6 +240,7 @@ int main(int argc, char **argv) {
   snprintf(fn, sizeof fn, "%s/lbf-lin.%.4d", indir, cin);
   read_history(fn, V.lin, V.linp, V.linpp, xdc, ydc);
 
+cold_start:
   V = solid_init(xdc, ydc, zdc, xdf, ydf, zdf, V);
 #ifdef RSLIP
   V = slip_ridges_init(xdf, ydf, zdf, V, pd);
@@ -247,6 +252,17 @@ int main(int argc, char **argv) {
   V = slip_spanwise_init(xdf, ydf, zdf, V, pd);
 #endif
 
+  if (cold) {
+    /* INDIR "-": the reference's own cold start (mode -s, init.c: f = w at
+       every non-solid node) with the interface history set to that state's
+       [rho, u, fneq] = [1, 0, 0, 0, 0...] on all three levels */
+    V = init(xdc, ydc, zdc, xdf, ydf, zdf, V);
+    DP *lv[6] = {V.lin, V.linp, V.linpp, V.uin, V.uinp, V.uinpp};
+    for (int q = 0; q < 6; q++)
+      for (int i = -2; i < xdc + 3; i++)
+        for (int j = -2; j < ydc + 3; j++) Fbi(lv[q], i, j, 0, 0, xdc, ydc, 4, 23) = 1.0;
+    V.force[0] = gconst;
+  }
   if (chdir(outdir) != 0) die("cannot enter", outdir);
   int TM = cin;
   DP Gx = 0.;
@@ -278,6 +294,10 @@ int main(int argc, char **argv) {
   double t2 = MPI_Wtime();
   printf("harness_seconds %.9f\n", t2 - t4);
 
+  if (cout < 0) { /* timing run: no restart output */
+    MPI_Finalize();
+    return 0;
+  }
   /* main writes a restart at the top of an iteration, after encalc2 has set the
      force for the state it is about to write (:1256-1306); do the same */
   V = encalc2(xdc, ydc, zdc, xdf, ydf, zdf, GR, V, pd, TM, nsteps, ubulk);

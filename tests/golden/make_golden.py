@@ -1,0 +1,78 @@
+"""Generate the golden fixtures of the oracle from the compiled reference.
+
+For each case: write the seeded initial state (oracle restatement) as restart
+files, run the reference's own routines (``oracle/_ref/<config>/ref_harness``,
+compiled from the mounted reference sources) for N coarse steps, and record
+SHA-256 digests of the post-stream lattices and interface histories it writes,
+plus a few sampled values and the logged flow rate.  The tests check the CPU
+restatement against these digests on machines where the reference tree is not
+mounted.
+
+Run from the repository root: ``python tests/golden/make_golden.py``.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import subprocess
+import sys
+import tempfile
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parents[2]
+sys.path.insert(0, str(ROOT / "oracle"))
+
+import port  # noqa: E402
+from ref_configs import REF_CONFIGS  # noqa: E402
+
+CASES = [
+    ("t_noslip", "const", 20), ("t_noslip", "cfr", 20), ("t_ridges", "cfr", 20), ("t_posts", "const", 20),
+    ("t_span", "cfr", 20), ("t_gr4", "cfr", 10), ("t_odd", "const", 20),
+]
+SEED, UC, AMP, GCONST = 42, 0.05, 0.005, 1.0e-5
+
+
+def digest(a: np.ndarray) -> str:
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
+
+
+def run_case(name, mode, n):
+    m = REF_CONFIGS[name]
+    p = port.Port(m)
+    g = GCONST if mode == "const" else 0.0
+    p.init_seeded(SEED, UC, AMP, g)
+    p.set_forcing(mode == "cfr", g)
+    with tempfile.TemporaryDirectory() as d:
+        din, dout = Path(d, "in"), Path(d, "out")
+        din.mkdir()
+        dout.mkdir()
+        p.save(din, 100)
+        exe = ROOT / "oracle" / "_ref" / name / "ref_harness"
+        subprocess.run([str(exe), str(din), "100", str(dout), "101", str(n), mode, g.hex()], check=True,
+                       capture_output=True)
+        nx, ny, zdc, nxf, nyf, zdf = p.nx, p.ny, p.zdc, p.nxf, p.nyf, p.zdf
+        out = {"config": name, "mode": mode, "steps": n, "seed": SEED, "uc": UC, "amp": AMP, "g": g}
+        shapes = {"lbf-c": (nx, ny, zdc, 19), "lbf-slf": (nxf, nyf, zdf, 19), "lbf-suf": (nxf, nyf, zdf, 19)}
+        for fn, sh in shapes.items():
+            a = np.fromfile(dout / f"{fn}.0101")
+            s = a[: a.size // 2].reshape(sh)
+            out[fn] = {"sha256": digest(s), "sum": float(s.sum()), "sample": [float(x) for x in s.reshape(-1)[::997][:16]]}
+        for w in ("lin", "uin"):
+            h = np.fromfile(dout / f"lbf-{w}.0101").reshape(3, nx, ny, 23)
+            out[f"lbf-{w}"] = {"sha256": digest(h)}
+        out["force_next"] = float(np.fromfile(dout / "force.0101")[0])
+        fl = np.loadtxt(dout / "flowrate.txt")
+        out["flowrate_log"] = [float(x) for x in np.atleast_2d(fl)[:, 1]]
+    return out
+
+
+def main():
+    cases = [run_case(*c) for c in CASES]
+    (Path(__file__).parent / "oracle_golden.json").write_text(json.dumps(cases, indent=1))
+    print(f"wrote {len(cases)} cases")
+
+
+if __name__ == "__main__":
+    main()

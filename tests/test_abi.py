@@ -1,0 +1,99 @@
+"""C ABI surface and host-only logic (no GPU calls)."""
+from __future__ import annotations
+
+import ctypes as C
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+HEADER = ROOT / "include" / "dns_embed.h"
+
+
+def declared_symbols():
+    txt = HEADER.read_text()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(dns_\w+)\s*\(", txt, re.M)))
+
+
+def test_library_exports_every_declared_symbol(pkg):
+    lib = pkg.lib()
+    syms = declared_symbols()
+    assert len(syms) >= 20
+    out = subprocess.run(["nm", "-D", "--defined-only", str(pkg.LIBPATH)], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (dns_\w+)", out))
+    missing = [s for s in syms if s not in exported]
+    assert not missing, missing
+    for s in syms:
+        assert getattr(lib, s) is not None
+
+
+def test_defaults_mirror_reference_definitions(pkg):
+    p = pkg.default_params()
+    assert (p.xdv, p.ydv, p.zdv, p.zds, p.gratio) == (512, 256, 220, 10, 4)
+    assert p.Rebs == 7200.0 and p.ub == 0.0866034 and p.CFL == 0.1
+    assert p.pattern == pkg.PATTERN_RSLIP and p.ITER < 0
+
+
+def test_params_from_definitions_file(pkg, tmp_path):
+    src = tmp_path / "definitions.h"
+    src.write_text("""
+#define Rebs 5533.0
+#define ub 0.0866034
+#define zdv  83
+#define ydv  128
+#define xdv  256
+#define gratio 2
+#define zds 16
+#define gyplussize 24
+#define wyplussize 24
+//#define PSLIP
+#define RSLIP
+//#define SSLIP
+#define XDIM 4
+#define YDIM 2
+//#define ITER 1
+""")
+    p = pkg.params_from_definitions(src)
+    assert (p.xdv, p.ydv, p.zdv, p.zds, p.gratio) == (256, 128, 83, 16, 2)
+    assert p.pattern == pkg.PATTERN_RSLIP and p.ITER < 0 and p.Rebs == 5533.0
+    with pytest.raises(pkg.DnsError) as e:
+        pkg.params_from_definitions(tmp_path / "missing.h")
+    assert e.value.code == pkg.DNS_EIO
+
+
+def test_geometry_matches_reference_formulas(pkg, port, ref_configs):
+    for name in ("t_noslip", "t_gr4", "c1", "c2"):
+        m = ref_configs[name]
+        p = pkg.make_params(xdv=m["xdv"], ydv=m["ydv"], zdv=m["zdv"], zds=m["zds"], gratio=m["gratio"],
+                            Rebs=float(m["Rebs"]), ub=m["ub"], CFL=m["CFL"], pattern=m.get("pattern"))
+        g = pkg.geometry(p)
+        q = port.Port(m)
+        oc, of, nzs = q.params()
+        assert g.nzs == nzs and g.omega_c == oc and g.omega_f == of
+        gr = m["gratio"]
+        assert g.updates_per_step == m["xdv"] * m["ydv"] * m["zdv"] + 2 * gr * (gr * m["xdv"]) * (gr * m["ydv"]) * m["zds"]
+    # config 1 / 2 work units quoted by the survey
+    p1 = pkg.make_params(xdv=64, ydv=64, zdv=27, zds=8, gratio=2)
+    assert pkg.geometry(p1).updates_per_step == 634880
+    p2 = pkg.make_params(xdv=256, ydv=128, zdv=83, zds=16, gratio=2)
+    assert pkg.geometry(p2).updates_per_step == 11108352
+
+
+@pytest.mark.parametrize("bad", [dict(gratio=1), dict(zds=2), dict(zdv=3), dict(xdv=2), dict(Rebs=-1.0),
+                                 dict(pattern=9), dict(precision=7)])
+def test_invalid_parameters_are_rejected(pkg, bad):
+    p = pkg.make_params(xdv=16, ydv=16, zdv=9, zds=6, gratio=2)
+    for k, v in bad.items():
+        setattr(p, k, v)
+    with pytest.raises(pkg.DnsError) as e:
+        pkg.geometry(p)
+    assert e.value.code == pkg.DNS_EINVAL
+
+
+def test_error_strings(pkg):
+    lib = pkg.lib()
+    for code in (0, -1, -2, -3, -4, -5, -6):
+        assert lib.dns_error_string(code)

@@ -1,0 +1,163 @@
+"""The oracle against the reference: known answers, golden fixtures, and the
+compiled reference itself (CPU only)."""
+from __future__ import annotations
+
+import hashlib
+import json
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, ref_binary
+
+GOLDEN = json.loads((ROOT / "tests" / "golden" / "oracle_golden.json").read_text())
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype="<f8").tobytes()).hexdigest()
+
+
+def test_philox_known_answers(port):
+    # Random123 known-answer vectors for Philox4x32-10 (Salmon et al. 2011)
+    assert port.philox((0, 0, 0, 0), (0, 0)) == (0x6627E8D5, 0xE169C58D, 0xBC57AC4C, 0x9B00DBD8)
+    assert port.philox((0xFFFFFFFF,) * 4, (0xFFFFFFFF,) * 2) == (0x408F276D, 0x41C83B0E, 0xA20BC7C6, 0x6D5451FD)
+    assert port.philox((0x243F6A88, 0x85A308D3, 0x13198A2E, 0x03707344), (0xA4093822, 0x299F31D0)) == (
+        0xD16CFE09, 0x94FDCCEB, 0x5001E420, 0x24126EA1)
+
+
+def test_bicubic_weights_reproduce_cubics():
+    """The generated coefficient map must interpolate any bicubic exactly."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location(
+        "gen_bicubic", ROOT / "dns-solvers-with-grid-embedding_b200" / "csrc" / "gen_bicubic.py")
+    gb = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gb)
+    W = np.array(gb.weights(), dtype=float)
+    rng = np.random.default_rng(1)
+    c = rng.normal(size=(4, 4))  # p(t,u) = sum c[n,m] t^n u^m
+    corners = [(0, 0), (1, 0), (1, 1), (0, 1)]
+
+    def ev(t, u, dn, dm):
+        s = 0.0
+        for n in range(4):
+            for m in range(4):
+                if n < dn or m < dm:
+                    continue
+                f = (n if dn else 1) * (m if dm else 1)
+                s += c[n, m] * f * t ** (n - dn) * u ** (m - dm)
+        return s
+
+    x = [ev(t, u, dn, dm) for (dn, dm) in ((0, 0), (1, 0), (0, 1), (1, 1)) for (t, u) in corners]
+    np.testing.assert_allclose(W @ np.array(x), c.reshape(-1), atol=1e-12)
+
+
+@pytest.mark.parametrize("case", GOLDEN, ids=lambda c: f"{c['config']}-{c['mode']}")
+def test_port_matches_golden(port, ref_configs, case):
+    """CPU restatement reproduces the reference's own output bit for bit."""
+    p = port.Port(ref_configs[case["config"]])
+    p.init_seeded(case["seed"], case["uc"], case["amp"], case["g"])
+    p.set_forcing(case["mode"] == "cfr", case["g"])
+    log = p.step(case["steps"])
+    for lvl, fn in enumerate(("lbf-c", "lbf-slf", "lbf-suf")):
+        assert _digest(p.export(lvl)) == case[fn]["sha256"], fn
+    h = p.history()
+    assert _digest(h[:, 0]) == case["lbf-lin"]["sha256"]
+    assert _digest(h[:, 1]) == case["lbf-uin"]["sha256"]
+    assert p.force() == case["force_next"]
+    # the reference logs with %.12f
+    np.testing.assert_allclose(log[:, 3], case["flowrate_log"][: case["steps"]], atol=6e-13, rtol=0)
+
+
+@pytest.mark.parametrize("name,mode,steps", [("t_noslip", "cfr", 12), ("t_posts", "cfr", 12),
+                                             ("t_gr4", "const", 6), ("t_odd", "cfr", 12)])
+def test_port_matches_compiled_reference(port, ref_configs, tmp_path, name, mode, steps):
+    exe = ref_binary(name)
+    if exe is None:
+        pytest.skip("compiled reference not available (reference tree not mounted)")
+    p = port.Port(ref_configs[name])
+    g = 2.0e-5 if mode == "const" else 0.0
+    p.init_seeded(7, 0.04, 0.01, g)
+    p.set_forcing(mode == "cfr", g)
+    din, dout = tmp_path / "in", tmp_path / "out"
+    din.mkdir()
+    dout.mkdir()
+    p.save(din, 3)
+    subprocess.run([str(exe), str(din), "3", str(dout), "4", str(steps), mode, g.hex()], check=True,
+                   capture_output=True)
+    p.step(steps)
+    for lvl, fn in enumerate(("lbf-c", "lbf-slf", "lbf-suf")):
+        a = np.fromfile(dout / f"{fn}.0004")
+        np.testing.assert_array_equal(p.export(lvl).reshape(-1), a[: a.size // 2])
+    h = p.history()
+    for w, fn in enumerate(("lbf-lin", "lbf-uin")):
+        np.testing.assert_array_equal(h[:, w].reshape(-1), np.fromfile(dout / f"{fn}.0004"))
+
+
+@pytest.mark.parametrize("name", ["t_noslip", "t_ridges"])
+def test_port_matches_reference_main(port, ref_configs, tmp_path, name):
+    """Pin against the unmodified reference main program (mode -p, ITER = 50,
+    one unit time per step): its restart written at step 50, and its
+    instantaneous plane statistics file at that step."""
+    exe = ref_binary(name, "ref_main")
+    if exe is None:
+        pytest.skip("compiled reference main not available")
+    p = port.Port(ref_configs[name])
+    p.init_seeded(42, 0.05, 0.005, 0.0)
+    p.set_forcing(True)
+    p.save(tmp_path, 100)
+    subprocess.run([str(exe), "-p"], cwd=tmp_path, check=True, capture_output=True)
+    p.step(50)
+    for lvl, fn in enumerate(("lbf-c", "lbf-slf", "lbf-suf")):
+        a = np.fromfile(tmp_path / f"{fn}.0150")
+        np.testing.assert_array_equal(p.export(lvl).reshape(-1), a[: a.size // 2])
+    h = p.history()
+    for w, fn in enumerate(("lbf-lin", "lbf-uin")):
+        np.testing.assert_array_equal(h[:, w].reshape(-1), np.fromfile(tmp_path / f"{fn}.0150"))
+    assert p.force() == np.fromfile(tmp_path / "force.0150")[0]
+    st = np.fromfile(tmp_path / "turb-fld.000.150").reshape(9, -1)
+    np.testing.assert_array_equal(p.plane_stats(), st)
+
+
+def test_port_restart_roundtrip(port, ref_configs, tmp_path):
+    a = port.Port(ref_configs["t_ridges"])
+    a.init_seeded(3, 0.05, 0.005, 0.0)
+    a.set_forcing(True)
+    a.step(5)
+    a.save(tmp_path, 9)
+    b = port.Port(ref_configs["t_ridges"])
+    b.load(tmp_path, 9)
+    b.set_forcing(True)
+    a.step(5)
+    b.step(5)
+    for lvl in range(3):
+        np.testing.assert_array_equal(a.export(lvl), b.export(lvl))
+
+
+def test_laminar_profile_known_answer(port, ref_configs):
+    """Laminar known answer of the reference (statistics.c:331-335): a
+    constant-flow-rate run from the exact parabola stays on it."""
+    m = dict(ref_configs["t_noslip"])
+    p = port.Port(m)
+    ub = m["ub"]
+    p.init_seeded(1, 1.5 * ub, 0.0, 0.0)  # centreline 1.5 ub, no perturbation
+    p.set_forcing(True)
+    p.step(200)
+    st = p.plane_stats()
+    nz = st.shape[1]
+    _, _, nzs = p.params()
+    H = nzs - 2.0
+    zdf, zdc, gr = p.zdf, p.zdc, m["gratio"]
+    z = np.zeros(nz)
+    for k in range(1, zdf):
+        z[k] = k - 0.5
+    for k in range(2, zdc - 2):
+        z[zdf - 2 + k] = gr * (k - 1) + (zdf - 1 - 0.5)
+    for k in range(0, zdf - 1):
+        z[zdf + zdc - 4 + k] = k + gr * (zdc - 3) + zdf - 1.0 - 0.5
+    zeta = z / H
+    exact = 6.0 * ub * zeta * (1.0 - zeta)
+    used = slice(1, nz - 1)
+    assert np.max(np.abs(st[0, used] - exact[used])) < 0.05 * ub
