@@ -35,7 +35,7 @@ int fail(int code, const std::string &msg) {
   } while (0)
 
 constexpr int kLogCap = 1024;
-constexpr int kProfSteps = 32;  // steps per chunk while profiling (bounds the event pool)
+constexpr int kProfSteps = 256;  // steps per chunk while profiling (bounds the event pool)
 
 // CUDA-event timing of every launch (dns_set_profiling)
 struct Profiler {
@@ -554,7 +554,22 @@ extern "C" int dns_load_restart(dns_handle *h, const char *dir, int cntr) {
   if ((rc = import_history(h, hist.data()))) return rc;
   h->ss = 0;
   h->tm = cntr;
-  return refresh_flow(h, h->p.forcing == DNS_FORCING_CFR ? force : h->p.force_const);
+  if ((rc = refresh_flow(h, h->p.forcing == DNS_FORCING_CFR ? force : h->p.force_const))) return rc;
+  if (h->p.forcing == DNS_FORCING_CFR) {
+    // The reference recomputes the force with encalc2 at the top of its loop;
+    // a restart it (or this solver) wrote holds that same value, up to the
+    // association of the domain sum.  When the file agrees to rounding, keep
+    // the file's bits so a resumed run continues exactly.
+    DevState st;
+    CUDA_TRY(cudaMemcpyAsync(&st, h->state, sizeof st, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (std::fabs(st.force - force) <= 1e-13 * h->p.ub) {
+      st.force = force;
+      CUDA_TRY(cudaMemcpyAsync(h->state, &st, sizeof st, cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(cudaStreamSynchronize(h->stream));
+    }
+  }
+  return DNS_OK;
 }
 
 static int write_file(const std::string &fn, const double *a, size_t n, int copies) {

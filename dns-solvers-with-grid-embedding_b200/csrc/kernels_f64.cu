@@ -25,7 +25,11 @@ namespace {
 
 constexpr int kMaxThreads = 128;
 
-__device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? v + n : (v >= n ? v - n : v); }
+// periodic index for any offset (an interface tile can be wider than the domain)
+__device__ __forceinline__ int wrapi(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
 
 // Fixed-order block reduction of N doubles; thread 0 returns the sums.
 template <int N>
@@ -233,15 +237,78 @@ struct IfaceArgs {
   double h1, h2, h3, h4, fac;
 };
 
+struct IfaceSmem {
+  double V[PY][PX];
+  double Dy[ITY + 1][PX];
+  double Dx[ITY + 1][ITX + 1];
+  double Dxy[ITY + 1][ITX + 1];
+};
+
+// Stage field `fo` (offset of one wall's field in the history slots) of the
+// tile's periodic patch: Hermite value, then d/dy, d/dx, d2/dxdy.
+__device__ __forceinline__ void iface_stage(IfaceSmem &S, const double *__restrict__ hn,
+                                            const double *__restrict__ hp, const double *__restrict__ hpp,
+                                            size_t fo, int i0, int j0, int nx, int ny, const IfaceArgs &ia) {
+  const double c2o3 = 2. / 3., c1o12 = 1. / 12.;
+  for (int q = threadIdx.x; q < PX * PY; q += blockDim.x) {
+    const int pi = q % PX, pj = q / PX;
+    const int gi = wrapi(i0 - 2 + pi, nx), gj = wrapi(j0 - 2 + pj, ny);
+    const size_t g = fo + (size_t)gj * nx + gi;
+    const double n = hn[g], pv = hp[g], pp = hpp[g];
+    const double c1 = pv;
+    const double c2 = (n - pp) * 0.5;
+    const double c3 = n;
+    const double c4 = (3. * n - 4. * pv + pp) * 0.5;
+    S.V[pj][pi] = ia.h1 * c1 + ia.h2 * c2 + ia.h3 * c3 + ia.h4 * c4;
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < PX * (ITY + 1); q += blockDim.x) {
+    const int pi = q % PX, r = q / PX, pj = r + 2;
+    S.Dy[r][pi] = c2o3 * (S.V[pj + 1][pi] - S.V[pj - 1][pi]) - c1o12 * (S.V[pj + 2][pi] - S.V[pj - 2][pi]);
+    if (pi >= 2 && pi < ITX + 3)
+      S.Dx[r][pi - 2] = c2o3 * (S.V[pj][pi + 1] - S.V[pj][pi - 1]) - c1o12 * (S.V[pj][pi + 2] - S.V[pj][pi - 2]);
+  }
+  __syncthreads();
+  for (int q = threadIdx.x; q < (ITX + 1) * (ITY + 1); q += blockDim.x) {
+    const int c = q % (ITX + 1), r = q / (ITX + 1), pi = c + 2;
+    S.Dxy[r][c] = c2o3 * (S.Dy[r][pi + 1] - S.Dy[r][pi - 1]) - c1o12 * (S.Dy[r][pi + 2] - S.Dy[r][pi - 2]);
+  }
+  __syncthreads();
+}
+
+// Bicubic coefficients of cell (tx, ty) of the staged field.
+__device__ __forceinline__ void iface_coeffs(const IfaceSmem &S, int tx, int ty, double (&cf)[16]) {
+  double x[16];
+  const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 0, 1, 1};
+#pragma unroll
+  for (int q = 0; q < 4; q++) {
+    const int c = tx + ci[q], r = ty + cj[q];
+    x[q] = S.V[r + 2][c + 2];
+    x[4 + q] = S.Dx[r][c];
+    x[8 + q] = S.Dy[r][c + 2];
+    x[12 + q] = S.Dxy[r][c];
+  }
+  DNS_BICUBIC_COEFFS(cf, x);
+}
+
+// Horner evaluation at (t, u) = (ii/GR, jj/GR), ctfdtransfer_opt.c:62-97 order.
+template <int GR>
+__device__ __forceinline__ double iface_eval(const double (&cf)[16], int ii, int jj) {
+  const double tt = ((double)ii) / ((double)GR);
+  const double uu = ((double)jj) / ((double)GR);
+  double val = 0.;
+#pragma unroll
+  for (int nn = 3; nn > -1; nn--)
+    val = tt * val + ((cf[nn * 4 + 3] * uu + cf[nn * 4 + 2]) * uu + cf[nn * 4 + 1]) * uu + cf[nn * 4 + 0];
+  return val;
+}
+
 template <int GR>
 __global__ void __launch_bounds__(ITX *ITY) interface_kernel(const double *__restrict__ hn,
                                                              const double *__restrict__ hp,
                                                              const double *__restrict__ hpp,
                                                              double *__restrict__ fdst, Dims d, IfaceArgs ia) {
-  __shared__ double V[PY][PX];
-  __shared__ double Dy[ITY + 1][PX];
-  __shared__ double Dx[ITY + 1][ITX + 1];
-  __shared__ double Dxy[ITY + 1][ITX + 1];
+  __shared__ IfaceSmem S;
   const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf, zds = d.zds;
   const int w = blockIdx.z;
   const int i0 = blockIdx.x * ITX, j0 = blockIdx.y * ITY;
@@ -252,71 +319,47 @@ __global__ void __launch_bounds__(ITX *ITY) interface_kernel(const double *__res
   const int pf = w == 0 ? zds - 1 : zds;  // interface plane of the fine block
   const size_t fstride = (size_t)2 * zds * nyf * nxf;
   constexpr int NN = GR * GR;
-  double rho[NN], ua[NN], ub[NN], uc[NN], t15v[NN];
-  const double c2o3 = 2. / 3., c1o12 = 1. / 12.;
-  for (int b = 0; b < 23; b++) {
-    const size_t fo = ((size_t)w * 23 + b) * plane;
-    for (int q = threadIdx.x; q < PX * PY; q += blockDim.x) {
-      const int pi = q % PX, pj = q / PX;
-      const int gi = wrapi(i0 - 2 + pi, nx), gj = wrapi(j0 - 2 + pj, ny);
-      const size_t g = fo + (size_t)gj * nx + gi;
-      const double n = hn[g], pv = hp[g], pp = hpp[g];
-      const double c1 = pv;
-      const double c2 = (n - pp) * 0.5;
-      const double c3 = n;
-      const double c4 = (3. * n - 4. * pv + pp) * 0.5;
-      V[pj][pi] = ia.h1 * c1 + ia.h2 * c2 + ia.h3 * c3 + ia.h4 * c4;
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < PX * (ITY + 1); q += blockDim.x) {
-      const int pi = q % PX, r = q / PX, pj = r + 2;
-      Dy[r][pi] = c2o3 * (V[pj + 1][pi] - V[pj - 1][pi]) - c1o12 * (V[pj + 2][pi] - V[pj - 2][pi]);
-      if (pi >= 2 && pi < ITX + 3)
-        Dx[r][pi - 2] = c2o3 * (V[pj][pi + 1] - V[pj][pi - 1]) - c1o12 * (V[pj][pi + 2] - V[pj][pi - 2]);
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < (ITX + 1) * (ITY + 1); q += blockDim.x) {
-      const int c = q % (ITX + 1), r = q / (ITX + 1), pi = c + 2;
-      Dxy[r][c] = c2o3 * (Dy[r][pi + 1] - Dy[r][pi - 1]) - c1o12 * (Dy[r][pi + 2] - Dy[r][pi - 2]);
-    }
-    __syncthreads();
-    if (valid) {
-      double x[16], cf[16];
-      const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 0, 1, 1};
+  // macroscopic fields rho, ux, uy, uz at the GR x GR fine nodes of this cell
+  double mac[4][NN];
 #pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int c = tx + ci[q], r = ty + cj[q];
-        x[q] = V[r + 2][c + 2];
-        x[4 + q] = Dx[r][c];
-        x[8 + q] = Dy[r][c + 2];
-        x[12 + q] = Dxy[r][c];
-      }
-      DNS_BICUBIC_COEFFS(cf, x);
+  for (int b = 0; b < 4; b++)
+#pragma unroll
+    for (int q = 0; q < NN; q++) mac[b][q] = 0.;
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + b) * plane, i0, j0, nx, ny, ia);
+    if (valid) {
+      double cf[16];
+      iface_coeffs(S, tx, ty, cf);
+#pragma unroll
+      for (int ii = 0; ii < GR; ii++)
+#pragma unroll
+        for (int jj = 0; jj < GR; jj++) mac[b][ii * GR + jj] = iface_eval<GR>(cf, ii, jj);
+    }
+    __syncthreads();
+  }
+  double t15v[NN];
+#pragma unroll
+  for (int q = 0; q < NN; q++)
+    t15v[q] = 1.5 * (mac[1][q] * mac[1][q] + mac[2][q] * mac[2][q] + mac[3][q] * mac[3][q]);
+  // populations: feq(rho, u) + omega_c / (GR omega_f) fneq
+#pragma unroll 1
+  for (int a = 0; a < 19; a++) {
+    iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + 4 + a) * plane, i0, j0, nx, ny, ia);
+    if (valid) {
+      double cf[16];
+      iface_coeffs(S, tx, ty, cf);
+      const int cls = a == 0 ? 0 : (a <= 6 ? 1 : 2);
+      const double wa = cls == 0 ? 1. / 3. : (cls == 1 ? 1. / 18. : 1. / 36.);
 #pragma unroll
       for (int ii = 0; ii < GR; ii++)
 #pragma unroll
         for (int jj = 0; jj < GR; jj++) {
-          const double tt = ((double)ii) / ((double)GR);
-          const double uu = ((double)jj) / ((double)GR);
-          double val = 0.;
-#pragma unroll
-          for (int nn = 3; nn > -1; nn--)
-            val = tt * val + ((cf[nn * 4 + 3] * uu + cf[nn * 4 + 2]) * uu + cf[nn * 4 + 1]) * uu + cf[nn * 4 + 0];
-          const int node = ii * GR + jj;
-          if (b == 0) rho[node] = val;
-          else if (b == 1) ua[node] = val;
-          else if (b == 2) ub[node] = val;
-          else if (b == 3) {
-            uc[node] = val;
-            t15v[node] = 1.5 * (ua[node] * ua[node] + ub[node] * ub[node] + uc[node] * uc[node]);
-          } else {
-            const int a = b - 4;
-            const int cls = a == 0 ? 0 : (a <= 6 ? 1 : 2);
-            const double wra = (cls == 0 ? 1. / 3. : (cls == 1 ? 1. / 18. : 1. / 36.)) * rho[node];
-            const double feq = feq_f64(wra, proj_f64(a, ua[node], ub[node], uc[node]), t15v[node]);
-            const int fi = ic * GR + ii, fj = jc * GR + jj;
-            fdst[(size_t)a * fstride + ((size_t)pf * nyf + fj) * nxf + fi] = feq + ia.fac * val;
-          }
+          const int q = ii * GR + jj;
+          const double val = iface_eval<GR>(cf, ii, jj);
+          const double feq = feq_f64(wa * mac[0][q], proj_f64(a, mac[1][q], mac[2][q], mac[3][q]), t15v[q]);
+          const int fi = ic * GR + ii, fj = jc * GR + jj;
+          fdst[(size_t)a * fstride + ((size_t)pf * nyf + fj) * nxf + fi] = feq + ia.fac * val;
         }
     }
     __syncthreads();
