@@ -22,6 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INC
 UNITS = {  # source -> extra flags
     "kernels_f64.cu": ["-fmad=false"],
     "dns_api.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -850,3 +850,5 @@ extern "C" const char *dns_error_string(int code) {
 }
 
 extern "C" const char *dns_last_error(void) { return g_last_error.c_str(); }
+
+void dns::set_last_error(const std::string &msg) { g_last_error = msg; }

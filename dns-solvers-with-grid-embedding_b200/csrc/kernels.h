@@ -3,6 +3,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <string>
 
 #include <cuda_runtime.h>
 
@@ -41,6 +42,9 @@ struct LaunchShape {
 
 LaunchShape make_shape(const Dims &d);
 
+// record a message for dns_last_error() on the calling thread (dns_api.cu)
+void set_last_error(const std::string &msg);
+
 // Reduction scratch sizes (doubles) for a given shape.
 struct PartialLayout {
   long coarse, fine, inject, wall, stats_c, stats_f, flow;  // offsets into one buffer
@@ -77,6 +81,11 @@ void launch_stats_finalize(double *acc, const double *partials, const PartialLay
 void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,
                           const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
                           cudaStream_t stream);
+// the same reduction over a caller-held state, with caller-provided block scratch
+// (scratch_pairs = flow_sums_pairs(d, s) pairs of doubles), result into *out
+long flow_sums_pairs(const Dims &d, const LaunchShape &s);
+void launch_flow_sums_scratch(const double *fc, const double *ff, DevState *out, double *scratch, const Dims &d,
+                              const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
 void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
                      cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order

@@ -827,6 +827,25 @@ void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, doub
   finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, nullptr, scratch, scratch, scratch, scratch, a);
 }
 
+long flow_sums_pairs(const Dims &d, const LaunchShape &s) {
+  const long gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
+  return gx * gy * (d.nzc + 2 * d.zds);
+}
+
+void launch_flow_sums_scratch(const double *fc, const double *ff, DevState *out, double *scratch, const Dims &d,
+                              const LaunchShape &s, const StepParams &sp, cudaStream_t stream) {
+  const int gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
+  dim3 grid(gx, gy, d.nzc + 2 * d.zds), block(s.bx);
+  flow_sums_kernel<<<grid, block, 0, stream>>>(fc, ff, d, s.jb, d.nzc, scratch);
+  PartialLayout unused{};
+  FinArgs a = fin_args(unused, d, s, sp);
+  a.nc = 0;
+  a.ni = 0;
+  a.nf = flow_sums_pairs(d, s);
+  a.with_log = 0;
+  finalize_kernel<<<1, kFinThreads, 0, stream>>>(out, nullptr, scratch, scratch, scratch, scratch, a);
+}
+
 void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
                      cudaStream_t stream) {
   const int nxm = d.nxf > d.nx ? d.nxf : d.nx, nym = d.nyf > d.ny ? d.nyf : d.ny;

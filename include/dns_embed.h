@@ -171,6 +171,25 @@ int dns_plane_stats(dns_handle *h, double *out9xnz);
 int dns_set_profiling(dns_handle *h, int on);
 int dns_kernel_times(dns_handle *h, double *ms, long *launches);
 
+/* ---- allocation-free reduction ------------------------------------------- */
+/* No counterpart in the reference.  For callers that cannot allocate device
+   memory — code running while a CUDA graph is being captured, hosts that give
+   the library a fixed memory budget and forbid allocation after start-up, or
+   pool-allocator embeddings where an extra cudaMalloc would fragment or overrun
+   the pool: the constant-flow-rate reduction (encalc2's momentum and mass sums
+   and the force they set) over a state the caller holds on the device in this
+   library's layout — coarse fc[19][zdv][ydv][xdv], fine ff[19][2 zds][GR ydv]
+   [GR xdv] with the lower block's planes k = 1..zds first, then the upper
+   block's k = 0..zds-1.  The result {force, momentum, mass, unused} is written
+   to out4 (4 doubles of device memory) on cuda_stream (NULL: default stream).
+   Nothing is allocated: the per-block partial sums live in a 4 MiB array
+   compiled into the library, which every GPU that loads the library holds
+   until the process exits; a domain needing more than 262144 reduction blocks
+   is rejected with DNS_EINVAL.  The first call on a device looks up that
+   array's device address; make it before any stream capture.  All calls share
+   the array, so calls that overlap on the GPU race: serialise them. */
+int dns_flow_sums_static(const dns_params *p, const double *fc, const double *ff, double *out4, void *cuda_stream);
+
 /* ---- errors -------------------------------------------------------------- */
 const char *dns_error_string(int code);
 const char *dns_last_error(void);
