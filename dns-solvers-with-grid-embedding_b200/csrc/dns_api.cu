@@ -68,6 +68,11 @@ struct dns_handle {
   DevLog *dlog = nullptr;              // kLogCap rows
   DevLog *hlog = nullptr;              // pinned mirror
   double *stats_acc = nullptr;         // [nz_profile][16]
+  double *iface_mac = nullptr;         // interface rho, u at fine nodes [2][4][nyf][nxf]
+  unsigned int *fin_counter = nullptr; // finalize's block counter
+  cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
+  cudaStream_t hip = nullptr;          // interface transfers (highest priority)
+  cudaEvent_t ev_start = nullptr, ev_inj = nullptr, ev_ext = nullptr, ev_fine[4] = {}, ev_if[4] = {};
   int cur_c = 0, cur_f = 0;
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
@@ -75,6 +80,8 @@ struct dns_handle {
   std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
   Profiler prof;
 };
+
+static bool d_gr_ok(const dns_handle *h) { return h->d.gr <= 4; }
 
 // Bracket one launch with events when profiling; returns the pair index or -1.
 static int prof_begin(dns_handle *h, int cls) {
@@ -222,7 +229,8 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   LaunchShape s = make_shape(d);
   PartialLayout pl = partial_layout(d, s);
   const long long nc = 19LL * g->nzc * g->ny * g->nx, nf = 19LL * 2 * p->zds * g->nyf * g->nxf;
-  g->device_bytes = 8 * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + pl.total + 16LL * g->nz_profile) +
+  g->device_bytes = 8 * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + pl.total + 16LL * g->nz_profile +
+                         8LL * g->nyf * g->nxf) +
                     (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
   return DNS_OK;
 }
@@ -265,9 +273,17 @@ extern "C" void dns_destroy(dns_handle *h) {
   cudaFree(h->state);
   cudaFree(h->dlog);
   cudaFree(h->stats_acc);
+  cudaFree(h->iface_mac);
+  cudaFree(h->fin_counter);
   if (h->hlog) cudaFreeHost(h->hlog);
   for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (h->aux) cudaStreamDestroy(h->aux);
+  if (h->hip) cudaStreamDestroy(h->hip);
+  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_ext, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
+                        &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
+  for (cudaEvent_t *e : evs)
+    if (*e) cudaEventDestroy(*e);
   delete h;
 }
 
@@ -311,6 +327,9 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   if ((rc = alloc((void **)&h->state, sizeof(DevState)))) return rc;
   if ((rc = alloc((void **)&h->dlog, kLogCap * sizeof(DevLog)))) return rc;
   if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * 16 * 8))) return rc;
+  if ((rc = alloc((void **)&h->iface_mac, 8ull * g.nyf * g.nxf * 8))) return rc;
+  if ((rc = alloc((void **)&h->fin_counter, 256))) return rc;
+  cudaMemset(h->fin_counter, 0, 256);
   if (cudaMallocHost((void **)&h->hlog, kLogCap * sizeof(DevLog)) != cudaSuccess) {
     dns_destroy(h);
     return fail(DNS_ENOMEM, "cudaMallocHost failed");
@@ -320,6 +339,17 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
     return fail(DNS_ECUDA, "cudaStreamCreate failed");
   }
   h->own_stream = true;
+  int prio_low = 0, prio_high = 0;
+  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
+  bool ev_ok = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_low) == cudaSuccess &&
+               cudaStreamCreateWithPriority(&h->hip, cudaStreamNonBlocking, prio_high) == cudaSuccess;
+  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_ext, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
+                        &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
+  for (cudaEvent_t *e : evs) ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+  if (!ev_ok) {
+    dns_destroy(h);
+    return fail(DNS_ECUDA, "stream / event creation failed");
+  }
   std::vector<int8_t> wf = wall_flags(*p, g);
   cudaMemcpy(h->wflag, wf.data(), wf.size(), cudaMemcpyHostToDevice);
   cudaMemset(h->partials, 0, (size_t)h->pl.total * 8);
@@ -610,7 +640,67 @@ extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
 }
 
 // ---------------------------------------------------------------- stepping
+// One coarse step on three streams.  The interface transfer of substep s
+// writes only the interface planes of the buffer whose other planes the fine
+// kernel of substep s writes, so the two run concurrently; the coarse kernel
+// and the extraction run beside the first fine substep.  The latency-bound
+// interface kernels sit on the highest-priority stream so that their blocks
+// take SM slots ahead of the bandwidth-bound fine blocks.
+//   main:  coarse, extract ........................................ [wait inject, iface(GR)] finalize
+//   aux:   [wait start] fine(1), [wait iface(1)] fine(2), ..., inject
+//   high:  [wait extract] iface(1), [wait fine(1)] iface(2), ...
+// Step schedule (compile-time): 0 one stream in order, 1 interface transfers on
+// the main stream beside the fine substeps, 2 interface transfers on their own
+// high-priority stream.
+#ifndef DNS_SCHED
+#define DNS_SCHED 1
+#endif
+static void issue_step_overlapped(dns_handle *h, DevLog *log_row, bool sample) {
+  const Dims &d = h->d;
+  const LaunchShape &s = h->shape;
+  cudaStream_t S = h->stream, T = h->aux, H = DNS_SCHED == 2 ? h->hip : h->stream;
+  const int nc = 1 - h->cur_c;
+  cudaEventRecord(h->ev_start, S);
+  cudaStreamWaitEvent(T, h->ev_start, 0);
+  launch_coarse_f64(h->fc[h->cur_c], h->fc[nc], d, s, h->g.omega_c, h->state, h->partials, h->pl, sample, S);
+  const int t = h->hpp;
+  h->hpp = h->hp;
+  h->hp = h->hn;
+  h->hn = t;
+  const size_t hslot = 2ull * 23 * d.ny * d.nx;
+  launch_extract_f64(h->fc[nc], h->hist + h->hn * hslot, d, s, S);
+  cudaEventRecord(h->ev_ext, S);
+  cudaStreamWaitEvent(H, h->ev_ext, 0);
+  int cur = h->cur_f;
+  for (int it = 1; it <= d.gr; it++) {
+    const int nf = 1 - cur;
+    if (it > 1) cudaStreamWaitEvent(T, h->ev_if[it - 2], 0);
+    launch_fine_f64(h->ff[cur], h->ff[nf], h->wflag, d, s, h->g.omega_f, h->state, h->partials, h->pl, it == 1,
+                    it == d.gr, sample && it == 1, T);
+    cudaEventRecord(h->ev_fine[it - 1], T);
+    if (it > 1) cudaStreamWaitEvent(H, h->ev_fine[it - 2], 0);
+    launch_interface_f64(h->hist + h->hn * hslot, h->hist + h->hp * hslot, h->hist + h->hpp * hslot, h->iface_mac,
+                         h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, H);
+    cudaEventRecord(h->ev_if[it - 1], H);
+    cur = nf;
+  }
+  launch_inject_f64(h->ff[cur], h->fc[nc], d, s, h->g.omega_c, h->g.omega_f, h->partials, h->pl, T);
+  cudaEventRecord(h->ev_inj, T);
+  cudaStreamWaitEvent(S, h->ev_inj, 0);
+  cudaStreamWaitEvent(S, h->ev_if[d.gr - 1], 0);
+  launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, s, h->sp, S);
+  if (sample) launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, s, S);
+  h->cur_f = cur;
+  h->cur_c = nc;
+}
+
+// The same step in stream order on one stream (used while profiling, so that
+// every launch can be bracketed by its own pair of events).
 static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
+  if (DNS_SCHED > 0 && !h->prof.on && d_gr_ok(h)) {
+    issue_step_overlapped(h, log_row, sample);
+    return;
+  }
   const Dims &d = h->d;
   const LaunchShape &s = h->shape;
   const int nc = 1 - h->cur_c;
@@ -628,12 +718,12 @@ static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
     PROFILED(h, 2, launch_fine_f64(h->ff[h->cur_f], h->ff[nf], h->wflag, d, s, h->g.omega_f, h->state,
                                    h->partials, h->pl, it == 1, it == d.gr, sample && it == 1, h->stream));
     PROFILED(h, 3, launch_interface_f64(h->hist + h->hn * hslot, h->hist + h->hp * hslot, h->hist + h->hpp * hslot,
-                                        h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, h->stream));
+                                        h->iface_mac, h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, h->stream));
     h->cur_f = nf;
   }
   PROFILED(h, 4, launch_inject_f64(h->ff[h->cur_f], h->fc[nc], d, s, h->g.omega_c, h->g.omega_f, h->partials,
                                    h->pl, h->stream));
-  PROFILED(h, 5, launch_finalize(h->state, log_row, h->partials, h->pl, d, s, h->sp, h->stream));
+  PROFILED(h, 5, launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, s, h->sp, h->stream));
   if (sample) PROFILED(h, 6, launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, s, h->stream));
   h->cur_c = nc;
 }

@@ -47,7 +47,7 @@ void set_last_error(const std::string &msg);
 
 // Reduction scratch sizes (doubles) for a given shape.
 struct PartialLayout {
-  long coarse, fine, inject, wall, stats_c, stats_f, flow;  // offsets into one buffer
+  long coarse, fine, inject, wall, stats_c, stats_f, flow, level2;  // offsets into one buffer
   long total;
 };
 PartialLayout partial_layout(const Dims &d, const LaunchShape &s);
@@ -68,13 +68,17 @@ void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const L
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
                      bool last, bool stats, cudaStream_t stream);
-void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *fdst, const Dims &d,
-                          const LaunchShape &s, int substep, double omega_c, double omega_f,
+// two launches: macroscopic fields into mac[2 walls][4][nyf][nxf], then one
+// block per (tile, wall, population) into the interface planes of fdst
+void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *mac, double *fdst,
+                          const Dims &d, const LaunchShape &s, int substep, double omega_c, double omega_f,
                           cudaStream_t stream);
 void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
                        double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
-void launch_finalize(DevState *st, DevLog *log_row, const double *partials, const PartialLayout &pl,
-                     const Dims &d, const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
+// counter: one device unsigned int, zero between launches (the kernel resets it)
+void launch_finalize(DevState *st, DevLog *log_row, double *partials, unsigned int *counter,
+                     const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
+                     cudaStream_t stream);
 void launch_stats_finalize(double *acc, const double *partials, const PartialLayout &pl, const Dims &d,
                            const LaunchShape &s, cudaStream_t stream);
 // direct encalc2 reduction of the stored state into st (momentum, denst, force)

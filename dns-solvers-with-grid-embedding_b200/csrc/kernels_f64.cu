@@ -23,7 +23,22 @@ namespace dns {
 
 namespace {
 
-constexpr int kMaxThreads = 128;
+// Launch-shape tuning knobs (compile-time): threads per block along x, rows per
+// block, and the minimum resident blocks per SM asked of the register
+// allocator for the two stream-collide kernels (0 = let the compiler choose).
+#ifndef DNS_BX
+#define DNS_BX 128
+#endif
+#ifndef DNS_JB
+#define DNS_JB 2
+#endif
+#ifndef DNS_MINB_FINE
+#define DNS_MINB_FINE 0
+#endif
+#ifndef DNS_MINB_COARSE
+#define DNS_MINB_COARSE 0
+#endif
+constexpr int kMaxThreads = DNS_BX;
 
 // periodic index for any offset (an interface tile can be wider than the domain)
 __device__ __forceinline__ int wrapi(int v, int n) {
@@ -55,6 +70,29 @@ __device__ __forceinline__ void block_reduce(double (&v)[N], double *out) {
   __syncthreads();
 }
 
+// Fixed-order block reduction of N doubles into shared out[N] (visible to all
+// threads on return); NT threads per block.
+template <int N, int NT>
+__device__ __forceinline__ void block_reduce_n(double (&v)[N], double *out) {
+  __shared__ double red[N][NT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x < N) {
+    double s = red[threadIdx.x][0];
+#pragma unroll
+    for (int w = 1; w < NT / 32; w++) s += red[threadIdx.x][w];
+    out[threadIdx.x] = s;
+  }
+  __syncthreads();
+}
+
 __device__ __forceinline__ void load19(const double *__restrict__ src, size_t idx, size_t stride, double (&f)[19]) {
 #pragma unroll
   for (int a = 0; a < 19; a++) f[a] = __ldg(src + idx + (size_t)a * stride);
@@ -67,7 +105,7 @@ __device__ __forceinline__ void load19(const double *__restrict__ src, size_t id
 // Partials: constant-flow-rate momentum/mass of what lands in dst (all weight
 // GR^3 in encalc2.c:57-84); with STATS the pre-collision plane moments.
 template <bool STATS>
-__global__ void __launch_bounds__(kMaxThreads) coarse_kernel(const double *__restrict__ src, double *__restrict__ dst,
+__global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                             Dims d, int jb, double om, const DevState *st,
                                                             double *__restrict__ part, double *__restrict__ spart) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc;
@@ -147,7 +185,7 @@ __global__ void __launch_bounds__(kMaxThreads) extract_kernel(const double *__re
 // substep; encalc2.c:33-53, 86-107 weights), 2 wall-shear plane sums of the
 // pre-collision state (first substep; wshearstr.c:37-134), 4 plane statistics.
 template <int MODE>
-__global__ void __launch_bounds__(kMaxThreads) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
+__global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                           const int8_t *__restrict__ wf, Dims d, int jb, double om,
                                                           const DevState *st, double *__restrict__ part,
                                                           double *__restrict__ wpart, double *__restrict__ spart) {
@@ -230,8 +268,9 @@ __global__ void __launch_bounds__(kMaxThreads) fine_kernel(const double *__restr
 // GR x GR fine nodes and f = feq + omega_c/(GR omega_f) fneq.  A tile of
 // ITX x ITY coarse cells stages the (ITX+5) x (ITY+5) periodic patch of one
 // field at a time in shared memory; one thread owns one coarse cell.
-constexpr int ITX = 16, ITY = 8;
-constexpr int PX = ITX + 5, PY = ITY + 5;
+constexpr int ITX = 32, ITY = 16;          // coarse cells per tile
+constexpr int TPX = 16, TPY = 8;           // threads per tile (each owns 2 x 2 cells)
+constexpr int PX = ITX + 5, PY = ITY + 5;  // staged periodic patch
 
 struct IfaceArgs {
   double h1, h2, h3, h4, fac;
@@ -276,13 +315,13 @@ __device__ __forceinline__ void iface_stage(IfaceSmem &S, const double *__restri
   __syncthreads();
 }
 
-// Bicubic coefficients of cell (tx, ty) of the staged field.
-__device__ __forceinline__ void iface_coeffs(const IfaceSmem &S, int tx, int ty, double (&cf)[16]) {
+// Bicubic coefficients of tile cell (cx, cy) of the staged field.
+__device__ __forceinline__ void iface_coeffs(const IfaceSmem &S, int cx, int cy, double (&cf)[16]) {
   double x[16];
   const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 0, 1, 1};
 #pragma unroll
   for (int q = 0; q < 4; q++) {
-    const int c = tx + ci[q], r = ty + cj[q];
+    const int c = cx + ci[q], r = cy + cj[q];
     x[q] = S.V[r + 2][c + 2];
     x[4 + q] = S.Dx[r][c];
     x[8 + q] = S.Dy[r][c + 2];
@@ -291,78 +330,103 @@ __device__ __forceinline__ void iface_coeffs(const IfaceSmem &S, int tx, int ty,
   DNS_BICUBIC_COEFFS(cf, x);
 }
 
-// Horner evaluation at (t, u) = (ii/GR, jj/GR), ctfdtransfer_opt.c:62-97 order.
+// Horner evaluation at (t, u) = (ii/GR, jj/GR), ctfdtransfer_opt.c:62-97 order:
+// val = t val + ((c3 u + c2) u + c1) u + c0 for nn = 3..0, starting from 0.
+// At t = 0 every t val term is an exact zero, so val is the nn = 0 polynomial;
+// at u = 0 each inner polynomial is its constant term.  Adding an exact zero
+// leaves a non-zero value unchanged, so the shortcuts give the same value
+// (a zero result can only differ in the sign of the zero).
 template <int GR>
 __device__ __forceinline__ double iface_eval(const double (&cf)[16], int ii, int jj) {
   const double tt = ((double)ii) / ((double)GR);
   const double uu = ((double)jj) / ((double)GR);
-  double val = 0.;
+  if (ii == 0 && jj == 0) return cf[0];
+  if (ii == 0) return ((cf[3] * uu + cf[2]) * uu + cf[1]) * uu + cf[0];
+  if (jj == 0) {
+    double val = cf[12];
+    val = tt * val + cf[8];
+    val = tt * val + cf[4];
+    return tt * val + cf[0];
+  }
+  double val = ((cf[15] * uu + cf[14]) * uu + cf[13]) * uu + cf[12];
 #pragma unroll
-  for (int nn = 3; nn > -1; nn--)
+  for (int nn = 2; nn > -1; nn--)
     val = tt * val + ((cf[nn * 4 + 3] * uu + cf[nn * 4 + 2]) * uu + cf[nn * 4 + 1]) * uu + cf[nn * 4 + 0];
   return val;
 }
 
+// Phase 1: macroscopic fields.  Block (tile, wall, field b < 4) writes field b
+// (rho, ux, uy, uz) at the tile's fine interface nodes into mac[wall][b][j][i].
 template <int GR>
-__global__ void __launch_bounds__(ITX *ITY) interface_kernel(const double *__restrict__ hn,
-                                                             const double *__restrict__ hp,
-                                                             const double *__restrict__ hpp,
-                                                             double *__restrict__ fdst, Dims d, IfaceArgs ia) {
+__global__ void __launch_bounds__(TPX *TPY) interface_macro_kernel(const double *__restrict__ hn,
+                                                                   const double *__restrict__ hp,
+                                                                   const double *__restrict__ hpp,
+                                                                   double *__restrict__ mac, Dims d, IfaceArgs ia) {
   __shared__ IfaceSmem S;
-  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf, zds = d.zds;
-  const int w = blockIdx.z;
+  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf;
+  const int w = blockIdx.z >> 2, b = blockIdx.z & 3;
   const int i0 = blockIdx.x * ITX, j0 = blockIdx.y * ITY;
-  const int tx = threadIdx.x % ITX, ty = threadIdx.x / ITX;
-  const int ic = i0 + tx, jc = j0 + ty;
-  const bool valid = ic < nx && jc < ny;
-  const size_t plane = (size_t)ny * nx;
-  const int pf = w == 0 ? zds - 1 : zds;  // interface plane of the fine block
-  const size_t fstride = (size_t)2 * zds * nyf * nxf;
-  constexpr int NN = GR * GR;
-  // macroscopic fields rho, ux, uy, uz at the GR x GR fine nodes of this cell
-  double mac[4][NN];
+  const int tx = threadIdx.x % TPX, ty = threadIdx.x / TPX;
+  const size_t plane = (size_t)ny * nx, fplane = (size_t)nyf * nxf;
+  iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + b) * plane, i0, j0, nx, ny, ia);
+  double *o = mac + ((size_t)w * 4 + b) * fplane;
 #pragma unroll
-  for (int b = 0; b < 4; b++)
-#pragma unroll
-    for (int q = 0; q < NN; q++) mac[b][q] = 0.;
-#pragma unroll
-  for (int b = 0; b < 4; b++) {
-    iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + b) * plane, i0, j0, nx, ny, ia);
-    if (valid) {
+  for (int q = 0; q < 4; q++) {
+    const int cx = tx + TPX * (q & 1), cy = ty + TPY * (q >> 1);
+    const int ic = i0 + cx, jc = j0 + cy;
+    if (ic < nx && jc < ny) {
       double cf[16];
-      iface_coeffs(S, tx, ty, cf);
+      iface_coeffs(S, cx, cy, cf);
 #pragma unroll
       for (int ii = 0; ii < GR; ii++)
 #pragma unroll
-        for (int jj = 0; jj < GR; jj++) mac[b][ii * GR + jj] = iface_eval<GR>(cf, ii, jj);
+        for (int jj = 0; jj < GR; jj++)
+          o[(size_t)(jc * GR + jj) * nxf + ic * GR + ii] = iface_eval<GR>(cf, ii, jj);
     }
-    __syncthreads();
   }
-  double t15v[NN];
+}
+
+// Phase 2: one population per block (tile, wall, a): feq(rho, u) of phase 1
+// plus omega_c / (GR omega_f) times the interpolated fneq, into the fine
+// block's interface plane.
+template <int GR>
+__global__ void __launch_bounds__(TPX *TPY) interface_pop_kernel(const double *__restrict__ hn,
+                                                                 const double *__restrict__ hp,
+                                                                 const double *__restrict__ hpp,
+                                                                 const double *__restrict__ mac,
+                                                                 double *__restrict__ fdst, Dims d, IfaceArgs ia) {
+  __shared__ IfaceSmem S;
+  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf, zds = d.zds;
+  const int w = blockIdx.z / 19, a = blockIdx.z % 19;
+  const int i0 = blockIdx.x * ITX, j0 = blockIdx.y * ITY;
+  const int tx = threadIdx.x % TPX, ty = threadIdx.x / TPX;
+  const size_t plane = (size_t)ny * nx, fplane = (size_t)nyf * nxf;
+  const int pf = w == 0 ? zds - 1 : zds;  // interface plane of the fine block
+  const size_t fstride = (size_t)2 * zds * fplane;
+  iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + 4 + a) * plane, i0, j0, nx, ny, ia);
+  const int cls = a == 0 ? 0 : (a <= 6 ? 1 : 2);
+  const double wa = cls == 0 ? 1. / 3. : (cls == 1 ? 1. / 18. : 1. / 36.);
+  const double *m = mac + (size_t)w * 4 * fplane;
+  double *out = fdst + (size_t)a * fstride + (size_t)pf * fplane;
 #pragma unroll
-  for (int q = 0; q < NN; q++)
-    t15v[q] = 1.5 * (mac[1][q] * mac[1][q] + mac[2][q] * mac[2][q] + mac[3][q] * mac[3][q]);
-  // populations: feq(rho, u) + omega_c / (GR omega_f) fneq
-#pragma unroll 1
-  for (int a = 0; a < 19; a++) {
-    iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + 4 + a) * plane, i0, j0, nx, ny, ia);
-    if (valid) {
+  for (int q = 0; q < 4; q++) {
+    const int cx = tx + TPX * (q & 1), cy = ty + TPY * (q >> 1);
+    const int ic = i0 + cx, jc = j0 + cy;
+    if (ic < nx && jc < ny) {
       double cf[16];
-      iface_coeffs(S, tx, ty, cf);
-      const int cls = a == 0 ? 0 : (a <= 6 ? 1 : 2);
-      const double wa = cls == 0 ? 1. / 3. : (cls == 1 ? 1. / 18. : 1. / 36.);
+      iface_coeffs(S, cx, cy, cf);
 #pragma unroll
       for (int ii = 0; ii < GR; ii++)
 #pragma unroll
         for (int jj = 0; jj < GR; jj++) {
-          const int q = ii * GR + jj;
+          const size_t qn = (size_t)(jc * GR + jj) * nxf + ic * GR + ii;
+          const double rho = m[qn], u0 = m[fplane + qn], u1 = m[2 * fplane + qn], u2 = m[3 * fplane + qn];
+          const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
           const double val = iface_eval<GR>(cf, ii, jj);
-          const double feq = feq_f64(wa * mac[0][q], proj_f64(a, mac[1][q], mac[2][q], mac[3][q]), t15v[q]);
-          const int fi = ic * GR + ii, fj = jc * GR + jj;
-          fdst[(size_t)a * fstride + ((size_t)pf * nyf + fj) * nxf + fi] = feq + ia.fac * val;
+          const double feq = feq_f64(wa * rho, proj_f64(a, u0, u1, u2), t15v);
+          out[qn] = feq + ia.fac * val;
         }
     }
-    __syncthreads();
   }
 }
 
@@ -511,6 +575,75 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(DevState *st, Dev
     st->momentum = mom;
     st->denst = den;
     st->force = a.cfr ? a.ub - mom : a.gconst;
+  }
+}
+
+// Per-step finalize in two levels: kFin2Blocks blocks each reduce a fixed
+// chunk of every partial region (fixed order), the last block to finish sums
+// the chunk results in block order.  Deterministic, one launch, no waiting.
+constexpr int kFin2Blocks = 64, kFin2Threads = 256, kFin2Comp = 18;
+
+__global__ void __launch_bounds__(kFin2Threads) finalize2_kernel(DevState *st, DevLog *lg, const double *part_c,
+                                                                const double *part_f, const double *part_i,
+                                                                const double *part_w, double *level2,
+                                                                unsigned int *counter, FinArgs a) {
+  __shared__ double sh[kFin2Comp];
+  __shared__ bool last;
+  const int b = blockIdx.x, nb = gridDim.x;
+  double v[kFin2Comp];
+#pragma unroll
+  for (int c = 0; c < kFin2Comp; c++) v[c] = 0.;
+  // this block's fixed chunk of every region; each thread strides through it
+  auto acc = [&](const double *p, long n, int c0) {
+    const long lo = n * b / nb, hi = n * (b + 1) / nb;
+    for (long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+      v[c0] += p[q * 2];
+      v[c0 + 1] += p[q * 2 + 1];
+    }
+  };
+  acc(part_c, a.nc, 0);
+  acc(part_f, a.nf, 2);
+  acc(part_i, a.ni, 4);
+#pragma unroll
+  for (int q = 0; q < 6; q++) acc(part_w + a.wb[q] * 2, a.wn, 6 + 2 * q);
+  block_reduce_n<kFin2Comp, kFin2Threads>(v, sh);
+  if (threadIdx.x == 0) {
+    for (int c = 0; c < kFin2Comp; c++) level2[b * kFin2Comp + c] = sh[c];
+    __threadfence();
+    last = atomicAdd(counter, 1u) == (unsigned)(nb - 1);
+  }
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x < kFin2Comp) {
+    const volatile double *l2 = level2;
+    double s = 0.;
+    for (int q = 0; q < nb; q++) s += l2[q * kFin2Comp + threadIdx.x];
+    sh[threadIdx.x] = s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const double *S = sh;
+    DevLog r;
+    r.force = st->force;
+    r.momentum = st->momentum;
+    r.denst = st->denst;
+    r.flowrate = st->momentum * a.flow_scale / st->denst;
+    const double *U = S + 6;  // (U, D) pairs per plane: lower k=1,2,3, upper zdf-2,-3,-4
+    const double stdown = ((-2. * U[0] + 3. * U[2] - U[4]) / a.norm2) * (a.mu * (U[1] / a.norm2));
+    const double stup = (-(2. * U[6] - 3. * U[8] + U[10]) / a.norm2) * (a.mu * (U[11] / a.norm2));
+    r.stup = stup;
+    r.stdown = stdown;
+    r.stress = 0.5 * (stup + stdown);
+    r.pgrad = st->force * a.pgrad_scale;
+    *lg = r;
+    const double mom = (a.g3 * S[0] + 0.5 * a.g3 * S[4] + S[2]) / a.norm;
+    const double den = (a.g3 * S[1] + 0.5 * a.g3 * S[5] + S[3]) / a.norm;
+    st->momentum = mom;
+    st->denst = den;
+    st->force = a.cfr ? a.ub - mom : a.gconst;
+    *counter = 0u;
   }
 }
 
@@ -675,8 +808,8 @@ __global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__rest
 // ====================================================================== host
 LaunchShape make_shape(const Dims &d) {
   LaunchShape s;
-  s.bx = 128;
-  s.jb = 2;
+  s.bx = DNS_BX;
+  s.jb = DNS_JB;
   s.cgx = (d.nx + s.bx - 1) / s.bx;
   s.cgy = (d.ny + s.jb - 1) / s.jb;
   s.fgx = (d.nxf + s.bx - 1) / s.bx;
@@ -701,6 +834,7 @@ PartialLayout partial_layout(const Dims &d, const LaunchShape &s) {
   pl.stats_f = o; o += nbf * 9;
   const long gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
   pl.flow = o; o += gx * gy * (d.nzc + 2 * d.zds) * 2;
+  pl.level2 = o; o += kFin2Blocks * kFin2Comp;
   pl.total = o;
   return pl;
 }
@@ -736,8 +870,9 @@ void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const 
 #undef FINE_CASE
 }
 
-void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *fdst, const Dims &d,
-                          const LaunchShape &s, int substep, double omega_c, double omega_f, cudaStream_t stream) {
+void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *mac, double *fdst,
+                          const Dims &d, const LaunchShape &s, int substep, double omega_c, double omega_f,
+                          cudaStream_t stream) {
   // Hermite basis at tau = substep / GR, evaluated as the reference writes it
   // (tinterpolate_hrmt.c:34); rescaling factor of ctfdtransfer_opt.c:101.
   const double tmp = (((double)substep) / ((double)d.gr));
@@ -747,13 +882,17 @@ void launch_interface_f64(const double *hn, const double *hp, const double *hpp,
   ia.h3 = -2. * tmp * tmp * tmp + 3. * tmp * tmp;
   ia.h4 = tmp * tmp * tmp - tmp * tmp;
   ia.fac = omega_c / ((double)d.gr * omega_f);
-  dim3 grid(s.igx, s.igy, 2), block(ITX * ITY);
-  if (d.gr == 2)
-    interface_kernel<2><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
-  else if (d.gr == 3)
-    interface_kernel<3><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
-  else
-    interface_kernel<4><<<grid, block, 0, stream>>>(hn, hp, hpp, fdst, d, ia);
+  dim3 gm(s.igx, s.igy, 2 * 4), gp(s.igx, s.igy, 2 * 19), block(TPX * TPY);
+  if (d.gr == 2) {
+    interface_macro_kernel<2><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
+    interface_pop_kernel<2><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+  } else if (d.gr == 3) {
+    interface_macro_kernel<3><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
+    interface_pop_kernel<3><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+  } else {
+    interface_macro_kernel<4><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
+    interface_pop_kernel<4><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+  }
 }
 
 void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
@@ -786,11 +925,13 @@ static FinArgs fin_args(const PartialLayout &pl, const Dims &d, const LaunchShap
   return a;
 }
 
-void launch_finalize(DevState *st, DevLog *log_row, const double *partials, const PartialLayout &pl, const Dims &d,
-                     const LaunchShape &s, const StepParams &sp, cudaStream_t stream) {
+void launch_finalize(DevState *st, DevLog *log_row, double *partials, unsigned int *counter,
+                     const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
+                     cudaStream_t stream) {
   FinArgs a = fin_args(pl, d, s, sp);
-  finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, log_row, partials + pl.coarse, partials + pl.fine,
-                                                 partials + pl.inject, partials + pl.wall, a);
+  finalize2_kernel<<<kFin2Blocks, kFin2Threads, 0, stream>>>(st, log_row, partials + pl.coarse, partials + pl.fine,
+                                                             partials + pl.inject, partials + pl.wall,
+                                                             partials + pl.level2, counter, a);
 }
 
 void launch_stats_finalize(double *acc, const double *partials, const PartialLayout &pl, const Dims &d,
