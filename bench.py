@@ -306,6 +306,34 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "log_tail": {"force": float(log[-1, 1]), "flowrate": float(log[-1, 4]), "stress": float(log[-1, 7])},
     }
+    # ---- the FP32 deviation-storage form on the same workload (same GPU)
+    if not args.no_fp32:
+        ch.close()
+        p32 = pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank, precision=pkg.FP32)
+        c32 = pkg.Channel(p32)
+        c32.set_stream(stream.cuda_stream)
+        c32.init_seeded(42 + rank, 0.05, 0.005)
+        c32.step(args.warmup, log=False)
+        torch.cuda.synchronize()
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        c32.step(args.steps, log=True)
+        s1.record(stream)
+        torch.cuda.synchronize()
+        ms32 = s0.elapsed_time(s1)
+        c32.set_profiling(True)
+        c32.step(prof_steps, log=False)
+        kt32 = c32.kernel_times()
+        c32.close()
+        f32_ms, f32_n = kt32["fine"]
+        ach32 = fine_nodes * 2 * 19 * 4 / (f32_ms / f32_n * 1e-3) / 1e9 if f32_n else None
+        v32 = U * args.steps * world / (ms32 * 1e-3) / 1e6
+        line["fp32"] = {"value": v32, "unit": "MLUPS", "ms_per_step": ms32 / args.steps, "dtype": "f32 (deviation)",
+                        "over_fp64": v32 / value,
+                        "roofline": {"bound": "hbm", "kernel": "fine_kernel", "achieved": ach32, "peak": peak,
+                                     "unit": "GB/s", "frac": (ach32 / peak) if ach32 else None},
+                        "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak,
+                        "kernel_ms_per_step": {k: (v[0] / prof_steps) for k, v in kt32.items()}}
     if world == 1 and not args.no_cpu_baseline:
         m_ = CONFIGS[args.config][0]
         secs = reference_cpu(args.config, args.cpu_steps, 1)
@@ -333,6 +361,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=4)
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-fp32", action="store_true")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))

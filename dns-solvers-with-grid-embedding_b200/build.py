@@ -21,6 +21,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INCLUDE), "-I", str(CSRC)]
 UNITS = {  # source -> extra flags
     "kernels_f64.cu": ["-fmad=false"],
+    "kernels_f32.cu": [],
     "dns_api.cu": [],
     "noalloc.cu": [],
 }

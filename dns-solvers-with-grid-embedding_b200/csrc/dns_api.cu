@@ -203,7 +203,8 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
     return fail(DNS_EINVAL, "zds must be >= max(4, gratio + 2) (transfer planes inside the fine block)");
   if (p->pattern < DNS_PATTERN_NONE || p->pattern > DNS_PATTERN_SSLIP) return fail(DNS_EINVAL, "bad pattern");
   if (p->Rebs <= 0 || p->ub <= 0 || p->CFL <= 0) return fail(DNS_EINVAL, "Rebs, ub and CFL must be positive");
-  if (p->precision != DNS_FP64) return fail(DNS_EINVAL, "only DNS_FP64 is available in this build");
+  if (p->precision != DNS_FP64 && p->precision != DNS_FP32) return fail(DNS_EINVAL, "precision must be DNS_FP64 or DNS_FP32");
+  if (p->precision == DNS_FP32 && p->zds > 32) return fail(DNS_EINVAL, "the FP32 form supports zds <= 32");
   std::memset(g, 0, sizeof(*g));
   const int GR = p->gratio;
   g->gr = GR;
@@ -229,8 +230,9 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   LaunchShape s = make_shape(d);
   PartialLayout pl = partial_layout(d, s);
   const long long nc = 19LL * g->nzc * g->ny * g->nx, nf = 19LL * 2 * p->zds * g->nyf * g->nxf;
-  g->device_bytes = 8 * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + pl.total + 16LL * g->nz_profile +
-                         8LL * g->nyf * g->nxf) +
+  const long long esz = p->precision == DNS_FP32 ? 4 : 8;  // bytes per stored population
+  g->device_bytes = esz * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + 8LL * g->nyf * g->nxf) +
+                    8 * (pl.total + 16LL * g->nz_profile) +
                     (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
   return DNS_OK;
 }
@@ -306,7 +308,10 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   h->d = Dims{g.nx, g.ny, g.nzc, g.nxf, g.nyf, g.zdf, p->zds, g.gr, g.nzs};
   h->shape = make_shape(h->d);
   h->pl = partial_layout(h->d, h->shape);
-  h->sp = StepParams{g.omega_c, g.omega_f, p->ub, p->force_const, p->forcing == DNS_FORCING_CFR ? 1 : 0};
+  h->sp = StepParams{g.omega_c, g.omega_f, p->ub, p->force_const, p->forcing == DNS_FORCING_CFR ? 1 : 0, 0.0};
+  // the FP32 form's mass partials sum deviations from w: add the weight sum once
+  if (p->precision == DNS_FP32) h->sp.den_offset = encalc2_weight_sum(h->d);
+  const size_t esz = p->precision == DNS_FP32 ? 4 : 8;
   h->tm = p->TSTR;
   const size_t nc = 19ull * g.nzc * g.ny * g.nx, nf = 19ull * 2 * p->zds * g.nyf * g.nxf;
   auto alloc = [&](void **ptr, size_t bytes) -> int {
@@ -318,16 +323,16 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
     return DNS_OK;
   };
   for (int q = 0; q < 2; q++) {
-    if ((rc = alloc((void **)&h->fc[q], nc * 8))) return rc;
-    if ((rc = alloc((void **)&h->ff[q], nf * 8))) return rc;
+    if ((rc = alloc((void **)&h->fc[q], nc * esz))) return rc;
+    if ((rc = alloc((void **)&h->ff[q], nf * esz))) return rc;
   }
-  if ((rc = alloc((void **)&h->hist, 3ull * 2 * 23 * g.ny * g.nx * 8))) return rc;
+  if ((rc = alloc((void **)&h->hist, 3ull * 2 * 23 * g.ny * g.nx * esz))) return rc;
   if ((rc = alloc((void **)&h->wflag, (size_t)g.nyf * g.nxf))) return rc;
   if ((rc = alloc((void **)&h->partials, (size_t)h->pl.total * 8))) return rc;
   if ((rc = alloc((void **)&h->state, sizeof(DevState)))) return rc;
   if ((rc = alloc((void **)&h->dlog, kLogCap * sizeof(DevLog)))) return rc;
   if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * 16 * 8))) return rc;
-  if ((rc = alloc((void **)&h->iface_mac, 8ull * g.nyf * g.nxf * 8))) return rc;
+  if ((rc = alloc((void **)&h->iface_mac, 8ull * g.nyf * g.nxf * esz))) return rc;
   if ((rc = alloc((void **)&h->fin_counter, 256))) return rc;
   cudaMemset(h->fin_counter, 0, 256);
   if (cudaMallocHost((void **)&h->hlog, kLogCap * sizeof(DevLog)) != cudaSuccess) {
@@ -389,7 +394,63 @@ extern "C" int dns_get_geometry(const dns_handle *h, dns_geometry *g) {
 
 // ---------------------------------------------------------------- state transfer
 // device SoA <-> reference AoS of one level, staged through the idle ping-pong buffer
+static bool is_f32(const dns_handle *h) { return h->p.precision == DNS_FP32; }
+static float *F(double *p) { return reinterpret_cast<float *>(p); }
+
+// FP32 form: float deviations on the device <-> reference AoS doubles, through
+// a temporary device staging buffer (an I/O path, not the step)
+static int export_level_f32(dns_handle *h, int level, double *out) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  const size_t n = level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
+  double *stage = nullptr;
+  if (cudaMalloc(&stage, n * 8) != cudaSuccess) return fail(DNS_ENOMEM, "staging buffer for export");
+  if (level == 0)
+    launch_dev_to_aos_f32(F(h->fc[h->cur_c]), stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+  else if (level == 1)
+    launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
+  else
+    launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
+  cudaError_t e = cudaMemcpyAsync(out, stage, n * 8, cudaMemcpyDeviceToHost, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(stage);
+  if (e != cudaSuccess) return fail(DNS_ECUDA, cudaGetErrorString(e));
+  if (level > 0) {
+    const std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+    const int kw = level == 1 ? 0 : g.zdf - 1;
+    for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
+      std::memcpy(out + (c * g.zdf + kw) * 19, wall.data() + c * 19, 19 * 8);
+  }
+  return DNS_OK;
+}
+
+static int import_level_f32(dns_handle *h, int level, const double *in) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  const size_t n = level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
+  double *stage = nullptr;
+  if (cudaMalloc(&stage, n * 8) != cudaSuccess) return fail(DNS_ENOMEM, "staging buffer for import");
+  cudaError_t e = cudaMemcpyAsync(stage, in, n * 8, cudaMemcpyHostToDevice, h->stream);
+  if (level == 0)
+    launch_aos_to_dev_f32(stage, F(h->fc[h->cur_c]), g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+  else if (level == 1)
+    launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
+  else
+    launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  cudaFree(stage);
+  if (e != cudaSuccess) return fail(DNS_ECUDA, cudaGetErrorString(e));
+  if (level > 0) {
+    std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+    const int kw = level == 1 ? 0 : g.zdf - 1;
+    for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
+      std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
+  }
+  return DNS_OK;
+}
+
 static int export_level(dns_handle *h, int level, double *out) {
+  if (is_f32(h)) return export_level_f32(h, level, out);
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
   if (level == 0) {
@@ -418,6 +479,7 @@ static int export_level(dns_handle *h, int level, double *out) {
 }
 
 static int import_level(dns_handle *h, int level, const double *in) {
+  if (is_f32(h)) return import_level_f32(h, level, in);
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
   if (level == 0) {
@@ -449,8 +511,18 @@ static int export_history(dns_handle *h, double *out) {
   const dns_geometry &g = h->g;
   const size_t plane = (size_t)g.ny * g.nx, per = 2 * 23 * plane;
   std::vector<double> tmp(3 * per);
-  CUDA_TRY(cudaMemcpyAsync(tmp.data(), h->hist, 3 * per * 8, cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  if (is_f32(h)) {
+    // float [drho, u, fneq] -> reference [rho, u, fneq]
+    std::vector<float> t32(3 * per);
+    CUDA_TRY(cudaMemcpyAsync(t32.data(), h->hist, 3 * per * 4, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    for (size_t q = 0; q < t32.size(); q++) tmp[q] = t32[q];
+    for (size_t sl = 0; sl < 6; sl++)
+      for (size_t q = 0; q < plane; q++) tmp[sl * 23 * plane + q] += 1.0;
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(tmp.data(), h->hist, 3 * per * 8, cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+  }
   const int slots[3] = {h->hn, h->hp, h->hpp};
   for (int l = 0; l < 3; l++)
     for (int w = 0; w < 2; w++)
@@ -473,7 +545,15 @@ static int import_history(dns_handle *h, const double *in) {
           for (int b = 0; b < 23; b++)
             tmp[(((size_t)l * 2 + w) * 23 + b) * plane + (size_t)j * g.nx + i] =
                 in[((((size_t)l * 2 + w) * g.nx + i) * g.ny + j) * 23 + b];
-  CUDA_TRY(cudaMemcpyAsync(h->hist, tmp.data(), 3 * per * 8, cudaMemcpyHostToDevice, h->stream));
+  if (is_f32(h)) {
+    std::vector<float> t32(3 * per);
+    for (size_t sl = 0; sl < 6; sl++)
+      for (size_t q = 0; q < plane; q++) tmp[sl * 23 * plane + q] -= 1.0;
+    for (size_t q = 0; q < t32.size(); q++) t32[q] = (float)tmp[q];
+    CUDA_TRY(cudaMemcpyAsync(h->hist, t32.data(), 3 * per * 4, cudaMemcpyHostToDevice, h->stream));
+  } else {
+    CUDA_TRY(cudaMemcpyAsync(h->hist, tmp.data(), 3 * per * 8, cudaMemcpyHostToDevice, h->stream));
+  }
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   h->hn = 0;
   h->hp = 1;
@@ -485,8 +565,12 @@ static int import_history(dns_handle *h, const double *in) {
 static int refresh_flow(dns_handle *h, double force_file) {
   DevState st{force_file, 0., 0., 0.};
   CUDA_TRY(cudaMemcpyAsync(h->state, &st, sizeof st, cudaMemcpyHostToDevice, h->stream));
-  launch_flow_sums_f64(h->fc[h->cur_c], h->ff[h->cur_f], h->state, h->partials, h->pl, h->d, h->shape, h->sp,
-                       h->stream);
+  if (is_f32(h))
+    launch_flow_sums_f32(F(h->fc[h->cur_c]), F(h->ff[h->cur_f]), h->state, h->partials, h->pl, h->d, h->shape, h->sp,
+                         h->stream);
+  else
+    launch_flow_sums_f64(h->fc[h->cur_c], h->ff[h->cur_f], h->state, h->partials, h->pl, h->d, h->shape, h->sp,
+                         h->stream);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DNS_OK;
@@ -530,7 +614,10 @@ extern "C" int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double a
   h->hn = 0;
   h->hp = 1;
   h->hpp = 2;
-  launch_seed_f64(h->fc[0], h->ff[0], h->hist, h->d, seed, uc, amp, h->stream);
+  if (is_f32(h))
+    launch_seed_f32(F(h->fc[0]), F(h->ff[0]), F(h->hist), h->d, seed, uc, amp, h->stream);
+  else
+    launch_seed_f64(h->fc[0], h->ff[0], h->hist, h->d, seed, uc, amp, h->stream);
   CUDA_TRY(cudaGetLastError());
   std::fill(h->wall_lo.begin(), h->wall_lo.end(), 0.0);
   std::fill(h->wall_hi.begin(), h->wall_hi.end(), 0.0);
@@ -640,56 +727,97 @@ extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
 }
 
 // ---------------------------------------------------------------- stepping
-// One coarse step on three streams.  The interface transfer of substep s
-// writes only the interface planes of the buffer whose other planes the fine
-// kernel of substep s writes, so the two run concurrently; the coarse kernel
-// and the extraction run beside the first fine substep.  The latency-bound
-// interface kernels sit on the highest-priority stream so that their blocks
-// take SM slots ahead of the bandwidth-bound fine blocks.
-//   main:  coarse, extract ........................................ [wait inject, iface(GR)] finalize
-//   aux:   [wait start] fine(1), [wait iface(1)] fine(2), ..., inject
-//   high:  [wait extract] iface(1), [wait fine(1)] iface(2), ...
-// Step schedule (compile-time): 0 one stream in order, 1 interface transfers on
-// the main stream beside the fine substeps, 2 interface transfers on their own
-// high-priority stream.
+// Precision dispatch for one launch of each kernel.  Buffers are addressed by
+// ping-pong index; history slots by ring index.
+static size_t hslot_elems(const dns_handle *h) { return 2ull * 23 * h->d.ny * h->d.nx; }
+
+static void L_coarse(dns_handle *h, int src, int dst, bool sample, cudaStream_t st) {
+  if (is_f32(h))
+    launch_coarse_f32(F(h->fc[src]), F(h->fc[dst]), h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl,
+                      sample, st);
+  else
+    launch_coarse_f64(h->fc[src], h->fc[dst], h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl, sample,
+                      st);
+}
+static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
+  if (is_f32(h))
+    launch_extract_f32(F(h->fc[cbuf]), F(h->hist) + slot * hslot_elems(h), h->d, h->shape, st);
+  else
+    launch_extract_f64(h->fc[cbuf], h->hist + slot * hslot_elems(h), h->d, h->shape, st);
+}
+static void L_fine(dns_handle *h, int src, int dst, bool first, bool last, bool stats, cudaStream_t st) {
+  if (is_f32(h))
+    launch_fine_f32(F(h->ff[src]), F(h->ff[dst]), h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials,
+                    h->pl, first, last, stats, st);
+  else
+    launch_fine_f64(h->ff[src], h->ff[dst], h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials, h->pl,
+                    first, last, stats, st);
+}
+static void L_iface(dns_handle *h, int fbuf, int it, cudaStream_t st) {
+  const size_t hs = hslot_elems(h);
+  if (is_f32(h)) {
+    float *H = F(h->hist);
+    launch_interface_f32(H + h->hn * hs, H + h->hp * hs, H + h->hpp * hs, F(h->iface_mac), F(h->ff[fbuf]), h->d, it,
+                         h->g.omega_c, h->g.omega_f, st);
+  } else {
+    launch_interface_f64(h->hist + h->hn * hs, h->hist + h->hp * hs, h->hist + h->hpp * hs, h->iface_mac,
+                         h->ff[fbuf], h->d, h->shape, it, h->g.omega_c, h->g.omega_f, st);
+  }
+}
+static void L_inject(dns_handle *h, int fbuf, int cbuf, cudaStream_t st) {
+  if (is_f32(h))
+    launch_inject_f32(F(h->ff[fbuf]), F(h->fc[cbuf]), h->d, h->shape, h->g.omega_c, h->g.omega_f, h->partials, h->pl,
+                      st);
+  else
+    launch_inject_f64(h->ff[fbuf], h->fc[cbuf], h->d, h->shape, h->g.omega_c, h->g.omega_f, h->partials, h->pl, st);
+}
+static void rotate_history(dns_handle *h) {
+  // the new level n takes the slot of pp (xcomputations.c:548-556)
+  const int t = h->hpp;
+  h->hpp = h->hp;
+  h->hp = h->hn;
+  h->hn = t;
+}
+
+// One coarse step on two (or three) streams.  The interface transfer of
+// substep s writes only the interface planes of the buffer whose other planes
+// the fine kernel of substep s writes, so the two run concurrently; the coarse
+// kernel and the extraction run beside the first fine substep.
+//   main:  coarse, extract, iface(1), [wait fine(s-1)] iface(s) ..., [wait inject] finalize
+//   aux:   [wait start] fine(1), [wait iface(s-1)] fine(s) ..., inject
+// Schedule (compile-time): 0 one stream in order, 1 interface transfers on the
+// main stream, 2 interface transfers on their own high-priority stream.
 #ifndef DNS_SCHED
 #define DNS_SCHED 1
 #endif
 static void issue_step_overlapped(dns_handle *h, DevLog *log_row, bool sample) {
   const Dims &d = h->d;
-  const LaunchShape &s = h->shape;
   cudaStream_t S = h->stream, T = h->aux, H = DNS_SCHED == 2 ? h->hip : h->stream;
   const int nc = 1 - h->cur_c;
   cudaEventRecord(h->ev_start, S);
   cudaStreamWaitEvent(T, h->ev_start, 0);
-  launch_coarse_f64(h->fc[h->cur_c], h->fc[nc], d, s, h->g.omega_c, h->state, h->partials, h->pl, sample, S);
-  const int t = h->hpp;
-  h->hpp = h->hp;
-  h->hp = h->hn;
-  h->hn = t;
-  const size_t hslot = 2ull * 23 * d.ny * d.nx;
-  launch_extract_f64(h->fc[nc], h->hist + h->hn * hslot, d, s, S);
+  L_coarse(h, h->cur_c, nc, sample, S);
+  rotate_history(h);
+  L_extract(h, nc, h->hn, S);
   cudaEventRecord(h->ev_ext, S);
   cudaStreamWaitEvent(H, h->ev_ext, 0);
   int cur = h->cur_f;
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - cur;
     if (it > 1) cudaStreamWaitEvent(T, h->ev_if[it - 2], 0);
-    launch_fine_f64(h->ff[cur], h->ff[nf], h->wflag, d, s, h->g.omega_f, h->state, h->partials, h->pl, it == 1,
-                    it == d.gr, sample && it == 1, T);
+    L_fine(h, cur, nf, it == 1, it == d.gr, sample && it == 1, T);
     cudaEventRecord(h->ev_fine[it - 1], T);
     if (it > 1) cudaStreamWaitEvent(H, h->ev_fine[it - 2], 0);
-    launch_interface_f64(h->hist + h->hn * hslot, h->hist + h->hp * hslot, h->hist + h->hpp * hslot, h->iface_mac,
-                         h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, H);
+    L_iface(h, nf, it, H);
     cudaEventRecord(h->ev_if[it - 1], H);
     cur = nf;
   }
-  launch_inject_f64(h->ff[cur], h->fc[nc], d, s, h->g.omega_c, h->g.omega_f, h->partials, h->pl, T);
+  L_inject(h, cur, nc, T);
   cudaEventRecord(h->ev_inj, T);
   cudaStreamWaitEvent(S, h->ev_inj, 0);
   cudaStreamWaitEvent(S, h->ev_if[d.gr - 1], 0);
-  launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, s, h->sp, S);
-  if (sample) launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, s, S);
+  launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, h->shape, h->sp, S);
+  if (sample) launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, h->shape, S);
   h->cur_f = cur;
   h->cur_c = nc;
 }
@@ -702,29 +830,19 @@ static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
     return;
   }
   const Dims &d = h->d;
-  const LaunchShape &s = h->shape;
   const int nc = 1 - h->cur_c;
-  PROFILED(h, 0, launch_coarse_f64(h->fc[h->cur_c], h->fc[nc], d, s, h->g.omega_c, h->state, h->partials, h->pl,
-                                   sample, h->stream));
-  // rotate history: the new level n takes the slot of pp (xcomputations.c:548-556)
-  const int t = h->hpp;
-  h->hpp = h->hp;
-  h->hp = h->hn;
-  h->hn = t;
-  const size_t hslot = 2ull * 23 * d.ny * d.nx;
-  PROFILED(h, 1, launch_extract_f64(h->fc[nc], h->hist + h->hn * hslot, d, s, h->stream));
+  PROFILED(h, 0, L_coarse(h, h->cur_c, nc, sample, h->stream));
+  rotate_history(h);
+  PROFILED(h, 1, L_extract(h, nc, h->hn, h->stream));
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - h->cur_f;
-    PROFILED(h, 2, launch_fine_f64(h->ff[h->cur_f], h->ff[nf], h->wflag, d, s, h->g.omega_f, h->state,
-                                   h->partials, h->pl, it == 1, it == d.gr, sample && it == 1, h->stream));
-    PROFILED(h, 3, launch_interface_f64(h->hist + h->hn * hslot, h->hist + h->hp * hslot, h->hist + h->hpp * hslot,
-                                        h->iface_mac, h->ff[nf], d, s, it, h->g.omega_c, h->g.omega_f, h->stream));
+    PROFILED(h, 2, L_fine(h, h->cur_f, nf, it == 1, it == d.gr, sample && it == 1, h->stream));
+    PROFILED(h, 3, L_iface(h, nf, it, h->stream));
     h->cur_f = nf;
   }
-  PROFILED(h, 4, launch_inject_f64(h->ff[h->cur_f], h->fc[nc], d, s, h->g.omega_c, h->g.omega_f, h->partials,
-                                   h->pl, h->stream));
-  PROFILED(h, 5, launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, s, h->sp, h->stream));
-  if (sample) PROFILED(h, 6, launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, s, h->stream));
+  PROFILED(h, 4, L_inject(h, h->cur_f, nc, h->stream));
+  PROFILED(h, 5, launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, h->shape, h->sp, h->stream));
+  if (sample) PROFILED(h, 6, launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, h->shape, h->stream));
   h->cur_c = nc;
 }
 

@@ -75,14 +75,19 @@ def emit(path: Path):
         "#pragma once",
         "#define DNS_BICUBIC_COEFFS(c, x) \\",
     ]
-    body = []
-    for r, row in enumerate(W):
-        terms = [f"({float(w)!r} * (x)[{k}])" for k, w in enumerate(row) if w != 0]
-        expr = terms[0]
-        for t in terms[1:]:
-            expr = f"({expr} + {t})"
-        body.append(f"  (c)[{r}] = {expr};")
-    lines.append(" \\\n".join(body))
+    def body(suffix):
+        out = []
+        for r, row in enumerate(W):
+            terms = [f"({float(w)!r}{suffix} * (x)[{k}])" for k, w in enumerate(row) if w != 0]
+            expr = terms[0]
+            for t in terms[1:]:
+                expr = f"({expr} + {t})"
+            out.append(f"  (c)[{r}] = {expr};")
+        return out
+    lines.append(" \\\n".join(body("")))
+    lines.append("// the same map for the FP32 form (float literals)")
+    lines.append("#define DNS_BICUBIC_COEFFS_F32(c, x) \\")
+    lines.append(" \\\n".join(body("f")))
     lines.append("")
     path.write_text("\n".join(lines))
 

@@ -57,6 +57,7 @@ struct StepParams {
   double ub;        // bulk velocity (constant flow rate target)
   double gconst;    // constant body force
   int cfr;          // 1: force = ub - momentum
+  double den_offset;  // encalc2 weight sum added to the mass partials (FP32 form: they sum deviations)
 };
 
 // --- FP64 kernels (kernels_f64.cu) ---
@@ -90,6 +91,11 @@ void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, doub
 long flow_sums_pairs(const Dims &d, const LaunchShape &s);
 void launch_flow_sums_scratch(const double *fc, const double *ff, DevState *out, double *scratch, const Dims &d,
                               const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
+// finalize a direct (flow_sums) reduction of npairs block partials into *st
+void finalize_flow_sums(DevState *st, const double *pairs, long npairs, const Dims &d, const LaunchShape &s,
+                        const StepParams &sp, cudaStream_t stream);
+// encalc2 weight of every node summed (the mass of a state with rho = 1)
+double encalc2_weight_sum(const Dims &d);
 void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
                      cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order
@@ -97,5 +103,27 @@ void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, in
                        int k0_aos, cudaStream_t stream);
 void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);
+
+// --- FP32 deviation-storage kernels (kernels_f32.cu); same layouts in float ---
+void launch_coarse_f32(const float *src, float *dst, const Dims &d, const LaunchShape &s, double om,
+                       const DevState *st, double *partials, const PartialLayout &pl, bool stats,
+                       cudaStream_t stream);
+void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream);
+void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
+                     double om, const DevState *st, double *partials, const PartialLayout &pl, bool first, bool last,
+                     bool stats, cudaStream_t stream);
+void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *mac, float *fdst, const Dims &d,
+                          int substep, double omega_c, double omega_f, cudaStream_t stream);
+void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,
+                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
+void launch_flow_sums_f32(const float *fc, const float *ff, DevState *st, double *partials, const PartialLayout &pl,
+                          const Dims &d, const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
+void launch_seed_f32(float *fc, float *ff, float *hist3, const Dims &d, uint64_t seed, double uc, double amp,
+                     cudaStream_t stream);
+// device float deviations <-> reference AoS doubles (f = w + d)
+void launch_dev_to_aos_f32(const float *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
+                           int k0_aos, cudaStream_t stream);
+void launch_aos_to_dev_f32(const double *aos, float *soa, int nx, int ny, int P, int p0, int np, int nz_aos,
+                           int k0_aos, cudaStream_t stream);
 
 }  // namespace dns

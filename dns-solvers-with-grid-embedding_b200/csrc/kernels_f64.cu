@@ -538,7 +538,7 @@ struct FinArgs {
   long nc, nf, ni;             // partial counts (pairs)
   long wb[6];                  // wall-shear plane block offsets (pairs), lower k=1,2,3 then upper zdf-2,-3,-4
   long wn;                     // blocks per plane
-  double g3, norm, norm2, mu, ub, gconst, pgrad_scale, flow_scale;
+  double g3, norm, norm2, mu, ub, gconst, pgrad_scale, flow_scale, den_offset;
   int cfr, with_log;
 };
 
@@ -571,7 +571,7 @@ __global__ void __launch_bounds__(kFinThreads) finalize_kernel(DevState *st, Dev
       *lg = r;
     }
     const double mom = (a.g3 * momc + 0.5 * a.g3 * momi + momf) / a.norm;
-    const double den = (a.g3 * denc + 0.5 * a.g3 * deni + denf) / a.norm;
+    const double den = (a.g3 * denc + 0.5 * a.g3 * deni + denf + a.den_offset) / a.norm;
     st->momentum = mom;
     st->denst = den;
     st->force = a.cfr ? a.ub - mom : a.gconst;
@@ -639,7 +639,7 @@ __global__ void __launch_bounds__(kFin2Threads) finalize2_kernel(DevState *st, D
     r.pgrad = st->force * a.pgrad_scale;
     *lg = r;
     const double mom = (a.g3 * S[0] + 0.5 * a.g3 * S[4] + S[2]) / a.norm;
-    const double den = (a.g3 * S[1] + 0.5 * a.g3 * S[5] + S[3]) / a.norm;
+    const double den = (a.g3 * S[1] + 0.5 * a.g3 * S[5] + S[3] + a.den_offset) / a.norm;
     st->momentum = mom;
     st->denst = den;
     st->force = a.cfr ? a.ub - mom : a.gconst;
@@ -920,6 +920,7 @@ static FinArgs fin_args(const PartialLayout &pl, const Dims &d, const LaunchShap
   a.pgrad_scale = (d.nzs - 2.) / (2. * d.gr);
   a.flow_scale = (double)((long)d.nyf * (d.nzs - 2));
   a.cfr = sp.cfr;
+  a.den_offset = sp.den_offset;
   a.with_log = 1;
   (void)pl;
   return a;
@@ -966,6 +967,25 @@ void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, doub
   // the fine path of finalize sums with weight 1: the kernel already applied
   // every encalc2 weight, so feed everything through the fine slot
   finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, nullptr, scratch, scratch, scratch, scratch, a);
+}
+
+void finalize_flow_sums(DevState *st, const double *pairs, long npairs, const Dims &d, const LaunchShape &s,
+                        const StepParams &sp, cudaStream_t stream) {
+  PartialLayout unused{};
+  FinArgs a = fin_args(unused, d, s, sp);
+  a.nc = 0;
+  a.ni = 0;
+  a.nf = npairs;
+  a.with_log = 0;
+  finalize_kernel<<<1, kFinThreads, 0, stream>>>(st, nullptr, pairs, pairs, pairs, pairs, a);
+}
+
+double encalc2_weight_sum(const Dims &d) {
+  const double g3 = (double)d.gr * d.gr * d.gr;
+  const double cplane = (double)d.nx * d.ny, fplane = (double)d.nxf * d.nyf;
+  // coarse: planes 1..zdc-2 weigh GR^3, planes 0 and zdc-1 half that;
+  // lower fine k in [1, zdf-GR); upper fine k in [GR, zdf-1) with k = GR halved
+  return g3 * cplane * (d.nzc - 1) + fplane * ((d.zdf - d.gr - 1) + (d.zdf - 2 - d.gr) + 0.5);
 }
 
 long flow_sums_pairs(const Dims &d, const LaunchShape &s) {
