@@ -65,6 +65,23 @@ class StepLog(C.Structure):
 
 LOG_FIELDS = tuple(n for n, _ in StepLog._fields_)
 
+
+class Tile(C.Structure):
+    """``dns_tile``: tile shape of one batched instance."""
+
+    _fields_ = [("cw", C.c_int), ("cjb", C.c_int), ("fw", C.c_int), ("fjb", C.c_int), ("igroups", C.c_int)]
+
+    def as_tuple(self):
+        return (self.cw, self.cjb, self.fw, self.fjb, self.igroups)
+
+
+class BatchInfo(C.Structure):
+    _fields_ = [
+        ("steps_done", C.c_longlong), ("remaining", C.c_longlong), ("status", C.c_int), ("slot", C.c_int),
+        ("force", C.c_double), ("flowrate", C.c_double), ("stress", C.c_double),
+        ("device_bytes", C.c_longlong), ("updates_per_step", C.c_longlong), ("tile", Tile),
+    ]
+
 _lib = None
 
 
@@ -99,6 +116,21 @@ def lib() -> C.CDLL:
         "dns_plane_stats": (I, [P, P]),
         "dns_set_profiling": (I, [P, I]),
         "dns_kernel_times": (I, [P, P, P]),
+        "dns_batch_create": (I, [I, C.POINTER(P)]),
+        "dns_batch_destroy": (None, [P]),
+        "dns_batch_footprint": (I, [C.POINTER(Params), C.POINTER(C.c_longlong)]),
+        "dns_batch_tile_for": (I, [P, C.POINTER(Params), C.POINTER(Tile)]),
+        "dns_batch_set_tile": (I, [P, C.POINTER(Params), C.POINTER(Tile)]),
+        "dns_batch_autotune": (I, [P, C.POINTER(Params), I, C.POINTER(Tile), C.POINTER(D)]),
+        "dns_batch_add": (I, [P, C.POINTER(Params), C.POINTER(Tile), C.c_uint64, D, D, C.c_longlong,
+                              C.c_longlong, C.POINTER(I)]),
+        "dns_batch_remove": (I, [P, I]),
+        "dns_batch_run": (I, [P, C.c_longlong, C.POINTER(I)]),
+        "dns_batch_info_of": (I, [P, I, C.POINTER(BatchInfo)]),
+        "dns_batch_stats": (I, [P, I, P, C.POINTER(C.c_long)]),
+        "dns_batch_export_state": (I, [P, I, I, P]),
+        "dns_batch_log": (I, [P, I, C.c_longlong, C.c_longlong, P]),
+        "dns_batch_stream": (I, [P, C.POINTER(P)]),
         "dns_error_string": (C.c_char_p, [I]),
         "dns_last_error": (C.c_char_p, []),
     }
@@ -250,3 +282,108 @@ class Channel:
         out = np.zeros((9, self.geom.nz_profile))
         _check(lib().dns_plane_stats(self.h, out.ctypes.data), "dns_plane_stats")
         return out
+
+
+def batch_footprint(p: Params) -> int:
+    """Device bytes one batched (FP32) instance of these parameters holds."""
+    b = C.c_longlong()
+    _check(lib().dns_batch_footprint(C.byref(p), C.byref(b)), "dns_batch_footprint")
+    return b.value
+
+
+class Batch:
+    """Many independent channels stepped together in the FP32 form (a ``dns_batch``).
+
+    ``add`` makes a seeded instance with its own step budget and returns its
+    id; ``run(n)`` advances every instance with budget left by up to n coarse
+    steps (captured CUDA graphs of persistent kernels over a per-instance
+    block table); results stay on the device until read or removed.
+    """
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().dns_batch_create(device, C.byref(h)), "dns_batch_create")
+        self.h = h
+        self.geoms = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().dns_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().dns_batch_stream(self.h, C.byref(s)), "dns_batch_stream")
+        return s.value or 0
+
+    def tile_for(self, p: Params) -> Tile:
+        t = Tile()
+        _check(lib().dns_batch_tile_for(self.h, C.byref(p), C.byref(t)), "dns_batch_tile_for")
+        return t
+
+    def set_tile(self, p: Params, tile):
+        t = tile if isinstance(tile, Tile) else Tile(*tile)
+        _check(lib().dns_batch_set_tile(self.h, C.byref(p), C.byref(t)), "dns_batch_set_tile")
+
+    def autotune(self, p: Params, steps: int = 10):
+        """Time tile shapes for this grid shape; returns (tile tuple, ms per step)."""
+        t, ms = Tile(), C.c_double()
+        _check(lib().dns_batch_autotune(self.h, C.byref(p), steps, C.byref(t), C.byref(ms)), "dns_batch_autotune")
+        return t.as_tuple(), ms.value
+
+    def add(self, p: Params, steps: int, seed: int = 42, uc: float = 0.05, amp: float = 0.005,
+            sample_every: int = 0, tile=None) -> int:
+        i = C.c_int()
+        t = None if tile is None else C.byref(tile if isinstance(tile, Tile) else Tile(*tile))
+        _check(lib().dns_batch_add(self.h, C.byref(p), t, seed, uc, amp, steps, sample_every, C.byref(i)),
+               "dns_batch_add")
+        q = Params.from_buffer_copy(p)
+        q.precision = FP32
+        self.geoms[i.value] = geometry(q)
+        return i.value
+
+    def remove(self, i: int):
+        _check(lib().dns_batch_remove(self.h, i), "dns_batch_remove")
+        self.geoms.pop(i, None)
+
+    def run(self, n: int) -> int:
+        """Advance up to n steps; returns the number of instances with budget left."""
+        a = C.c_int()
+        _check(lib().dns_batch_run(self.h, n, C.byref(a)), "dns_batch_run")
+        return a.value
+
+    def info(self, i: int) -> BatchInfo:
+        out = BatchInfo()
+        _check(lib().dns_batch_info_of(self.h, i, C.byref(out)), "dns_batch_info_of")
+        return out
+
+    def stats(self, i: int):
+        nz = self.geoms[i].nz_profile
+        out = np.zeros((NSTAT, nz))
+        ns = C.c_long()
+        _check(lib().dns_batch_stats(self.h, i, out.ctypes.data, C.byref(ns)), "dns_batch_stats")
+        return out, ns.value
+
+    def export_state(self, i: int, level: int) -> np.ndarray:
+        g = self.geoms[i]
+        shape = (g.nx, g.ny, g.nzc, 19) if level == 0 else (g.nxf, g.nyf, g.zdf, 19)
+        out = np.empty(shape, dtype=np.float64)
+        _check(lib().dns_batch_export_state(self.h, i, level, out.ctypes.data), "dns_batch_export_state")
+        return out
+
+    def log(self, i: int, first: int = 0, n: int | None = None) -> np.ndarray:
+        if n is None:
+            n = self.info(i).steps_done - first
+        buf = (StepLog * max(n, 1))()
+        _check(lib().dns_batch_log(self.h, i, first, n, buf), "dns_batch_log")
+        return np.frombuffer(buf, dtype=np.float64).reshape(-1, len(LOG_FIELDS))[:n].copy()

@@ -22,7 +22,9 @@ COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", str(INC
 UNITS = {  # source -> extra flags
     "kernels_f64.cu": ["-fmad=false"],
     "kernels_f32.cu": [],
+    "batch_f32.cu": [],
     "dns_api.cu": [],
+    "batch_api.cu": [],
     "noalloc.cu": [],
 }
 

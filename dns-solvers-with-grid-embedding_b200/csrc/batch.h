@@ -1,0 +1,99 @@
+// Batched FP32 engine: many independent channels stepped by one set of
+// persistent kernels over a per-instance block table (internal to
+// libdnsembed; the C ABI is dns_batch_* in include/dns_embed.h).
+//
+// Every phase of the coarse step (statistics, coarse collide-stream, plane
+// extraction, fine substeps, interface transfer, injection, finalize) is one
+// persistent kernel: a grid sized to the machine walks the phase's work items
+// of all resident instances.  Instance s owns items [start[ph][s],
+// start[ph][s+1]); an item is one tile of one instance, decoded against that
+// instance's own sizes and tile shape.  Everything a step needs that changes
+// from step to step (ping-pong parity, history ring, step count, remaining
+// budget) lives in device memory and is advanced by the finalize kernel, so a
+// captured CUDA graph of a step group replays unchanged while instances join
+// and leave (only the tables it reads are rewritten between groups).
+#pragma once
+
+#include <cstdint>
+
+#include <cuda_runtime.h>
+
+#include "kernels.h"
+
+namespace dns {
+namespace batch {
+
+constexpr int kMaxInst = 1024;  // resident instances per batch
+constexpr int kLogRows = 64;    // per-instance log ring (>= steps per graph replay)
+
+enum Phase {
+  PH_STATS = 0,  // plane statistics of the sampled state (coarse 2..zdc-3, every fine plane)
+  PH_SFINAL,     // per-plane accumulation of those sums
+  PH_CBULK,      // coarse planes 2..zdc-3
+  PH_CEDGE,      // coarse planes 0, 1, zdc-2, zdc-1
+  PH_EXTRACT,    // interface history planes k = 1 and zdc-2
+  PH_FBULK,      // fine planes k = 2..zdf-3 of both blocks
+  PH_FEDGE,      // the remaining fine planes
+  PH_IFACE,      // interface transfer tiles x walls x population groups
+  PH_INJECT,     // fine-to-coarse injection rows
+  PH_NPHASE
+};
+
+// Constant while the instance is resident.
+struct Inst {
+  int nx, ny, nzc, nxf, nyf, zdf, zds, gr;
+  int cw, cjb, cgx, cgy;  // coarse tile: width (threads in x), row iterations, grid per plane
+  int fw, fjb, fgx, fgy;  // fine tile
+  int igx, igy, igroups;  // interface tiles and population groups
+  int egx;                // extraction / injection blocks per row
+  int nzp;                // composite profile planes
+  int slot;               // row of the batch-level dyn / state / log arrays
+  long long sample_every; // statistics every n steps of the instance (0: none)
+  float om_c, om_f, fac_if, fac_inj;
+  // finalize constants (encalc2.c, wshearstr.c)
+  double g3, norm, norm2, mu, ub, gconst, pgrad_scale, flow_scale, den_offset;
+  int cfr, pad;
+  float *fc[2], *ff[2];   // coarse / fine SoA deviations, ping-pong
+  float *hist;            // 3 ring slots x [2 walls][23][ny][nx]
+  int8_t *wflag;          // [nyf][nxf]
+  double *part;           // block partials
+  long long pc, pf, pi, pw, psc, psf;  // region offsets (doubles) in part
+  double *stats;          // [nzp][16] running sums
+};
+
+// Advanced on the device by the finalize kernel.
+struct Dyn {
+  int cc, cf;             // coarse / fine buffer holding the post-stream state
+  int hn, hp, hpp;        // history ring slots of levels n, p, pp
+  int pad;
+  long long step;         // coarse steps done
+  long long remaining;    // steps left in the budget
+};
+
+struct Mix {
+  int n;                  // resident instances (entries of inst)
+  int pad[3];
+  int start[PH_NPHASE][kMaxInst + 1];
+  Inst inst[kMaxInst];
+};
+
+// Hermite-in-time weights of one substep (same for every instance of a batch)
+struct TimeW {
+  float an, ap, app;
+};
+
+// Interface tile (coarse cells) per refinement ratio: IfTile<GR> of f32_core.cuh.
+constexpr int iface_tx(int gr) { return gr == 2 ? 32 : (gr == 3 ? 21 : 16); }
+constexpr int iface_ty(int gr) { return gr == 2 ? 8 : (gr == 3 ? 6 : 4); }
+
+// Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
+struct Grids {
+  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, iface, inject, final_;
+};
+int query_grids(int gr, Grids *g);
+void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, int gr, const Grids &g, cudaStream_t s,
+                 cudaStream_t aux, cudaEvent_t *ev);  // ev: 10 events (fork/join of the two streams)
+void tile_counts(const Inst &I, int counts[PH_NPHASE]);
+
+}  // namespace batch
+}  // namespace dns

@@ -1,0 +1,592 @@
+// Persistent kernels of the batched FP32 engine (see batch.h).  The node
+// arithmetic is f32_core.cuh's, shared with the single-channel form; what is
+// new here is the work decomposition: each kernel walks a table of work items
+// across all resident instances, and each instance's reductions land in its
+// own partial arrays in an order fixed by its own tiling, so an instance's
+// trajectory does not depend on which other instances share the batch.
+#include "batch.h"
+#include "f32_core.cuh"
+#include "kernels.h"
+#include "lattice.cuh"
+
+namespace dns {
+namespace batch {
+
+namespace {
+
+using namespace f32;
+
+static_assert(IfTile<2>::TX == iface_tx(2) && IfTile<2>::TY == iface_ty(2) && IfTile<3>::TX == iface_tx(3) &&
+                  IfTile<3>::TY == iface_ty(3) && IfTile<4>::TX == iface_tx(4) && IfTile<4>::TY == iface_ty(4),
+              "host and device interface tiles");
+
+// advance s to the instance owning item w (items are walked in increasing order)
+__device__ __forceinline__ int owner(const int *__restrict__ st, int n, int w, int s) {
+  while (s < n && __ldg(st + s + 1) <= w) s++;
+  return s;
+}
+
+__device__ __forceinline__ int log2i(int v) { return 31 - __clz(v); }
+
+// the item this block would take after leaving instance s's range: the
+// smallest w' >= end with w' = w (mod stride), minus one stride (the loop adds it)
+__device__ __forceinline__ int past(int w, int end, int stride) {
+  return w >= end ? w - stride : w + ((end - w + stride - 1) / stride) * stride - stride;
+}
+
+__device__ __forceinline__ bool sampling(const Inst &I, const Dyn &D) {
+  return D.remaining > 0 && I.sample_every > 0 && D.step % I.sample_every == 0;
+}
+
+__device__ __forceinline__ Dims dims_of(const Inst &I) {
+  return Dims{I.nx, I.ny, I.nzc, I.nxf, I.nyf, I.zdf, I.zds, I.gr, 0};
+}
+
+__device__ __forceinline__ void stat_acc(const float (&f)[19], double (&sacc)[9]) {
+  const Mac32 m = macro_f32(f);
+  const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+  sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+  sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+}
+
+// ------------------------------------------------------------------ statistics
+// Sums of the state at the start of the step (the state the single-channel
+// form samples inside its coarse kernel and first fine substep).
+__global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
+  const int n = M->n;
+  const int *st = M->start[PH_STATS];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (!sampling(I, D)) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    int local = w - st[s];
+    const int ncs = (I.nzc - 4) * I.cgy * I.cgx;
+    const bool coarse = local < ncs;
+    if (!coarse) local -= ncs;
+    const int W = coarse ? I.cw : I.fw, jb = coarse ? I.cjb : I.fjb;
+    const int gx = coarse ? I.cgx : I.fgx, gy = coarse ? I.cgy : I.fgy;
+    const int nx = coarse ? I.nx : I.nxf, ny = coarse ? I.ny : I.nyf;
+    const int z = local / (gx * gy), rem = local - z * gx * gy, by = rem / gx, bx = rem - by * gx;
+    const int p = coarse ? z + 2 : z;  // coarse plane k, or fine device plane
+    const int lw = log2i(W), tx = threadIdx.x & (W - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
+    const int i = bx * W + tx;
+    const float *src = coarse ? I.fc[D.cc] : I.ff[D.cf];
+    const size_t pstride = coarse ? (size_t)I.nzc * I.ny * I.nx : (size_t)2 * I.zds * I.nyf * I.nxf;
+    double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+    for (int r = 0; r < jb; r++) {
+      const int j = (by * jb + r) * R + ty;
+      if (i >= nx || j >= ny) continue;
+      float f[19];
+      load19f(src, ((size_t)p * ny + j) * nx + i, pstride, f);
+      stat_acc(f, sacc);
+    }
+    const size_t blk = ((size_t)p * gy + by) * gx + bx;
+    block_reduce32<9>(sacc, I.part + (coarse ? I.psc : I.psf) + blk * 9);
+  }
+}
+
+// per composite-profile plane: sum the plane's block partials (fixed order) and
+// add the sample into the running sums (layout of the single-channel form:
+// 0..8 plane sums, 9..13 per-sample plane variances, 14 nodes, 15 samples)
+__global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
+  __shared__ double sh[9][kThreads];
+  const int n = M->n;
+  const int *st = M->start[PH_SFINAL];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (!sampling(I, D)) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int idx = w - st[s];
+    const int zdf = I.zdf, nzc = I.nzc;
+    const double *src = nullptr;
+    long nb = 0;
+    double nn = 0.;
+    const long bc = (long)I.cgx * I.cgy, bf = (long)I.fgx * I.fgy;
+    if (idx >= 1 && idx <= zdf - 1) {  // lower fine k = idx (device plane idx - 1)
+      src = I.part + I.psf + (size_t)(idx - 1) * bf * 9; nb = bf; nn = (double)I.nxf * I.nyf;
+    } else if (idx >= zdf && idx <= zdf + nzc - 5) {  // coarse k = idx - zdf + 2
+      src = I.part + I.psc + (size_t)(idx - zdf + 2) * bc * 9; nb = bc; nn = (double)I.nx * I.ny;
+    } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {  // upper fine k
+      const int k = idx - (zdf + nzc - 4);
+      src = I.part + I.psf + (size_t)(I.zds + k) * bf * 9; nb = bf; nn = (double)I.nxf * I.nyf;
+    }
+    if (!src) continue;
+#pragma unroll
+    for (int c = 0; c < 9; c++) {
+      double a = 0.;
+      for (long q = threadIdx.x; q < nb; q += blockDim.x) a += src[q * 9 + c];
+      sh[c][threadIdx.x] = a;
+    }
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o)
+#pragma unroll
+        for (int c = 0; c < 9; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      double *o = I.stats + (size_t)idx * 16;
+      double s9[9];
+      for (int c = 0; c < 9; c++) s9[c] = sh[c][0];
+      for (int c = 0; c < 9; c++) o[c] += s9[c];
+      const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
+      o[9] += s9[4] / nn - mu * mu;
+      o[10] += s9[5] / nn - mv * mv;
+      o[11] += s9[6] / nn - mw * mw;
+      o[12] += s9[7] / nn - mu * mw;
+      o[13] += s9[8] / nn - mr * mr;
+      o[14] = nn;
+      o[15] += 1.0;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------------------------ coarse
+template <bool BULK>
+__global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
+    b_coarse(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state) {
+  const int n = M->n;
+  const int *st = M->start[BULK ? PH_CBULK : PH_CEDGE];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int local = w - st[s];
+    const int gxy = I.cgx * I.cgy;
+    const int z = local / gxy, rem = local - z * gxy, by = rem / I.cgx, bx = rem - by * I.cgx;
+    const int k = BULK ? 2 + z : (z < 2 ? z : I.nzc - 4 + z);
+    const int lw = log2i(I.cw), tx = threadIdx.x & (I.cw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
+    const int i = bx * I.cw + tx;
+    const Dims d = dims_of(I);
+    const size_t pstride = (size_t)I.nzc * I.ny * I.nx;
+    const float *src = I.fc[D.cc];
+    float *dst = I.fc[D.cc ^ 1];
+    const float om = I.om_c, G = (float)state[I.slot].force;
+    double acc[2] = {0., 0.};
+    double sacc[9];
+    for (int r = 0; r < I.cjb; r++) {
+      const int j = (by * I.cjb + r) * R + ty;
+      if (i >= I.nx || j >= I.ny) continue;
+      float fa[19];
+      const size_t idx0 = ((size_t)k * I.ny + j) * I.nx + i;
+      load19f(src, idx0, pstride, fa);
+      if (BULK)
+        coarse_bulk_f32<false>(fa, i, j, idx0, d, om, G, dst, pstride, acc, sacc);
+      else
+        coarse_node_f32<false>(fa, i, j, k, d, om, G, dst, pstride, acc, sacc);
+    }
+    const size_t blk = ((size_t)k * I.cgy + by) * I.cgx + bx;
+    block_reduce32<2>(acc, I.part + I.pc + blk * 2);
+  }
+}
+
+// ------------------------------------------------------------------ extraction
+// new history level n (ring slot of the old pp) from the coarse state just streamed
+__global__ void __launch_bounds__(kThreads) b_extract(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
+  const int n = M->n;
+  const int *st = M->start[PH_EXTRACT];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int local = w - st[s];
+    const int row = local / I.egx, bx = local - row * I.egx;
+    const int wall = row / I.ny, j = row - wall * I.ny;
+    const int i = bx * kThreads + threadIdx.x;
+    if (i >= I.nx) continue;
+    const int k = wall == 0 ? 1 : I.nzc - 2;
+    const size_t pstride = (size_t)I.nzc * I.ny * I.nx, plane = (size_t)I.ny * I.nx;
+    float f[19];
+    load19f(I.fc[D.cc ^ 1], ((size_t)k * I.ny + j) * I.nx + i, pstride, f);
+    const Mac32 m = macro_f32(f);
+    float *o = I.hist + (size_t)D.hpp * 2 * 23 * plane + (size_t)wall * 23 * plane + (size_t)j * I.nx + i;
+    o[0] = m.drho;
+    o[plane] = m.u0;
+    o[2 * plane] = m.u1;
+    o[3 * plane] = m.u2;
+#pragma unroll
+    for (int a = 0; a < 19; a++) o[(size_t)(4 + a) * plane] = f[a] - deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+  }
+}
+
+// ------------------------------------------------------------------ fine
+__device__ __forceinline__ int fine_plane(bool bulk, int q, int zds) {
+  if (bulk) return q < zds - 3 ? q + 1 : zds + 2 + (q - (zds - 3));
+  // edge planes: lower k = 1, zdf-2, zdf-1; upper k = 0, 1, zdf-2
+  return q < 3 ? (q == 0 ? 0 : zds - 3 + q) : (q < 5 ? zds + (q - 3) : 2 * zds - 1);
+}
+
+template <int MODE, bool BULK>
+__global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
+    b_fine(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state, int sub) {
+  const int n = M->n;
+  const int *st = M->start[BULK ? PH_FBULK : PH_FEDGE];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int local = w - st[s];
+    const int gxy = I.fgx * I.fgy;
+    const int q = local / gxy, rem = local - q * gxy, by = rem / I.fgx, bx = rem - by * I.fgx;
+    const int zds = I.zds, zdf = I.zdf, gr = I.gr;
+    const int p = fine_plane(BULK, q, zds);
+    const bool upper = p >= zds;
+    const int k = upper ? p - zds : p + 1;
+    const int kwall = upper ? zdf - 1 : 0;
+    const int lw = log2i(I.fw), tx = threadIdx.x & (I.fw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
+    const int i = bx * I.fw + tx;
+    const Dims d = dims_of(I);
+    const size_t pstride = (size_t)2 * zds * I.nyf * I.nxf;
+    const float *src = I.ff[D.cf ^ ((sub - 1) & 1)];
+    float *dst = I.ff[D.cf ^ (sub & 1)];
+    const float om = I.om_f, Gf = (float)((1. / (double)gr) * state[I.slot].force);
+    const bool wall_sum_plane =
+        upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
+    const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
+    double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
+    double sacc[9];
+    float wz[3] = {0.f, 0.f, 0.f};
+    if (BULK) {
+#pragma unroll
+      for (int c = 0; c < 3; c++) {
+        const int kd = k + c - 1;
+        wz[c] = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
+                       : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
+      }
+    }
+    for (int r = 0; r < I.fjb; r++) {
+      const int j = (by * I.fjb + r) * R + ty;
+      if (i >= I.nxf || j >= I.nyf) continue;
+      float fa[19];
+      const size_t idx0 = ((size_t)p * I.nyf + j) * I.nxf + i;
+      load19f(src, idx0, pstride, fa);
+      if (BULK)
+        fine_bulk_f32<MODE>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc, wacc,
+                            sacc);
+      else
+        fine_node_f32<MODE>(fa, i, j, p, k, upper, kwall, d, om, Gf, I.wflag, dst, pstride, wall_sum_plane,
+                            wall_rho_plane, acc, wacc, sacc);
+    }
+    const size_t blk = ((size_t)p * I.fgy + by) * I.fgx + bx;
+    if (MODE & 1) block_reduce32<2>(acc, I.part + I.pf + blk * 2);
+    if ((MODE & 2) && wall_sum_plane) block_reduce32<2>(wacc, I.part + I.pw + blk * 2);
+  }
+}
+
+// ------------------------------------------------------------------ interface
+template <int GR>
+__global__ void __launch_bounds__(kThreads) b_iface(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
+                                                    TimeW tw) {
+  __shared__ IfSmem32<GR> S;
+  const int n = M->n;
+  const int *st = M->start[PH_IFACE];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    int local = w - st[s];
+    const int tx = local % I.igx;
+    local /= I.igx;
+    const int ty = local % I.igy;
+    local /= I.igy;
+    const int G = I.igroups, g = local % G, wall = local / G;
+    const size_t hs = (size_t)2 * 23 * I.ny * I.nx;
+    IfParams32 P;
+    // ring after this step's rotation: n in the old pp slot, p in old n, pp in old p
+    P.hn = I.hist + (size_t)D.hpp * hs;
+    P.hp = I.hist + (size_t)D.hn * hs;
+    P.hpp = I.hist + (size_t)D.hp * hs;
+    P.fdst = I.ff[D.cf ^ (sub & 1)];
+    P.nx = I.nx;
+    P.ny = I.ny;
+    P.nxf = I.nxf;
+    P.nyf = I.nyf;
+    P.zds = I.zds;
+    P.an = tw.an;
+    P.ap = tw.ap;
+    P.app = tw.app;
+    P.fac = I.fac_if;
+    iface_tile32<GR>(S, P, tx, ty, wall, 19 * g / G, 19 * (g + 1) / G);
+  }
+}
+
+// ------------------------------------------------------------------ injection
+__global__ void __launch_bounds__(kThreads) b_inject(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
+  const int n = M->n;
+  const int *st = M->start[PH_INJECT];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int local = w - st[s];
+    const int row = local / I.egx, bx = local - row * I.egx;
+    const int wall = row / I.ny, jc = row - wall * I.ny;
+    const int ic = bx * kThreads + threadIdx.x;
+    const int gr = I.gr, zdf = I.zdf, zds = I.zds, nx = I.nx, ny = I.ny, nzc = I.nzc;
+    double acc[2] = {0., 0.};
+    if (ic < nx) {
+      const int ps = wall == 0 ? (zdf - 1 - gr) - 1 : zds + gr;
+      const size_t fstride = (size_t)2 * zds * I.nyf * I.nxf;
+      float f[19];
+      load19f(I.ff[D.cf ^ (gr & 1)], ((size_t)ps * I.nyf + (size_t)jc * gr) * I.nxf + (size_t)ic * gr, fstride, f);
+      const Mac32 m = macro_f32(f);
+      const int kc = wall == 0 ? 0 : nzc - 1;
+      const size_t cstride = (size_t)nzc * ny * nx;
+      float *cdst = I.fc[D.cc ^ 1];
+      float mom = 0.f, den = 0.f;
+#pragma unroll
+      for (int a = 0; a < 19; a++) {
+        const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+        const float fn = deq + I.fac_inj * (f[a] - deq);
+        cdst[(size_t)a * cstride + ((size_t)kc * ny + jc) * nx + ic] = fn;
+        den += fn;
+        if (ex_of(a) > 0) mom += fn;
+        if (ex_of(a) < 0) mom -= fn;
+      }
+      acc[0] = mom;
+      acc[1] = den;
+    }
+    block_reduce32<2>(acc, I.part + I.pi + (size_t)local * 2);
+  }
+}
+
+// ------------------------------------------------------------------ finalize
+// One block per instance: the instance's block partials in a fixed order ->
+// log row, encalc2 values and force of the next step; then the step's
+// parity, history ring and counters advance.
+constexpr int kFinComp = 18;
+
+__global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, Dyn *__restrict__ dyn,
+                                                   DevState *__restrict__ state, DevLog *__restrict__ log) {
+  __shared__ double sh[kFinComp][kThreads];
+  const int n = M->n;
+  for (int s = blockIdx.x; s < n; s += gridDim.x) {
+    const Inst &I = M->inst[s];
+    Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) continue;
+    double v[kFinComp];
+#pragma unroll
+    for (int c = 0; c < kFinComp; c++) v[c] = 0.;
+    const long nc = (long)I.nzc * I.cgy * I.cgx, nf = (long)2 * I.zds * I.fgy * I.fgx;
+    const long ni = (long)2 * I.ny * I.egx, wn = (long)I.fgy * I.fgx;
+    const double *P = I.part;
+    for (long q = threadIdx.x; q < nc; q += kThreads) {
+      v[0] += P[I.pc + q * 2];
+      v[1] += P[I.pc + q * 2 + 1];
+    }
+    for (long q = threadIdx.x; q < nf; q += kThreads) {
+      v[2] += P[I.pf + q * 2];
+      v[3] += P[I.pf + q * 2 + 1];
+    }
+    for (long q = threadIdx.x; q < ni; q += kThreads) {
+      v[4] += P[I.pi + q * 2];
+      v[5] += P[I.pi + q * 2 + 1];
+    }
+    const int zds = I.zds, zdf = I.zdf;
+    const int planes[6] = {0, 1, 2, zds + zdf - 2, zds + zdf - 3, zds + zdf - 4};
+#pragma unroll
+    for (int c = 0; c < 6; c++) {
+      const double *pw = P + I.pw + (size_t)planes[c] * wn * 2;
+      for (long q = threadIdx.x; q < wn; q += kThreads) {
+        v[6 + 2 * c] += pw[q * 2];
+        v[7 + 2 * c] += pw[q * 2 + 1];
+      }
+    }
+#pragma unroll
+    for (int c = 0; c < kFinComp; c++) sh[c][threadIdx.x] = v[c];
+    __syncthreads();
+    for (int o = kThreads / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o)
+#pragma unroll
+        for (int c = 0; c < kFinComp; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + o];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      double S[kFinComp];
+      for (int c = 0; c < kFinComp; c++) S[c] = sh[c][0];
+      DevState &X = state[I.slot];
+      DevLog r;
+      r.force = X.force;
+      r.momentum = X.momentum;
+      r.denst = X.denst;
+      r.flowrate = X.momentum * I.flow_scale / X.denst;
+      const double *U = S + 6;  // (U, D) per plane: lower k = 1, 2, 3; upper zdf-2, zdf-3, zdf-4
+      const double stdown = ((-2. * U[0] + 3. * U[2] - U[4]) / I.norm2) * (I.mu * (U[1] / I.norm2));
+      const double stup = (-(2. * U[6] - 3. * U[8] + U[10]) / I.norm2) * (I.mu * (U[11] / I.norm2));
+      r.stup = stup;
+      r.stdown = stdown;
+      r.stress = 0.5 * (stup + stdown);
+      r.pgrad = X.force * I.pgrad_scale;
+      log[(size_t)I.slot * kLogRows + (size_t)(D.step % kLogRows)] = r;
+      const double mom = (I.g3 * S[0] + 0.5 * I.g3 * S[4] + S[2]) / I.norm;
+      const double den = (I.g3 * S[1] + 0.5 * I.g3 * S[5] + S[3] + I.den_offset) / I.norm;
+      X.momentum = mom;
+      X.denst = den;
+      X.force = I.cfr ? I.ub - mom : I.gconst;
+      // xcomputations.c:548-556 (history rotation); exchange.c / fexchange.c (pointer swaps)
+      const int t = D.hpp;
+      D.hpp = D.hp;
+      D.hp = D.hn;
+      D.hn = t;
+      D.cc ^= 1;
+      D.cf ^= (I.gr & 1);
+      D.step += 1;
+      D.remaining -= 1;
+      dyn[I.slot] = D;
+    }
+    __syncthreads();
+  }
+}
+
+template <class K>
+int occupancy_grid(K kernel, int *grid) {
+  int dev = 0, sms = 0, per = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return -1;
+  if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0) != cudaSuccess) return -1;
+  *grid = sms * (per > 0 ? per : 1);
+  return 0;
+}
+
+}  // namespace
+
+void tile_counts(const Inst &I, int c[PH_NPHASE]) {
+  const int cb = I.cgx * I.cgy, fb = I.fgx * I.fgy;
+  c[PH_STATS] = (I.nzc - 4) * cb + 2 * I.zds * fb;
+  c[PH_SFINAL] = I.nzp;
+  c[PH_CBULK] = (I.nzc - 4) * cb;
+  c[PH_CEDGE] = 4 * cb;
+  c[PH_EXTRACT] = 2 * I.ny * I.egx;
+  c[PH_FBULK] = 2 * (I.zds - 3) * fb;
+  c[PH_FEDGE] = 6 * fb;
+  c[PH_IFACE] = 2 * I.igroups * I.igx * I.igy;
+  c[PH_INJECT] = 2 * I.ny * I.egx;
+}
+
+int query_grids(int gr, Grids *g) {
+  int rc = 0;
+  rc |= occupancy_grid(b_stats, &g->stats);
+  rc |= occupancy_grid(b_sfinal, &g->sfinal);
+  rc |= occupancy_grid(b_coarse<true>, &g->cbulk);
+  rc |= occupancy_grid(b_coarse<false>, &g->cedge);
+  rc |= occupancy_grid(b_extract, &g->extract);
+  rc |= occupancy_grid(b_fine<1, true>, &g->fbulk);
+  rc |= occupancy_grid(b_fine<3, false>, &g->fedge);
+  if (gr == 2) rc |= occupancy_grid(b_iface<2>, &g->iface);
+  else if (gr == 3) rc |= occupancy_grid(b_iface<3>, &g->iface);
+  else rc |= occupancy_grid(b_iface<4>, &g->iface);
+  rc |= occupancy_grid(b_inject, &g->inject);
+  rc |= occupancy_grid(b_final, &g->final_);
+  return rc;
+}
+
+static void launch_fine(const Mix *m, Dyn *dyn, DevState *state, int mode, int sub, const Grids &g,
+                        cudaStream_t s) {
+  switch (mode) {
+    case 0:
+      b_fine<0, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
+      b_fine<0, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
+      break;
+    case 1:
+      b_fine<1, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
+      b_fine<1, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
+      break;
+    case 2:
+      b_fine<2, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
+      b_fine<2, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
+      break;
+    default:
+      b_fine<3, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
+      b_fine<3, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
+      break;
+  }
+}
+
+static TimeW time_weights(int sub, int gr) {
+  const double t = (double)sub / (double)gr, t2 = t * t, t3 = t2 * t;
+  const double h1 = 2. * t3 - 3. * t2 + 1., h2 = t3 - 2. * t2 + t, h3 = -2. * t3 + 3. * t2, h4 = t3 - t2;
+  return TimeW{(float)(0.5 * h2 + h3 + 1.5 * h4), (float)(h1 - 2. * h4), (float)(-0.5 * h2 + 0.5 * h4)};
+}
+
+static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, cudaStream_t s) {
+  const TimeW tw = time_weights(sub, gr);
+  if (gr == 2) b_iface<2><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else if (gr == 3) b_iface<3><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else b_iface<4><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
+}
+
+// One coarse step of every resident instance on two streams, with the
+// dependency structure of the single-channel schedule:
+//   s:   stats, sfinal, coarse, extract, iface(1), [fine(1)] iface(2) ..., [inject] final
+//   aux: [start] fine(1), [iface(1)] fine(2) ..., inject
+// The statistics read the state fine(2) and iface(2) overwrite; both follow
+// iface(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject.
+void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, int gr, const Grids &g, cudaStream_t s,
+                 cudaStream_t aux, cudaEvent_t *ev) {
+  cudaEventRecord(ev[0], s);
+  cudaStreamWaitEvent(aux, ev[0], 0);
+  b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
+  b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
+  b_coarse<true><<<g.cbulk, kThreads, 0, s>>>(m, dyn, state);
+  b_coarse<false><<<g.cedge, kThreads, 0, s>>>(m, dyn, state);
+  b_extract<<<g.extract, kThreads, 0, s>>>(m, dyn);
+  for (int sub = 1; sub <= gr; sub++) {
+    const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);
+    if (sub > 1) cudaStreamWaitEvent(aux, ev[5 + sub - 2], 0);
+    launch_fine(m, dyn, state, mode, sub, g, aux);
+    cudaEventRecord(ev[1 + sub - 1], aux);
+    if (sub > 1) cudaStreamWaitEvent(s, ev[1 + sub - 2], 0);
+    launch_iface(m, dyn, gr, sub, g, s);
+    cudaEventRecord(ev[5 + sub - 1], s);
+  }
+  b_inject<<<g.inject, kThreads, 0, aux>>>(m, dyn);
+  cudaEventRecord(ev[9], aux);
+  cudaStreamWaitEvent(s, ev[9], 0);
+  b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log);
+}
+
+}  // namespace batch
+}  // namespace dns

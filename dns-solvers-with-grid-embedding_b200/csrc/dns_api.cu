@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/dns_embed.h"
+#include "host.h"
 #include "kernels.h"
 
 using namespace dns;
@@ -239,7 +240,7 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
 
 // wall flags: solid_init.c:46-69, slip_ridges_init.c:35-66, slip_posts_init.c:45-117,
 // slip_spanwise_init.c:34-66 (global index; writes past the span are dropped)
-static std::vector<int8_t> wall_flags(const dns_params &p, const dns_geometry &g) {
+std::vector<int8_t> dns::wall_flags(const dns_params &p, const dns_geometry &g) {
   std::vector<int8_t> sx(g.nxf, -1), sy(g.nyf, -1), w((size_t)g.nyf * g.nxf, -1);
   const bool ys = p.pattern == DNS_PATTERN_RSLIP || p.pattern == DNS_PATTERN_PSLIP;
   const bool xs = p.pattern == DNS_PATTERN_SSLIP || p.pattern == DNS_PATTERN_PSLIP;
@@ -914,21 +915,16 @@ static void profile_z(const dns_geometry &g, std::vector<double> &z) {
   for (int k = 0; k < NZ; k++) z[k] /= ((double)(g.nzs - 2.));
 }
 
-extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
-  if (!h || !out) return fail(DNS_EINVAL, "bad argument");
-  CUDA_TRY(cudaSetDevice(h->p.device));
-  const int NZ = h->g.nz_profile;
-  std::vector<double> acc((size_t)NZ * 16);
-  CUDA_TRY(cudaMemcpyAsync(acc.data(), h->stats_acc, acc.size() * 8, cudaMemcpyDeviceToHost, h->stream));
-  CUDA_TRY(cudaStreamSynchronize(h->stream));
+void dns::stats_from_acc(const dns_geometry &g, const double *acc, double *out, long *nsamples) {
+  const int NZ = g.nz_profile;
   std::vector<double> z;
-  profile_z(h->g, z);
+  profile_z(g, z);
   long ns = 0;
   for (int p = 0; p < NZ; p++) ns = std::max(ns, (long)acc[(size_t)p * 16 + 15]);
   if (nsamples) *nsamples = ns;
   std::memset(out, 0, sizeof(double) * DNS_NSTAT * NZ);
   for (int p = 0; p < NZ; p++) {
-    const double *a = acc.data() + (size_t)p * 16;
+    const double *a = acc + (size_t)p * 16;
     out[0 * NZ + p] = z[p];
     const double S = a[15], N = a[14];
     if (S <= 0 || N <= 0) continue;
@@ -944,6 +940,15 @@ extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
     out[12 * NZ + p] = a[6] / T - mw * mw;
     out[13 * NZ + p] = a[7] / T - mu * mw;
   }
+}
+
+extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
+  if (!h || !out) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  std::vector<double> acc((size_t)h->g.nz_profile * 16);
+  CUDA_TRY(cudaMemcpyAsync(acc.data(), h->stats_acc, acc.size() * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  dns::stats_from_acc(h->g, acc.data(), out, nsamples);
   return DNS_OK;
 }
 
@@ -1060,3 +1065,5 @@ extern "C" const char *dns_error_string(int code) {
 extern "C" const char *dns_last_error(void) { return g_last_error.c_str(); }
 
 void dns::set_last_error(const std::string &msg) { g_last_error = msg; }
+
+int dns::fail_with(int code, const std::string &msg) { return fail(code, msg); }

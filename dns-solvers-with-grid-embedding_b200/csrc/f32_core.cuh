@@ -1,0 +1,558 @@
+// Device arithmetic of the FP32 deviation-storage form, shared by the
+// single-channel kernels (kernels_f32.cu) and the batched engine
+// (batch_f32.cu).
+//
+// Populations are stored as float deviations d_a = f_a - w_a (reference
+// density rho0 = 1) and collided in FP32; the constant-flow-rate momentum and
+// mass sums, the wall-shear sums and the statistics are accumulated in FP64.
+// Storing the deviation keeps the float mantissa on the part of f that varies
+// (|d| ~ 1e-2..1e-4 instead of f ~ 0.03..0.33).
+//
+// Exact identities used:  rho = 1 + sum d,  rho u = sum e d  (sum e w = 0),
+// feq_a - w_a = w_a (drho + rho (3 e.u + 4.5 (e.u)^2 - 1.5 u^2)), and the
+// bounce-back / mirror rules move d exactly as f (w is invariant under
+// opposite and mirror).  Layout and wall rules are those of kernels_f64.cu;
+// the interface history holds [drho, ux, uy, uz, fneq_0..18] in FP32.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "kernels.h"
+#include "lattice.cuh"
+
+namespace dns {
+namespace f32 {
+
+constexpr int kThreads = 128;
+// minimum resident blocks asked of the register allocator for the bulk-plane
+// kernels (0: compiler's choice); fused: collide each population right before
+// its store so collided values die as they are written
+#ifndef DNS_F32_BULK_MINB
+#define DNS_F32_BULK_MINB 6
+#endif
+#ifndef DNS_F32_FUSED
+#define DNS_F32_FUSED 1
+#endif
+// population groups per (tile, wall) of the interface transfer (1..19)
+#ifndef DNS_F32_IFACE_GROUPS
+#define DNS_F32_IFACE_GROUPS 2
+#endif
+
+__device__ __forceinline__ int wrapf(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+__host__ __device__ constexpr float w_of(int a) { return a == 0 ? 1.f / 3.f : (a <= 6 ? 1.f / 18.f : 1.f / 36.f); }
+__host__ __device__ constexpr float bi_of(int a) { return a == 0 ? 0.f : (a <= 6 ? 1.f / 6.f : 1.f / 12.f); }
+
+__device__ __forceinline__ float proj_f32(int a, float u0, float u1, float u2) {
+  return (float)ex_of(a) * u0 + (float)ey_of(a) * u1 + (float)ez_of(a) * u2;
+}
+
+// deviation of the equilibrium from w_a
+__device__ __forceinline__ float deq_f32(int a, float drho, float rho, float u0, float u1, float u2, float usq) {
+  const float eu = proj_f32(a, u0, u1, u2);
+  return w_of(a) * (drho + rho * (3.f * eu + 4.5f * eu * eu - 1.5f * usq));
+}
+
+struct Mac32 {
+  float drho, rho, u0, u1, u2, usq;
+};
+
+__device__ __forceinline__ Mac32 macro_f32(const float (&d)[19]) {
+  float dr = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    dr += d[a];
+    if (ex_of(a) > 0) mx += d[a];
+    if (ex_of(a) < 0) mx -= d[a];
+    if (ey_of(a) > 0) my += d[a];
+    if (ey_of(a) < 0) my -= d[a];
+    if (ez_of(a) > 0) mz += d[a];
+    if (ez_of(a) < 0) mz -= d[a];
+  }
+  Mac32 m;
+  m.drho = dr;
+  m.rho = 1.f + dr;
+  const float inv = 1.f / m.rho;
+  m.u0 = mx * inv;
+  m.u1 = my * inv;
+  m.u2 = mz * inv;
+  m.usq = m.u0 * m.u0 + m.u1 * m.u1 + m.u2 * m.u2;
+  return m;
+}
+
+__device__ __forceinline__ Mac32 collide_f32(float (&d)[19], float om, float G) {
+  const Mac32 m = macro_f32(d);
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+    float dn = d[a] - om * (d[a] - deq);
+    if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * G;
+    d[a] = dn;
+  }
+  return m;
+}
+
+template <int N>
+__device__ __forceinline__ void block_reduce32(double (&v)[N], double *out) {
+  __shared__ double red[N][kThreads / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+  for (int q = 0; q < N; q++) {
+    double x = v[q];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+    if (lane == 0) red[q][warp] = x;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int q = 0; q < N; q++) {
+      double s = red[q][0];
+      for (int w = 1; w < nw; w++) s += red[q][w];
+      out[q] = s;
+    }
+  }
+  __syncthreads();
+}
+
+__device__ __forceinline__ void load19f(const float *__restrict__ src, size_t idx, size_t stride, float (&d)[19]) {
+#pragma unroll
+  for (int a = 0; a < 19; a++) d[a] = __ldg(src + idx + (size_t)a * stride);
+}
+
+// ------------------------------------------------------------------ coarse
+template <bool STATS>
+__device__ __forceinline__ void coarse_node_f32(float (&f)[19], int i, int j, int k, const Dims &d, float om,
+                                                float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
+                                                double (&sacc)[9]) {
+  const int nx = d.nx, ny = d.ny, nzc = d.nzc;
+  const Mac32 m = collide_f32(f, om, G);
+  if (STATS) {
+    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  }
+  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int k2 = k + ez_of(a);
+    if (k2 < 1 || k2 > nzc - 2) continue;
+    const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
+    const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
+    (dst + (size_t)a * pstride)[(unsigned)((k2 * ny + j2) * nx + i2)] = f[a];
+    den += f[a];
+    if (ex_of(a) > 0) mom += f[a];
+    if (ex_of(a) < 0) mom -= f[a];
+  }
+  acc[0] += mom;
+  acc[1] += den;
+}
+
+template <bool STATS>
+__device__ __forceinline__ void coarse_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
+                                                float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
+                                                double (&sacc)[9]) {
+  const int nx = d.nx, ny = d.ny;
+  const Mac32 m = collide_f32(f, om, G);
+  if (STATS) {
+    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  }
+  const int plane = ny * nx;
+  const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
+  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+  // each population array holds fewer than 2^31 floats: 32-bit offsets from
+  // the population's (thread-uniform) base
+  const unsigned u0 = (unsigned)idx0;
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
+                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
+    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
+    den += f[a];
+    if (ex_of(a) > 0) mom += f[a];
+    if (ex_of(a) < 0) mom -= f[a];
+  }
+  acc[0] += mom;
+  acc[1] += den;
+}
+
+// ------------------------------------------------------------------ fine
+template <int MODE>
+__device__ __forceinline__ void fine_node_f32(float (&f)[19], int i, int j, int p, int k, bool upper, int kwall,
+                                              const Dims &d, float om, float Gf, const int8_t *__restrict__ wf,
+                                              float *__restrict__ dst, size_t pstride, bool wall_sum_plane,
+                                              bool wall_rho_plane, double (&acc)[2], double (&wacc)[2],
+                                              double (&sacc)[9]) {
+  const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
+  const Mac32 m = collide_f32(f, om, Gf);
+  if (MODE & 2) {
+    if (wall_sum_plane) wacc[0] += (double)m.u0;
+    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
+  }
+  if (MODE & 4) {
+    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  }
+  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
+  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
+  const bool wall_adjacent = upper ? (k == zdf - 2) : (k == 1);
+  const int8_t own = wall_adjacent ? wf[(size_t)j * nx + i] : (int8_t)-1;
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int k2 = k + ez_of(a);
+    const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
+    const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
+    int pd, id, jd, ad, kd, exd;
+    if (k2 == kwall) {
+      const int8_t sld = wf[(size_t)j2 * nx + i2];
+      if (sld == -1 && own == -1) {
+        pd = p; id = i; jd = j; ad = opp_of(a); exd = -ex_of(a);
+      } else {
+        pd = p; id = i2; jd = j2; ad = mir_of(a); exd = ex_of(a);
+      }
+      kd = k;
+    } else {
+      if (!upper && k2 >= zdf - 1) continue;
+      if (upper && k2 <= 0) continue;
+      pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
+    }
+    (dst + (size_t)ad * pstride)[(unsigned)((pd * ny + jd) * nx + id)] = f[a];
+    if (MODE & 1) {
+      const float wgt = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
+                               : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
+      den += wgt * f[a];
+      if (exd > 0) mom += wgt * f[a];
+      if (exd < 0) mom -= wgt * f[a];
+    }
+  }
+  acc[0] += mom;
+  acc[1] += den;
+}
+
+// Bulk planes (every push lands on a fluid plane of the same block: no wall,
+// no interface): destinations from precomputed +-1 / +-row / +-plane offsets
+// with the periodic wrap folded in; encalc2 weights per destination plane.
+template <int MODE>
+__device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
+                                              float Gf, float *__restrict__ dst, size_t pstride, const float (&wz)[3],
+                                              bool wall_sum_plane, bool wall_rho_plane, double (&acc)[2],
+                                              double (&wacc)[2], double (&sacc)[9]) {
+  const int nx = d.nxf, ny = d.nyf;
+#if DNS_F32_FUSED
+  const Mac32 m = macro_f32(f);
+#else
+  const Mac32 m = collide_f32(f, om, Gf);
+#endif
+  if (MODE & 2) {
+    if (wall_sum_plane) wacc[0] += (double)m.u0;
+    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
+  }
+  if (MODE & 4) {
+    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  }
+  const int plane = ny * nx;
+  const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
+  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+  // each population array holds fewer than 2^31 floats: 32-bit offsets from
+  // the population's (thread-uniform) base
+  const unsigned u0 = (unsigned)idx0;
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
+                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
+#if DNS_F32_FUSED
+    {
+      const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+      float dn = f[a] - om * (f[a] - deq);
+      if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * Gf;
+      f[a] = dn;
+    }
+#endif
+    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
+    if (MODE & 1) {
+      const float wgt = wz[ez_of(a) + 1];
+      den += wgt * f[a];
+      if (ex_of(a) > 0) mom += wgt * f[a];
+      if (ex_of(a) < 0) mom -= wgt * f[a];
+    }
+  }
+  acc[0] += mom;
+  acc[1] += den;
+}
+
+// ------------------------------------------------------------------ interface
+// Coarse-to-fine transfer of one tile of interface cells (ctfdtransfer_opt.c,
+// tinterpolate_hrmt.c, derivative.c, bcucof_opt.c).  Per field: the three
+// history levels are combined with the Hermite-in-time weights, the fourth-order
+// x, y and cross derivatives are formed at the tile's cell corners, and every
+// fine node of the tile is evaluated from its cell's bicubic patch.  The patch
+// with unit spacing matching value, d/dx, d/dy and d2/dxdy at the four corners
+// is the tensor product of the cubic Hermite basis
+//   h00(t) = 2t^3 - 3t^2 + 1, h01(t) = -2t^3 + 3t^2, h10(t) = t^3 - 2t^2 + t, h11(t) = t^3 - t^2,
+// so p(t, u) = sum_{a,b in 0,1} [h0a(t) h0b(u) V + h1a(t) h0b(u) Dx + h0a(t) h1b(u) Dy + h1a(t) h1b(u) Dxy]
+// at corner (a, b): the same polynomial as the 16 coefficients of the
+// reference's bicubic map, evaluated in 20 multiply-adds per node instead of
+// 256 + 16.  The FP32 form keeps its own rounding order (it is compared with
+// the FP64 oracle within a tolerance, not bit for bit).
+//
+// Tile: TX x TY coarse cells; the fine tile is GR*TX (<= 64) columns wide and
+// thread t evaluates fine column (t & 63) of rows (t >> 6) + 2r, r < NR.
+template <int GR>
+struct IfTile;
+template <>
+struct IfTile<2> {
+  static constexpr int TX = 32, TY = 8;
+};
+template <>
+struct IfTile<3> {
+  static constexpr int TX = 21, TY = 6;
+};
+template <>
+struct IfTile<4> {
+  static constexpr int TX = 16, TY = 4;
+};
+
+struct IfParams32 {
+  const float *hn, *hp, *hpp;  // history slots of levels n, p, pp: [2 walls][23][ny][nx]
+  float *fdst;                 // fine lattice receiving the interface planes
+  int nx, ny, nxf, nyf, zds;
+  float an, ap, app;           // Hermite-in-time weights of levels n, p, pp
+  float fac;                   // omega_c / (GR omega_f): non-equilibrium rescaling
+};
+
+// launch parameters of one substep's transfer (substep s of GR: time s/GR)
+inline IfParams32 iface_params32(const float *hn, const float *hp, const float *hpp, float *fdst, const Dims &d,
+                                 int substep, double omega_c, double omega_f) {
+  // value = h00 p + h10 (n - pp)/2 + h01 n + h11 (3n - 4p + pp)/2 (tinterpolate_hrmt.c:28-34),
+  // gathered per level
+  const double t = (double)substep / (double)d.gr, t2 = t * t, t3 = t2 * t;
+  const double h1 = 2. * t3 - 3. * t2 + 1., h2 = t3 - 2. * t2 + t, h3 = -2. * t3 + 3. * t2, h4 = t3 - t2;
+  IfParams32 P;
+  P.hn = hn;
+  P.hp = hp;
+  P.hpp = hpp;
+  P.fdst = fdst;
+  P.nx = d.nx;
+  P.ny = d.ny;
+  P.nxf = d.nxf;
+  P.nyf = d.nyf;
+  P.zds = d.zds;
+  P.an = (float)(0.5 * h2 + h3 + 1.5 * h4);
+  P.ap = (float)(h1 - 2. * h4);
+  P.app = (float)(-0.5 * h2 + 0.5 * h4);
+  P.fac = (float)(omega_c / ((double)d.gr * omega_f));
+  return P;
+}
+
+template <int GR>
+struct IfSmem32 {
+  static constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY;
+  float V[TY + 5][TX + 5];
+  float DY[TY + 1][TX + 5];
+  float4 C[TY + 1][TX + 1];  // value, d/dx, d/dy, d2/dxdy at the cell corners
+};
+
+// Staging of one field: the thread's share of the tile-plus-halo values is
+// prefetched into registers (offsets into a history plane precomputed once per
+// tile, with the periodic wrap), written as the time-interpolated value, and
+// the corner derivatives are formed in shared memory.
+template <int GR>
+struct IfStage {
+  static constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, QX = TX + 5, QY = TY + 5;
+  static constexpr int NV = (QX * QY + kThreads - 1) / kThreads;
+  int off[NV];                    // offset into a history plane, -1: no slot
+  float vn[NV], vp[NV], vpp[NV];  // prefetched levels n, p, pp
+  __device__ __forceinline__ void init(const IfParams32 &P, int i0, int j0) {
+#pragma unroll
+    for (int s = 0; s < NV; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      off[s] = -1;
+      if (q < QX * QY) {
+        const int pi = q % QX, pj = q / QX;
+        off[s] = wrapf(j0 - 2 + pj, P.ny) * P.nx + wrapf(i0 - 2 + pi, P.nx);
+      }
+    }
+  }
+  __device__ __forceinline__ void prefetch(const float *__restrict__ hn, const float *__restrict__ hp,
+                                           const float *__restrict__ hpp) {
+#pragma unroll
+    for (int s = 0; s < NV; s++)
+      if (off[s] >= 0) {
+        vn[s] = __ldg(hn + off[s]);
+        vp[s] = __ldg(hp + off[s]);
+        vpp[s] = __ldg(hpp + off[s]);
+      }
+  }
+  __device__ __forceinline__ void build(IfSmem32<GR> &S, const IfParams32 &P) {
+    const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
+    float *V = &S.V[0][0];
+#pragma unroll
+    for (int s = 0; s < NV; s++)
+      if (off[s] >= 0) V[threadIdx.x + s * kThreads] = P.an * vn[s] + P.ap * vp[s] + P.app * vpp[s];
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < (QX * (TY + 1) + kThreads - 1) / kThreads; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      if (q < QX * (TY + 1)) {
+        const int pi = q % QX, r = q / QX;
+        S.DY[r][pi] = c2o3 * (S.V[r + 3][pi] - S.V[r + 1][pi]) - c1o12 * (S.V[r + 4][pi] - S.V[r][pi]);
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < ((TX + 1) * (TY + 1) + kThreads - 1) / kThreads; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      if (q < (TX + 1) * (TY + 1)) {
+        const int c = q % (TX + 1), r = q / (TX + 1);
+        const float dx =
+            c2o3 * (S.V[r + 2][c + 3] - S.V[r + 2][c + 1]) - c1o12 * (S.V[r + 2][c + 4] - S.V[r + 2][c]);
+        const float dxy = c2o3 * (S.DY[r][c + 3] - S.DY[r][c + 1]) - c1o12 * (S.DY[r][c + 4] - S.DY[r][c]);
+        S.C[r][c] = make_float4(S.V[r + 2][c + 2], dx, S.DY[r][c + 2], dxy);
+      }
+    }
+    __syncthreads();
+  }
+};
+
+struct Herm {
+  float a0, a1, b0, b1;  // h00, h01, h10, h11
+};
+__host__ __device__ constexpr float herm_c(int which, int j, int gr) {
+  return which == 0   ? 2.f * (float)(j * j * j) / (float)(gr * gr * gr) - 3.f * (float)(j * j) / (float)(gr * gr) + 1.f
+         : which == 1 ? -2.f * (float)(j * j * j) / (float)(gr * gr * gr) + 3.f * (float)(j * j) / (float)(gr * gr)
+         : which == 2 ? (float)(j * j * j) / (float)(gr * gr * gr) - 2.f * (float)(j * j) / (float)(gr * gr) +
+                            (float)j / (float)gr
+                      : (float)(j * j * j) / (float)(gr * gr * gr) - (float)(j * j) / (float)(gr * gr);
+}
+// basis at t = j / GR, j < GR <= 4: [GR - 2][j][h00 h01 h10 h11]
+#define DNS_HERM_ROW(j, g) {herm_c(0, j, g), herm_c(1, j, g), herm_c(2, j, g), herm_c(3, j, g)}
+#define DNS_HERM_GR(g) {DNS_HERM_ROW(0, g), DNS_HERM_ROW(1, g), DNS_HERM_ROW(2, g), DNS_HERM_ROW(3, g)}
+static __constant__ float c_herm[3][4][4] = {DNS_HERM_GR(2), DNS_HERM_GR(3), DNS_HERM_GR(4)};
+#undef DNS_HERM_GR
+#undef DNS_HERM_ROW
+template <int GR>
+__device__ __forceinline__ Herm herm_at(int j) {
+  return Herm{c_herm[GR - 2][j][0], c_herm[GR - 2][j][1], c_herm[GR - 2][j][2], c_herm[GR - 2][j][3]};
+}
+
+// patch value at local cell (cx, cy) with basis hx (in x) and hy (in y)
+template <int GR>
+__device__ __forceinline__ float if_eval32(const IfSmem32<GR> &S, int cx, int cy, const Herm &hx, const Herm &hy) {
+  const float4 c00 = S.C[cy][cx], c10 = S.C[cy][cx + 1], c01 = S.C[cy + 1][cx], c11 = S.C[cy + 1][cx + 1];
+  // along x on the two corner rows: value part P and d/dy part Q
+  const float p0 = hx.a0 * c00.x + hx.a1 * c10.x + hx.b0 * c00.y + hx.b1 * c10.y;
+  const float q0 = hx.a0 * c00.z + hx.a1 * c10.z + hx.b0 * c00.w + hx.b1 * c10.w;
+  const float p1 = hx.a0 * c01.x + hx.a1 * c11.x + hx.b0 * c01.y + hx.b1 * c11.y;
+  const float q1 = hx.a0 * c01.z + hx.a1 * c11.z + hx.b0 * c01.w + hx.b1 * c11.w;
+  return hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+}
+
+// The NR node values of the thread's fine column (cell column cx, basis hx);
+// thread row group fy0 (0 or 1) takes fine rows fy0 + 2r.  For GR = 2 every
+// node of the column has jj = fy0 and cell row r, so each corner row's
+// x-pass is shared by two consecutive nodes.
+template <int GR>
+__device__ __forceinline__ void if_rowpass32(const IfSmem32<GR> &S, int cx, int cr, const Herm &hx, float &p,
+                                             float &q) {
+  const float4 c0 = S.C[cr][cx], c1 = S.C[cr][cx + 1];
+  p = hx.a0 * c0.x + hx.a1 * c1.x + hx.b0 * c0.y + hx.b1 * c1.y;
+  q = hx.a0 * c0.z + hx.a1 * c1.z + hx.b0 * c0.w + hx.b1 * c1.w;
+}
+
+template <int GR, int NR>
+__device__ __forceinline__ void if_eval_column32(const IfSmem32<GR> &S, int cx, int fy0, const Herm &hx,
+                                                 float (&val)[NR]) {
+  if constexpr (GR == 2) {
+    const Herm hy = herm_at<2>(fy0);
+    float p0, q0;
+    if_rowpass32<GR>(S, cx, 0, hx, p0, q0);
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      float p1, q1;
+      if_rowpass32<GR>(S, cx, r + 1, hx, p1, q1);
+      val[r] = hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+      p0 = p1;
+      q0 = q1;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
+      val[r] = if_eval32<GR>(S, cx, cy, hx, herm_at<GR>(jj));
+    }
+  }
+}
+
+// One tile, one wall, populations [a0, a1) (the macroscopic fields always):
+// f_a = feq_a(rho^, u^) + fac fneq^_a written into the wall's interface plane
+// (lower block plane zds-1 = k zdf-1, upper block plane zds = k 0).  The
+// next field's history values are in flight while the current one is
+// evaluated.  Requires blockDim.x == kThreads.
+template <int GR>
+__device__ __forceinline__ void iface_tile32(IfSmem32<GR> &S, const IfParams32 &P, int tx, int ty, int w, int a0,
+                                             int a1) {
+  constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, NR = GR * TY / 2;
+  const int i0 = tx * TX, j0 = ty * TY;
+  const int t = threadIdx.x, fx = t & 63, fy0 = (t >> 6) & 1;
+  const bool colok = fx < GR * TX && i0 + fx / GR < P.nx;
+  const int cx = colok ? fx / GR : 0, ii = colok ? fx - cx * GR : 0;  // in-bounds reads for idle lanes
+  const Herm hx = herm_at<GR>(ii);
+  const size_t plane = (size_t)P.ny * P.nx, fplane = (size_t)P.nyf * P.nxf;
+  const size_t wo = (size_t)w * 23 * plane;
+  const int pf = w == 0 ? P.zds - 1 : P.zds;
+  float *out = P.fdst + (size_t)pf * fplane;
+  const size_t fstride = (size_t)2 * P.zds * fplane;
+  IfStage<GR> st;
+  st.init(P, i0, j0);
+  st.prefetch(P.hn + wo, P.hp + wo, P.hpp + wo);
+  float mac[4][NR];
+#pragma unroll
+  for (int b = 0; b < 4; b++) {
+    st.build(S, P);
+    // next field: macroscopic b + 1, or the first population of the group
+    const size_t nf = wo + (size_t)(b < 3 ? b + 1 : 4 + a0) * plane;
+    if (b < 3 || a0 < a1) st.prefetch(P.hn + nf, P.hp + nf, P.hpp + nf);
+    if_eval_column32<GR, NR>(S, cx, fy0, hx, mac[b]);
+  }
+  float usq[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) usq[r] = mac[1][r] * mac[1][r] + mac[2][r] * mac[2][r] + mac[3][r] * mac[3][r];
+  for (int a = a0; a < a1; a++) {
+    st.build(S, P);
+    if (a + 1 < a1) {
+      const size_t nf = wo + (size_t)(5 + a) * plane;
+      st.prefetch(P.hn + nf, P.hp + nf, P.hpp + nf);
+    }
+    const float ex = (float)ex_of(a), ey = (float)ey_of(a), ez = (float)ez_of(a), wa = w_of(a);
+    float *oa = out + (size_t)a * fstride;
+    float fv[NR];
+    if_eval_column32<GR, NR>(S, cx, fy0, hx, fv);
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
+      if (colok && j0 + cy < P.ny) {
+        const float fneq = fv[r];
+        const float dr = mac[0][r], eu = ex * mac[1][r] + ey * mac[2][r] + ez * mac[3][r];
+        const float deq = wa * (dr + (1.f + dr) * (3.f * eu + 4.5f * eu * eu - 1.5f * usq[r]));
+        oa[(size_t)((j0 + cy) * GR + jj) * P.nxf + (i0 + cx) * GR + ii] = deq + P.fac * fneq;
+      }
+    }
+  }
+}
+
+}  // namespace f32
+}  // namespace dns

@@ -85,9 +85,6 @@ def emit(path: Path):
             out.append(f"  (c)[{r}] = {expr};")
         return out
     lines.append(" \\\n".join(body("")))
-    lines.append("// the same map for the FP32 form (float literals)")
-    lines.append("#define DNS_BICUBIC_COEFFS_F32(c, x) \\")
-    lines.append(" \\\n".join(body("f")))
     lines.append("")
     path.write_text("\n".join(lines))
 

@@ -1,18 +1,8 @@
-// FP32 deviation-storage form of the grid-embedded D3Q19 channel step.
-//
-// Populations are stored as float deviations d_a = f_a - w_a (reference
-// density rho0 = 1) and collided in FP32; the constant-flow-rate momentum and
-// mass sums, the wall-shear sums and the statistics are accumulated in FP64.
-// Storing the deviation keeps the float mantissa on the part of f that varies
-// (|d| ~ 1e-2..1e-4 instead of f ~ 0.03..0.33).
-//
-// Exact identities used:  rho = 1 + sum d,  rho u = sum e d  (sum e w = 0),
-// feq_a - w_a = w_a (drho + rho (3 e.u + 4.5 (e.u)^2 - 1.5 u^2)), and the
-// bounce-back / mirror rules move d exactly as f (w is invariant under
-// opposite and mirror).  Layout, launch shapes, wall rules and the interface
-// algorithm are those of kernels_f64.cu; the interface history holds
-// [drho, ux, uy, uz, fneq_0..18] in FP32.
-#include "bicubic_gen.cuh"
+// FP32 deviation-storage form of the grid-embedded D3Q19 channel step: the
+// kernels of one channel.  The device arithmetic (collision, streaming rules,
+// interface evaluation) is in f32_core.cuh; layout, launch shapes and wall
+// rules follow kernels_f64.cu.
+#include "f32_core.cuh"
 #include "kernels.h"
 #include "lattice.cuh"
 
@@ -20,163 +10,9 @@ namespace dns {
 
 namespace {
 
-constexpr int kThreads = 128;
-// minimum resident blocks asked of the register allocator for the bulk-plane
-// kernels (0: compiler's choice); fused: collide each population right before
-// its store so collided values die as they are written
-#ifndef DNS_F32_BULK_MINB
-#define DNS_F32_BULK_MINB 6
-#endif
-#ifndef DNS_F32_FUSED
-#define DNS_F32_FUSED 1
-#endif
-
-__device__ __forceinline__ int wrapf(int v, int n) {
-  v %= n;
-  return v < 0 ? v + n : v;
-}
-
-__host__ __device__ constexpr float w_of(int a) { return a == 0 ? 1.f / 3.f : (a <= 6 ? 1.f / 18.f : 1.f / 36.f); }
-__host__ __device__ constexpr float bi_of(int a) { return a == 0 ? 0.f : (a <= 6 ? 1.f / 6.f : 1.f / 12.f); }
-
-__device__ __forceinline__ float proj_f32(int a, float u0, float u1, float u2) {
-  return (float)ex_of(a) * u0 + (float)ey_of(a) * u1 + (float)ez_of(a) * u2;
-}
-
-// deviation of the equilibrium from w_a
-__device__ __forceinline__ float deq_f32(int a, float drho, float rho, float u0, float u1, float u2, float usq) {
-  const float eu = proj_f32(a, u0, u1, u2);
-  return w_of(a) * (drho + rho * (3.f * eu + 4.5f * eu * eu - 1.5f * usq));
-}
-
-struct Mac32 {
-  float drho, rho, u0, u1, u2, usq;
-};
-
-__device__ __forceinline__ Mac32 macro_f32(const float (&d)[19]) {
-  float dr = 0.f, mx = 0.f, my = 0.f, mz = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    dr += d[a];
-    if (ex_of(a) > 0) mx += d[a];
-    if (ex_of(a) < 0) mx -= d[a];
-    if (ey_of(a) > 0) my += d[a];
-    if (ey_of(a) < 0) my -= d[a];
-    if (ez_of(a) > 0) mz += d[a];
-    if (ez_of(a) < 0) mz -= d[a];
-  }
-  Mac32 m;
-  m.drho = dr;
-  m.rho = 1.f + dr;
-  const float inv = 1.f / m.rho;
-  m.u0 = mx * inv;
-  m.u1 = my * inv;
-  m.u2 = mz * inv;
-  m.usq = m.u0 * m.u0 + m.u1 * m.u1 + m.u2 * m.u2;
-  return m;
-}
-
-__device__ __forceinline__ Mac32 collide_f32(float (&d)[19], float om, float G) {
-  const Mac32 m = macro_f32(d);
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
-    float dn = d[a] - om * (d[a] - deq);
-    if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * G;
-    d[a] = dn;
-  }
-  return m;
-}
-
-template <int N>
-__device__ __forceinline__ void block_reduce32(double (&v)[N], double *out) {
-  __shared__ double red[N][kThreads / 32];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-  for (int q = 0; q < N; q++) {
-    double x = v[q];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) red[q][warp] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int q = 0; q < N; q++) {
-      double s = red[q][0];
-      for (int w = 1; w < nw; w++) s += red[q][w];
-      out[q] = s;
-    }
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void load19f(const float *__restrict__ src, size_t idx, size_t stride, float (&d)[19]) {
-#pragma unroll
-  for (int a = 0; a < 19; a++) d[a] = __ldg(src + idx + (size_t)a * stride);
-}
+using namespace f32;
 
 // ------------------------------------------------------------------ coarse
-template <bool STATS>
-__device__ __forceinline__ void coarse_node_f32(float (&f)[19], int i, int j, int k, const Dims &d, float om,
-                                                float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
-                                                double (&sacc)[9]) {
-  const int nx = d.nx, ny = d.ny, nzc = d.nzc;
-  const Mac32 m = collide_f32(f, om, G);
-  if (STATS) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
-  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const int k2 = k + ez_of(a);
-    if (k2 < 1 || k2 > nzc - 2) continue;
-    const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
-    const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
-    (dst + (size_t)a * pstride)[(unsigned)((k2 * ny + j2) * nx + i2)] = f[a];
-    den += f[a];
-    if (ex_of(a) > 0) mom += f[a];
-    if (ex_of(a) < 0) mom -= f[a];
-  }
-  acc[0] += mom;
-  acc[1] += den;
-}
-
-template <bool STATS>
-__device__ __forceinline__ void coarse_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
-                                                float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
-                                                double (&sacc)[9]) {
-  const int nx = d.nx, ny = d.ny;
-  const Mac32 m = collide_f32(f, om, G);
-  if (STATS) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
-  const int plane = ny * nx;
-  const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
-  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
-  // each population array holds fewer than 2^31 floats: 32-bit offsets from
-  // the population's (thread-uniform) base
-  const unsigned u0 = (unsigned)idx0;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
-                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
-    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
-    den += f[a];
-    if (ex_of(a) > 0) mom += f[a];
-    if (ex_of(a) < 0) mom -= f[a];
-  }
-  acc[0] += mom;
-  acc[1] += den;
-}
-
 template <bool STATS, bool BULK>
 __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) coarse_f32(const float *__restrict__ src, float *__restrict__ dst, Dims d,
                                                       int jb, float om, const DevState *st,
@@ -226,114 +62,6 @@ __global__ void __launch_bounds__(kThreads) extract_f32(const float *__restrict_
 }
 
 // ------------------------------------------------------------------ fine
-template <int MODE>
-__device__ __forceinline__ void fine_node_f32(float (&f)[19], int i, int j, int p, int k, bool upper, int kwall,
-                                              const Dims &d, float om, float Gf, const int8_t *__restrict__ wf,
-                                              float *__restrict__ dst, size_t pstride, bool wall_sum_plane,
-                                              bool wall_rho_plane, double (&acc)[2], double (&wacc)[2],
-                                              double (&sacc)[9]) {
-  const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
-  const Mac32 m = collide_f32(f, om, Gf);
-  if (MODE & 2) {
-    if (wall_sum_plane) wacc[0] += (double)m.u0;
-    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
-  }
-  if (MODE & 4) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
-  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
-  const bool wall_adjacent = upper ? (k == zdf - 2) : (k == 1);
-  const int8_t own = wall_adjacent ? wf[(size_t)j * nx + i] : (int8_t)-1;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const int k2 = k + ez_of(a);
-    const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
-    const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
-    int pd, id, jd, ad, kd, exd;
-    if (k2 == kwall) {
-      const int8_t sld = wf[(size_t)j2 * nx + i2];
-      if (sld == -1 && own == -1) {
-        pd = p; id = i; jd = j; ad = opp_of(a); exd = -ex_of(a);
-      } else {
-        pd = p; id = i2; jd = j2; ad = mir_of(a); exd = ex_of(a);
-      }
-      kd = k;
-    } else {
-      if (!upper && k2 >= zdf - 1) continue;
-      if (upper && k2 <= 0) continue;
-      pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
-    }
-    (dst + (size_t)ad * pstride)[(unsigned)((pd * ny + jd) * nx + id)] = f[a];
-    if (MODE & 1) {
-      const float wgt = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
-                               : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
-      den += wgt * f[a];
-      if (exd > 0) mom += wgt * f[a];
-      if (exd < 0) mom -= wgt * f[a];
-    }
-  }
-  acc[0] += mom;
-  acc[1] += den;
-}
-
-// Bulk planes (every push lands on a fluid plane of the same block: no wall,
-// no interface): destinations from precomputed +-1 / +-row / +-plane offsets
-// with the periodic wrap folded in; encalc2 weights per destination plane.
-template <int MODE>
-__device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
-                                              float Gf, float *__restrict__ dst, size_t pstride, const float (&wz)[3],
-                                              bool wall_sum_plane, bool wall_rho_plane, double (&acc)[2],
-                                              double (&wacc)[2], double (&sacc)[9]) {
-  const int nx = d.nxf, ny = d.nyf;
-#if DNS_F32_FUSED
-  const Mac32 m = macro_f32(f);
-#else
-  const Mac32 m = collide_f32(f, om, Gf);
-#endif
-  if (MODE & 2) {
-    if (wall_sum_plane) wacc[0] += (double)m.u0;
-    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
-  }
-  if (MODE & 4) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
-  const int plane = ny * nx;
-  const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
-  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
-  // each population array holds fewer than 2^31 floats: 32-bit offsets from
-  // the population's (thread-uniform) base
-  const unsigned u0 = (unsigned)idx0;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
-                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
-#if DNS_F32_FUSED
-    {
-      const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
-      float dn = f[a] - om * (f[a] - deq);
-      if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * Gf;
-      f[a] = dn;
-    }
-#endif
-    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
-    if (MODE & 1) {
-      const float wgt = wz[ez_of(a) + 1];
-      den += wgt * f[a];
-      if (ex_of(a) > 0) mom += wgt * f[a];
-      if (ex_of(a) < 0) mom -= wgt * f[a];
-    }
-  }
-  acc[0] += mom;
-  acc[1] += den;
-}
-
 // The fine step is two launches: BULK over planes k = 2..zdf-3 of both blocks
 // (every push regular) and the edge planes (wall-adjacent, interface, and the
 // planes next to them).  blockIdx.z indexes a list of planes; partial sums
@@ -393,129 +121,15 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f
 }
 
 // ------------------------------------------------------------------ interface
-constexpr int JTX = 32, JTY = 16, JPX = 16, JPY = 8;
-constexpr int QX = JTX + 5, QY = JTY + 5;
-
-struct IfaceArgs32 {
-  float h1, h2, h3, h4, fac;
-};
-
-struct IfaceSmem32 {
-  float V[QY][QX];
-  float Dy[JTY + 1][QX];
-  float Dx[JTY + 1][JTX + 1];
-  float Dxy[JTY + 1][JTX + 1];
-};
-
-__device__ __forceinline__ void stage32(IfaceSmem32 &S, const float *__restrict__ hn, const float *__restrict__ hp,
-                                        const float *__restrict__ hpp, size_t fo, int i0, int j0, int nx, int ny,
-                                        const IfaceArgs32 &ia) {
-  const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
-  for (int q = threadIdx.x; q < QX * QY; q += blockDim.x) {
-    const int pi = q % QX, pj = q / QX;
-    const size_t g = fo + (size_t)wrapf(j0 - 2 + pj, ny) * nx + wrapf(i0 - 2 + pi, nx);
-    const float n = hn[g], pv = hp[g], pp = hpp[g];
-    S.V[pj][pi] = ia.h1 * pv + ia.h2 * ((n - pp) * 0.5f) + ia.h3 * n + ia.h4 * ((3.f * n - 4.f * pv + pp) * 0.5f);
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < QX * (JTY + 1); q += blockDim.x) {
-    const int pi = q % QX, r = q / QX, pj = r + 2;
-    S.Dy[r][pi] = c2o3 * (S.V[pj + 1][pi] - S.V[pj - 1][pi]) - c1o12 * (S.V[pj + 2][pi] - S.V[pj - 2][pi]);
-    if (pi >= 2 && pi < JTX + 3)
-      S.Dx[r][pi - 2] = c2o3 * (S.V[pj][pi + 1] - S.V[pj][pi - 1]) - c1o12 * (S.V[pj][pi + 2] - S.V[pj][pi - 2]);
-  }
-  __syncthreads();
-  for (int q = threadIdx.x; q < (JTX + 1) * (JTY + 1); q += blockDim.x) {
-    const int c = q % (JTX + 1), r = q / (JTX + 1), pi = c + 2;
-    S.Dxy[r][c] = c2o3 * (S.Dy[r][pi + 1] - S.Dy[r][pi - 1]) - c1o12 * (S.Dy[r][pi + 2] - S.Dy[r][pi - 2]);
-  }
-  __syncthreads();
-}
-
-__device__ __forceinline__ void coeffs32(const IfaceSmem32 &S, int cx, int cy, float (&cf)[16]) {
-  float x[16];
-  const int ci[4] = {0, 1, 1, 0}, cj[4] = {0, 0, 1, 1};
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int c = cx + ci[q], r = cy + cj[q];
-    x[q] = S.V[r + 2][c + 2];
-    x[4 + q] = S.Dx[r][c];
-    x[8 + q] = S.Dy[r][c + 2];
-    x[12 + q] = S.Dxy[r][c];
-  }
-  DNS_BICUBIC_COEFFS_F32(cf, x);
-}
-
+// one block per (tile, wall, population group)
+#ifndef DNS_F32_IFACE_MINB
+#define DNS_F32_IFACE_MINB 0
+#endif
 template <int GR>
-__device__ __forceinline__ float eval32(const float (&cf)[16], int ii, int jj) {
-  const float tt = (float)ii / (float)GR, uu = (float)jj / (float)GR;
-  float val = 0.f;
-#pragma unroll
-  for (int nn = 3; nn > -1; nn--)
-    val = tt * val + ((cf[nn * 4 + 3] * uu + cf[nn * 4 + 2]) * uu + cf[nn * 4 + 1]) * uu + cf[nn * 4 + 0];
-  return val;
-}
-
-template <int GR>
-__global__ void __launch_bounds__(JPX *JPY) iface_macro_f32(const float *__restrict__ hn, const float *__restrict__ hp,
-                                                            const float *__restrict__ hpp, float *__restrict__ mac,
-                                                            Dims d, IfaceArgs32 ia) {
-  __shared__ IfaceSmem32 S;
-  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf;
-  const int w = blockIdx.z >> 2, b = blockIdx.z & 3;
-  const int i0 = blockIdx.x * JTX, j0 = blockIdx.y * JTY;
-  const int tx = threadIdx.x % JPX, ty = threadIdx.x / JPX;
-  const size_t plane = (size_t)ny * nx, fplane = (size_t)nyf * nxf;
-  stage32(S, hn, hp, hpp, ((size_t)w * 23 + b) * plane, i0, j0, nx, ny, ia);
-  float *o = mac + ((size_t)w * 4 + b) * fplane;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int cx = tx + JPX * (q & 1), cy = ty + JPY * (q >> 1);
-    const int ic = i0 + cx, jc = j0 + cy;
-    if (ic < nx && jc < ny) {
-      float cf[16];
-      coeffs32(S, cx, cy, cf);
-#pragma unroll
-      for (int ii = 0; ii < GR; ii++)
-#pragma unroll
-        for (int jj = 0; jj < GR; jj++) o[(size_t)(jc * GR + jj) * nxf + ic * GR + ii] = eval32<GR>(cf, ii, jj);
-    }
-  }
-}
-
-template <int GR>
-__global__ void __launch_bounds__(JPX *JPY) iface_pop_f32(const float *__restrict__ hn, const float *__restrict__ hp,
-                                                          const float *__restrict__ hpp, const float *__restrict__ mac,
-                                                          float *__restrict__ fdst, Dims d, IfaceArgs32 ia) {
-  __shared__ IfaceSmem32 S;
-  const int nx = d.nx, ny = d.ny, nxf = d.nxf, nyf = d.nyf, zds = d.zds;
-  const int w = blockIdx.z / 19, a = blockIdx.z % 19;
-  const int i0 = blockIdx.x * JTX, j0 = blockIdx.y * JTY;
-  const int tx = threadIdx.x % JPX, ty = threadIdx.x / JPX;
-  const size_t plane = (size_t)ny * nx, fplane = (size_t)nyf * nxf;
-  const int pf = w == 0 ? zds - 1 : zds;
-  const size_t fstride = (size_t)2 * zds * fplane;
-  stage32(S, hn, hp, hpp, ((size_t)w * 23 + 4 + a) * plane, i0, j0, nx, ny, ia);
-  const float *m = mac + (size_t)w * 4 * fplane;
-  float *out = fdst + (size_t)a * fstride + (size_t)pf * fplane;
-#pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int cx = tx + JPX * (q & 1), cy = ty + JPY * (q >> 1);
-    const int ic = i0 + cx, jc = j0 + cy;
-    if (ic < nx && jc < ny) {
-      float cf[16];
-      coeffs32(S, cx, cy, cf);
-#pragma unroll
-      for (int ii = 0; ii < GR; ii++)
-#pragma unroll
-        for (int jj = 0; jj < GR; jj++) {
-          const size_t qn = (size_t)(jc * GR + jj) * nxf + ic * GR + ii;
-          const float dr = m[qn], u0 = m[fplane + qn], u1 = m[2 * fplane + qn], u2 = m[3 * fplane + qn];
-          const float usq = u0 * u0 + u1 * u1 + u2 * u2;
-          out[qn] = deq_f32(a, dr, 1.f + dr, u0, u1, u2, usq) + ia.fac * eval32<GR>(cf, ii, jj);
-        }
-    }
-  }
+__global__ void __launch_bounds__(kThreads, DNS_F32_IFACE_MINB) iface_f32(IfParams32 P, int groups) {
+  __shared__ IfSmem32<GR> S;
+  const int w = blockIdx.z / groups, g = blockIdx.z - w * groups;
+  iface_tile32<GR>(S, P, blockIdx.x, blockIdx.y, w, 19 * g / groups, 19 * (g + 1) / groups);
 }
 
 // ------------------------------------------------------------------ injection
@@ -753,24 +367,18 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
 
 void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *mac, float *fdst, const Dims &d,
                           int substep, double omega_c, double omega_f, cudaStream_t stream) {
-  const double tmp = (((double)substep) / ((double)d.gr));
-  IfaceArgs32 ia;
-  ia.h1 = (float)(2. * tmp * tmp * tmp - 3. * tmp * tmp + 1.);
-  ia.h2 = (float)(tmp * tmp * tmp - 2. * tmp * tmp + tmp);
-  ia.h3 = (float)(-2. * tmp * tmp * tmp + 3. * tmp * tmp);
-  ia.h4 = (float)(tmp * tmp * tmp - tmp * tmp);
-  ia.fac = (float)(omega_c / ((double)d.gr * omega_f));
-  const int gx = (d.nx + JTX - 1) / JTX, gy = (d.ny + JTY - 1) / JTY;
-  dim3 gm(gx, gy, 2 * 4), gp(gx, gy, 2 * 19), block(JPX * JPY);
+  (void)mac;
+  IfParams32 P = iface_params32(hn, hp, hpp, fdst, d, substep, omega_c, omega_f);
+  const int groups = DNS_F32_IFACE_GROUPS;
   if (d.gr == 2) {
-    iface_macro_f32<2><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
-    iface_pop_f32<2><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+    dim3 grid((d.nx + IfTile<2>::TX - 1) / IfTile<2>::TX, (d.ny + IfTile<2>::TY - 1) / IfTile<2>::TY, 2 * groups);
+    iface_f32<2><<<grid, kThreads, 0, stream>>>(P, groups);
   } else if (d.gr == 3) {
-    iface_macro_f32<3><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
-    iface_pop_f32<3><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+    dim3 grid((d.nx + IfTile<3>::TX - 1) / IfTile<3>::TX, (d.ny + IfTile<3>::TY - 1) / IfTile<3>::TY, 2 * groups);
+    iface_f32<3><<<grid, kThreads, 0, stream>>>(P, groups);
   } else {
-    iface_macro_f32<4><<<gm, block, 0, stream>>>(hn, hp, hpp, mac, d, ia);
-    iface_pop_f32<4><<<gp, block, 0, stream>>>(hn, hp, hpp, mac, fdst, d, ia);
+    dim3 grid((d.nx + IfTile<4>::TX - 1) / IfTile<4>::TX, (d.ny + IfTile<4>::TY - 1) / IfTile<4>::TY, 2 * groups);
+    iface_f32<4><<<grid, kThreads, 0, stream>>>(P, groups);
   }
 }
 

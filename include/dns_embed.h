@@ -190,6 +190,73 @@ int dns_kernel_times(dns_handle *h, double *ms, long *launches);
    the array, so calls that overlap on the GPU race: serialise them. */
 int dns_flow_sums_static(const dns_params *p, const double *fc, const double *ff, double *out4, void *cuda_stream);
 
+/* ---- batched FP32 engine --------------------------------------------------- */
+/* No counterpart in the reference (one MPI job per channel).  Many independent
+   channels of any size, wall pattern and Re_tau (one refinement ratio per
+   batch) are stepped together in the FP32 deviation-storage form: each phase
+   of the coarse step is one persistent kernel over a per-instance block table,
+   and run() replays a captured CUDA graph of a step group.  Instances keep
+   their lattice, history and statistics resident on the device until removed;
+   each has its own step budget and stops when it is spent.  An instance's
+   results depend only on its own parameters and tile shape, not on which
+   other instances share the batch. */
+typedef struct dns_batch dns_batch;
+
+/* Tile shape of one instance: threads per row along x (32, 64 or 128) and row
+   iterations per work item of the coarse and fine kernels, and the number of
+   population groups of the interface transfer (1..19). */
+typedef struct dns_tile {
+  int cw, cjb;
+  int fw, fjb;
+  int igroups;
+} dns_tile;
+
+typedef struct dns_batch_info {
+  long long steps_done;       /* coarse steps taken */
+  long long remaining;        /* steps left in the budget */
+  int status;                 /* DNS_OK, or DNS_ENAN after a non-finite wall shear stress */
+  int slot;                   /* internal row (diagnostics) */
+  double force;               /* force[0] of the next step */
+  double flowrate, stress;    /* last logged values */
+  long long device_bytes;     /* device memory held by the instance */
+  long long updates_per_step; /* node updates per coarse step */
+  dns_tile tile;              /* tile shape in use */
+} dns_batch_info;
+
+int dns_batch_create(int device, dns_batch **out);
+void dns_batch_destroy(dns_batch *b);
+/* Device bytes an instance of these parameters holds (FP32 form). */
+int dns_batch_footprint(const dns_params *p, long long *bytes);
+/* Tile shape an instance of these parameters gets: the batch's tuning-table
+   entry for its shape if any (b may be NULL), else a fixed default. */
+int dns_batch_tile_for(const dns_batch *b, const dns_params *p, dns_tile *t);
+/* Tuning-table entry for every later instance of the same grid shape. */
+int dns_batch_set_tile(dns_batch *b, const dns_params *shape, const dns_tile *t);
+/* Time `steps` steps of each candidate tile shape on a throw-away instance of
+   this grid shape (in a scratch batch; resident instances are untouched) and
+   store the fastest in the tuning table.  best and ms (per step) may be NULL. */
+int dns_batch_autotune(dns_batch *b, const dns_params *shape, int steps, dns_tile *best, double *ms);
+/* Add a seeded instance (the state dns_init_seeded builds) with a budget of
+   `steps` coarse steps; statistics are sampled every sample_every steps of the
+   instance (0: none).  tile NULL: dns_batch_tile_for.  *id receives a handle. */
+int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *tile, uint64_t seed, double uc, double amp,
+                  long long steps, long long sample_every, int *id);
+/* Release an instance's device memory. */
+int dns_batch_remove(dns_batch *b, int id);
+/* Advance every resident instance with budget left by up to nsteps coarse
+   steps; *active (may be NULL) receives how many still have budget. */
+int dns_batch_run(dns_batch *b, long long nsteps, int *active);
+int dns_batch_info_of(dns_batch *b, int id, dns_batch_info *out);
+/* The instance's statistics, as dns_stats. */
+int dns_batch_stats(dns_batch *b, int id, double *out, long *nsamples);
+/* The instance's post-stream state, as dns_export_state. */
+int dns_batch_export_state(dns_batch *b, int id, int level, double *aos_out);
+/* Log rows [first, first + n) of the instance (rows of steps taken). */
+int dns_batch_log(dns_batch *b, int id, long long first, long long n, dns_step_log *rows);
+/* The batch's CUDA stream (cudaStream_t as void*): run() is ordered on it, so
+   events recorded there bracket a run's device time. */
+int dns_batch_stream(dns_batch *b, void **stream);
+
 /* ---- errors -------------------------------------------------------------- */
 const char *dns_error_string(int code);
 const char *dns_last_error(void);

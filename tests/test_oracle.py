@@ -54,6 +54,38 @@ def test_bicubic_weights_reproduce_cubics():
     np.testing.assert_allclose(W @ np.array(x), c.reshape(-1), atol=1e-12)
 
 
+def test_hermite_tensor_form_equals_bicubic_map():
+    """The FP32 interface evaluates the patch as a tensor product of cubic
+    Hermite bases; with exact rationals it equals the reference's coefficient
+    map followed by the power-series evaluation at every GR-th point."""
+    import importlib.util
+    from fractions import Fraction as Fr
+
+    spec = importlib.util.spec_from_file_location(
+        "gen_bicubic", ROOT / "dns-solvers-with-grid-embedding_b200" / "csrc" / "gen_bicubic.py")
+    gb = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gb)
+    W = gb.weights()
+    rng = np.random.default_rng(7)
+    x = [Fr(int(v), 97) for v in rng.integers(-500, 500, size=16)]  # [V, Dx, Dy, Dxy] x corners
+    coef = [sum(W[r][k] * x[k] for k in range(16)) for r in range(16)]
+    h = [lambda t: 2 * t ** 3 - 3 * t ** 2 + 1, lambda t: -2 * t ** 3 + 3 * t ** 2,
+         lambda t: t ** 3 - 2 * t ** 2 + t, lambda t: t ** 3 - t ** 2]
+    corner = {(0, 0): 0, (1, 0): 1, (1, 1): 2, (0, 1): 3}
+    for gr in (2, 3, 4):
+        for ii in range(gr):
+            for jj in range(gr):
+                t, u = Fr(ii, gr), Fr(jj, gr)
+                power = sum(coef[n * 4 + m] * t ** n * u ** m for n in range(4) for m in range(4))
+                tensor = Fr(0)
+                for a in (0, 1):
+                    for b in (0, 1):
+                        q = corner[(a, b)]
+                        tensor += (h[a](t) * h[b](u) * x[q] + h[2 + a](t) * h[b](u) * x[4 + q]
+                                   + h[a](t) * h[2 + b](u) * x[8 + q] + h[2 + a](t) * h[2 + b](u) * x[12 + q])
+                assert tensor == power, (gr, ii, jj)
+
+
 @pytest.mark.parametrize("case", GOLDEN, ids=lambda c: f"{c['config']}-{c['mode']}")
 def test_port_matches_golden(port, ref_configs, case):
     """CPU restatement reproduces the reference's own output bit for bit."""
