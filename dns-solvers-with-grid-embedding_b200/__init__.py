@@ -69,10 +69,10 @@ LOG_FIELDS = tuple(n for n, _ in StepLog._fields_)
 class Tile(C.Structure):
     """``dns_tile``: tile shape of one batched instance."""
 
-    _fields_ = [("cw", C.c_int), ("cjb", C.c_int), ("fw", C.c_int), ("fjb", C.c_int), ("igroups", C.c_int)]
+    _fields_ = [("cw", C.c_int), ("cjb", C.c_int), ("fw", C.c_int), ("fjb", C.c_int)]
 
     def as_tuple(self):
-        return (self.cw, self.cjb, self.fw, self.fjb, self.igroups)
+        return (self.cw, self.cjb, self.fw, self.fjb)
 
 
 class BatchInfo(C.Structure):

@@ -25,6 +25,7 @@ namespace batch {
 
 constexpr int kMaxInst = 1024;  // resident instances per batch
 constexpr int kLogRows = 64;    // per-instance log ring (>= steps per graph replay)
+constexpr int kFinChunks = 32;  // blocks per instance in the finalize
 
 enum Phase {
   PH_STATS = 0,  // plane statistics of the sampled state (coarse 2..zdc-3, every fine plane)
@@ -34,8 +35,10 @@ enum Phase {
   PH_EXTRACT,    // interface history planes k = 1 and zdc-2
   PH_FBULK,      // fine planes k = 2..zdf-3 of both blocks
   PH_FEDGE,      // the remaining fine planes
-  PH_IFACE,      // interface transfer tiles x walls x population groups
+  PH_ICORNER,    // interface corner data: tiles x walls x fields
+  PH_IEVAL,      // interface evaluation: fine rows x walls
   PH_INJECT,     // fine-to-coarse injection rows
+  PH_FINAL,      // reduction chunks of the finalize
   PH_NPHASE
 };
 
@@ -44,7 +47,7 @@ struct Inst {
   int nx, ny, nzc, nxf, nyf, zdf, zds, gr;
   int cw, cjb, cgx, cgy;  // coarse tile: width (threads in x), row iterations, grid per plane
   int fw, fjb, fgx, fgy;  // fine tile
-  int igx, igy, igroups;  // interface tiles and population groups
+  int igx, igy;           // interface corner tiles
   int egx;                // extraction / injection blocks per row
   int nzp;                // composite profile planes
   int slot;               // row of the batch-level dyn / state / log arrays
@@ -55,9 +58,10 @@ struct Inst {
   int cfr, pad;
   float *fc[2], *ff[2];   // coarse / fine SoA deviations, ping-pong
   float *hist;            // 3 ring slots x [2 walls][23][ny][nx]
+  float4 *corner;         // interface corner data [2 walls][23][ny][nx]
   int8_t *wflag;          // [nyf][nxf]
   double *part;           // block partials
-  long long pc, pf, pi, pw, psc, psf;  // region offsets (doubles) in part
+  long long pc, pf, pi, pw, psc, psf, pl2;  // region offsets (doubles) in part; pl2: finalize level 2
   double *stats;          // [nzp][16] running sums
 };
 
@@ -82,17 +86,17 @@ struct TimeW {
   float an, ap, app;
 };
 
-// Interface tile (coarse cells) per refinement ratio: IfTile<GR> of f32_core.cuh.
-constexpr int iface_tx(int gr) { return gr == 2 ? 32 : (gr == 3 ? 21 : 16); }
-constexpr int iface_ty(int gr) { return gr == 2 ? 8 : (gr == 3 ? 6 : 4); }
+// Interface corner tile (coarse nodes): CTX x CTY of f32_core.cuh.
+constexpr int kCornerTX = 32, kCornerTY = 8;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
-  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, iface, inject, final_;
+  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, icorner, ieval, inject, final_;
 };
 int query_grids(int gr, Grids *g);
-void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, int gr, const Grids &g, cudaStream_t s,
-                 cudaStream_t aux, cudaEvent_t *ev);  // ev: 10 events (fork/join of the two streams)
+// count: one zeroed counter per slot (the finalize resets it)
+void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev);  // ev: 10 events (fork/join of the two streams)
 void tile_counts(const Inst &I, int counts[PH_NPHASE]);
 
 }  // namespace batch

@@ -60,8 +60,7 @@ int pick_width(int n) {
 
 bool width_ok(int w) { return w == 32 || w == 64 || w == 128; }
 bool tile_ok(const dns_tile &t) {
-  return width_ok(t.cw) && width_ok(t.fw) && t.cjb >= 1 && t.cjb <= 64 && t.fjb >= 1 && t.fjb <= 64 &&
-         t.igroups >= 1 && t.igroups <= 19;
+  return width_ok(t.cw) && width_ok(t.fw) && t.cjb >= 1 && t.cjb <= 64 && t.fjb >= 1 && t.fjb <= 64;
 }
 
 dns_tile default_tile(const dns_geometry &g) {
@@ -70,7 +69,6 @@ dns_tile default_tile(const dns_geometry &g) {
   t.cjb = 2;
   t.fw = pick_width(g.nxf);
   t.fjb = 2;
-  t.igroups = 2;
   return t;
 }
 
@@ -101,16 +99,15 @@ void shape_inst(Inst &I, const dns_params &p, const dns_geometry &g, const dns_t
   I.fjb = t.fjb;
   I.fgx = cdiv(g.nxf, t.fw);
   I.fgy = cdiv(g.nyf, (long long)(128 / t.fw) * t.fjb);
-  I.igx = cdiv(g.nx, iface_tx(g.gr));
-  I.igy = cdiv(g.ny, iface_ty(g.gr));
-  I.igroups = t.igroups;
+  I.igx = cdiv(g.nx, kCornerTX);
+  I.igy = cdiv(g.ny, kCornerTY);
   I.egx = cdiv(g.nx, 128);
   I.nzp = g.nz_profile;
 }
 
 struct Layout {
-  size_t fc[2], ff[2], hist, wflag, part, stats, total;
-  long long pc, pf, pi, pw, psc, psf, npart;
+  size_t fc[2], ff[2], hist, corner, wflag, part, stats, total;
+  long long pc, pf, pi, pw, psc, psf, pl2, npart;
 };
 
 size_t take(size_t &off, size_t bytes) {
@@ -128,6 +125,7 @@ Layout layout_of(const Inst &I) {
   L.ff[0] = take(off, nf);
   L.ff[1] = take(off, nf);
   L.hist = take(off, 3ull * 2 * 23 * I.ny * I.nx * 4);
+  L.corner = take(off, 2ull * 23 * I.ny * I.nx * 16);
   L.wflag = take(off, (size_t)I.nyf * I.nxf);
   const long long cb = (long long)I.nzc * I.cgy * I.cgx, fb = 2LL * I.zds * I.fgy * I.fgx,
                   ib = 2LL * I.ny * I.egx;
@@ -138,6 +136,7 @@ Layout layout_of(const Inst &I) {
   L.pw = o; o += fb * 2;
   L.psc = o; o += cb * 9;
   L.psf = o; o += fb * 9;
+  L.pl2 = o; o += (long long)kFinChunks * 18;
   L.npart = o;
   L.part = take(off, (size_t)o * 8);
   L.stats = take(off, (size_t)I.nzp * 16 * 8);
@@ -158,6 +157,7 @@ struct dns_batch {
   Dyn *ddyn = nullptr;
   DevState *dstate = nullptr;
   DevLog *dlog = nullptr;
+  unsigned int *dcount = nullptr;         // finalize counters, one per slot
   Dyn *hdyn[2] = {nullptr, nullptr};      // pinned snapshots
   DevLog *hlog[2] = {nullptr, nullptr};
   Grids grids{};
@@ -181,6 +181,7 @@ static void release(dns_batch *b) {
   cudaFree(b->ddyn);
   cudaFree(b->dstate);
   cudaFree(b->dlog);
+  cudaFree(b->dcount);
   for (int q = 0; q < 2; q++) {
     if (b->hdyn[q]) cudaFreeHost(b->hdyn[q]);
     if (b->hlog[q]) cudaFreeHost(b->hlog[q]);
@@ -213,7 +214,8 @@ extern "C" int dns_batch_create(int device, dns_batch **out) {
   ok = ok && cudaMalloc(&b->dmix, sizeof(Mix)) == cudaSuccess &&
        cudaMalloc(&b->ddyn, sizeof(Dyn) * kMaxInst) == cudaSuccess &&
        cudaMalloc(&b->dstate, sizeof(DevState) * kMaxInst) == cudaSuccess &&
-       cudaMalloc(&b->dlog, sizeof(DevLog) * kMaxInst * kLogRows) == cudaSuccess;
+       cudaMalloc(&b->dlog, sizeof(DevLog) * kMaxInst * kLogRows) == cudaSuccess &&
+       cudaMalloc(&b->dcount, sizeof(unsigned int) * kMaxInst) == cudaSuccess;
   for (int q = 0; q < 2; q++)
     ok = ok && cudaMallocHost(&b->hdyn[q], sizeof(Dyn) * kMaxInst) == cudaSuccess &&
          cudaMallocHost(&b->hlog[q], sizeof(DevLog) * kMaxInst * kLogRows) == cudaSuccess;
@@ -225,6 +227,7 @@ extern "C" int dns_batch_create(int device, dns_batch **out) {
   cudaMemset(b->ddyn, 0, sizeof(Dyn) * kMaxInst);
   cudaMemset(b->dstate, 0, sizeof(DevState) * kMaxInst);
   cudaMemset(b->dlog, 0, sizeof(DevLog) * kMaxInst * kLogRows);
+  cudaMemset(b->dcount, 0, sizeof(unsigned int) * kMaxInst);
   // keep freed instance memory in the stream-ordered pool for the next admission
   cudaMemPool_t pool;
   if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
@@ -272,7 +275,7 @@ extern "C" int dns_batch_tile_for(const dns_batch *b, const dns_params *p, dns_t
 
 extern "C" int dns_batch_set_tile(dns_batch *b, const dns_params *shape, const dns_tile *t) {
   if (!b || !shape || !t) return fail_with(DNS_EINVAL, "null argument");
-  if (!tile_ok(*t)) return fail_with(DNS_EINVAL, "tile widths must be 32, 64 or 128, row iterations 1..64, groups 1..19");
+  if (!tile_ok(*t)) return fail_with(DNS_EINVAL, "tile widths must be 32, 64 or 128, row iterations 1..64");
   b->tuned[key_of(*shape)] = *t;
   return DNS_OK;
 }
@@ -317,6 +320,7 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
     I.ff[k] = reinterpret_cast<float *>(base + L.ff[k]);
   }
   I.hist = reinterpret_cast<float *>(base + L.hist);
+  I.corner = reinterpret_cast<float4 *>(base + L.corner);
   I.wflag = reinterpret_cast<int8_t *>(base + L.wflag);
   I.part = reinterpret_cast<double *>(base + L.part);
   I.pc = L.pc;
@@ -325,6 +329,7 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
   I.pw = L.pw;
   I.psc = L.psc;
   I.psf = L.psf;
+  I.pl2 = L.pl2;
   I.stats = reinterpret_cast<double *>(base + L.stats);
   I.sample_every = sample_every;
   I.om_c = (float)g.omega_c;
@@ -427,7 +432,7 @@ static int capture(dns_batch *b, int steps, cudaGraphExec_t *out) {
   cudaGraph_t graph = nullptr;
   BTRY(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
   for (int q = 0; q < steps; q++)
-    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->gr, b->grids, b->s, b->aux, b->ev);
+    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->dcount, b->gr, b->grids, b->s, b->aux, b->ev);
   cudaError_t e = cudaStreamEndCapture(b->s, &graph);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   e = cudaGraphInstantiate(out, graph, 0);
@@ -593,7 +598,7 @@ extern "C" int dns_batch_log(dns_batch *b, int id, long long first, long long n,
 // ---------------------------------------------------------------- autotuner
 // Coordinate search over the tile shape on a throw-away instance of the
 // shape: the fine tile first (the fine kernels carry most of the traffic),
-// then the coarse tile, then the interface grouping; each candidate is timed
+// then the coarse tile; each candidate is timed
 // over `steps` steps with CUDA events after two warm-up steps.
 static int time_tile(int device, const dns_params &p, const dns_tile &t, int steps, double *ms) {
   dns_batch *sb = nullptr;
@@ -641,7 +646,7 @@ extern "C" int dns_batch_autotune(dns_batch *b, const dns_params *shape, int ste
     }
     return DNS_OK;
   };
-  const int widths[3] = {32, 64, 128}, iters[3] = {1, 2, 4}, groups[4] = {1, 2, 4, 19};
+  const int widths[3] = {32, 64, 128}, iters[3] = {1, 2, 4};
   dns_tile base = cur;
   for (int w : widths)
     for (int j : iters) {
@@ -660,13 +665,6 @@ extern "C" int dns_batch_autotune(dns_batch *b, const dns_params *shape, int ste
       if (t.cw == base.cw && t.cjb == base.cjb) continue;
       if ((rc = consider(t))) return rc;
     }
-  base = cur;
-  for (int gq : groups) {
-    dns_tile t = base;
-    t.igroups = gq;
-    if (t.igroups == base.igroups) continue;
-    if ((rc = consider(t))) return rc;
-  }
   b->tuned[key_of(q)] = cur;
   if (best) *best = cur;
   if (ms) *ms = cur_ms;

@@ -16,9 +16,7 @@ namespace {
 
 using namespace f32;
 
-static_assert(IfTile<2>::TX == iface_tx(2) && IfTile<2>::TY == iface_ty(2) && IfTile<3>::TX == iface_tx(3) &&
-                  IfTile<3>::TY == iface_ty(3) && IfTile<4>::TX == iface_tx(4) && IfTile<4>::TY == iface_ty(4),
-              "host and device interface tiles");
+static_assert(CTX == kCornerTX && CTY == kCornerTY, "host and device interface tiles");
 
 // advance s to the instance owning item w (items are walked in increasing order)
 __device__ __forceinline__ int owner(const int *__restrict__ st, int n, int w, int s) {
@@ -305,12 +303,32 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
 }
 
 // ------------------------------------------------------------------ interface
-template <int GR>
-__global__ void __launch_bounds__(kThreads) b_iface(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
-                                                    TimeW tw) {
-  __shared__ IfSmem32<GR> S;
+// the item's parameters, built in shared memory by thread 0 (not registers)
+__device__ __forceinline__ void iface_params_of(IfParams32 &P, const Inst &I, const Dyn &D, int sub, const TimeW &tw) {
+  const size_t hs = (size_t)2 * 23 * I.ny * I.nx;
+  // ring after this step's rotation: n in the old pp slot, p in old n, pp in old p
+  P.hn = I.hist + (size_t)D.hpp * hs;
+  P.hp = I.hist + (size_t)D.hn * hs;
+  P.hpp = I.hist + (size_t)D.hp * hs;
+  P.corner = I.corner;
+  P.fdst = I.ff[D.cf ^ (sub & 1)];
+  P.nx = I.nx;
+  P.ny = I.ny;
+  P.nxf = I.nxf;
+  P.nyf = I.nyf;
+  P.zds = I.zds;
+  P.an = tw.an;
+  P.ap = tw.ap;
+  P.app = tw.app;
+  P.fac = I.fac_if;
+}
+
+__global__ void __launch_bounds__(kThreads) b_icorner(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
+                                                      TimeW tw) {
+  __shared__ IfCornerSmem S;
+  __shared__ IfParams32 P;
   const int n = M->n;
-  const int *st = M->start[PH_IFACE];
+  const int *st = M->start[PH_ICORNER];
   const int total = st[n];
   int s = 0;
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -326,24 +344,38 @@ __global__ void __launch_bounds__(kThreads) b_iface(const Mix *__restrict__ M, c
     local /= I.igx;
     const int ty = local % I.igy;
     local /= I.igy;
-    const int G = I.igroups, g = local % G, wall = local / G;
-    const size_t hs = (size_t)2 * 23 * I.ny * I.nx;
-    IfParams32 P;
-    // ring after this step's rotation: n in the old pp slot, p in old n, pp in old p
-    P.hn = I.hist + (size_t)D.hpp * hs;
-    P.hp = I.hist + (size_t)D.hn * hs;
-    P.hpp = I.hist + (size_t)D.hp * hs;
-    P.fdst = I.ff[D.cf ^ (sub & 1)];
-    P.nx = I.nx;
-    P.ny = I.ny;
-    P.nxf = I.nxf;
-    P.nyf = I.nyf;
-    P.zds = I.zds;
-    P.an = tw.an;
-    P.ap = tw.ap;
-    P.app = tw.app;
-    P.fac = I.fac_if;
-    iface_tile32<GR>(S, P, tx, ty, wall, 19 * g / G, 19 * (g + 1) / G);
+    const int wall = local / 23, field = local - wall * 23;
+    if (threadIdx.x == 0) iface_params_of(P, I, D, sub, tw);
+    __syncthreads();
+    iface_corner_tile32(S, P, tx, ty, wall, field);  // ends with a barrier
+  }
+}
+
+template <int GR>
+__global__ void __launch_bounds__(kThreads) b_ieval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
+                                                    TimeW tw) {
+  __shared__ IfParams32 P;
+  const int n = M->n;
+  const int *st = M->start[PH_IEVAL];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int local = w - st[s];
+    const int gx = (I.nxf + kThreads - 1) / kThreads;
+    const int row = local / gx, bx = local - row * gx;
+    const int wall = row / I.nyf, J = row - wall * I.nyf;
+    __syncthreads();  // the previous item is done with P
+    if (threadIdx.x == 0) iface_params_of(P, I, D, sub, tw);
+    __syncthreads();
+    const int Ii = bx * kThreads + threadIdx.x;
+    if (Ii < P.nxf) iface_node32<GR>(P, Ii, J, wall);
   }
 }
 
@@ -394,88 +426,110 @@ __global__ void __launch_bounds__(kThreads) b_inject(const Mix *__restrict__ M, 
 }
 
 // ------------------------------------------------------------------ finalize
-// One block per instance: the instance's block partials in a fixed order ->
-// log row, encalc2 values and force of the next step; then the step's
-// parity, history ring and counters advance.
+// Per instance, kFinChunks blocks each reduce a fixed chunk of every partial
+// region (fixed order) into the instance's level-2 row; the last of them to
+// finish sums the rows in chunk order and writes the log row, the encalc2
+// values and force of the next step, then advances the step's parity,
+// history ring and counters.  Deterministic, one launch, no waiting.
 constexpr int kFinComp = 18;
 
 __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, Dyn *__restrict__ dyn,
-                                                   DevState *__restrict__ state, DevLog *__restrict__ log) {
+                                                   DevState *__restrict__ state, DevLog *__restrict__ log,
+                                                   unsigned int *__restrict__ count) {
   __shared__ double sh[kFinComp][kThreads];
+  __shared__ bool last;
   const int n = M->n;
-  for (int s = blockIdx.x; s < n; s += gridDim.x) {
+  const int *st = M->start[PH_FINAL];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
     const Inst &I = M->inst[s];
     Dyn D = dyn[I.slot];
-    if (D.remaining <= 0) continue;
+    if (D.remaining <= 0) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    const int c = w - st[s];
     double v[kFinComp];
 #pragma unroll
-    for (int c = 0; c < kFinComp; c++) v[c] = 0.;
+    for (int q = 0; q < kFinComp; q++) v[q] = 0.;
     const long nc = (long)I.nzc * I.cgy * I.cgx, nf = (long)2 * I.zds * I.fgy * I.fgx;
     const long ni = (long)2 * I.ny * I.egx, wn = (long)I.fgy * I.fgx;
     const double *P = I.part;
-    for (long q = threadIdx.x; q < nc; q += kThreads) {
-      v[0] += P[I.pc + q * 2];
-      v[1] += P[I.pc + q * 2 + 1];
-    }
-    for (long q = threadIdx.x; q < nf; q += kThreads) {
-      v[2] += P[I.pf + q * 2];
-      v[3] += P[I.pf + q * 2 + 1];
-    }
-    for (long q = threadIdx.x; q < ni; q += kThreads) {
-      v[4] += P[I.pi + q * 2];
-      v[5] += P[I.pi + q * 2 + 1];
-    }
+    auto chunk = [&](long long off, long cnt, int q0) {
+      const long lo = cnt * c / kFinChunks, hi = cnt * (c + 1) / kFinChunks;
+      for (long q = lo + threadIdx.x; q < hi; q += kThreads) {
+        v[q0] += P[off + q * 2];
+        v[q0 + 1] += P[off + q * 2 + 1];
+      }
+    };
+    chunk(I.pc, nc, 0);
+    chunk(I.pf, nf, 2);
+    chunk(I.pi, ni, 4);
     const int zds = I.zds, zdf = I.zdf;
     const int planes[6] = {0, 1, 2, zds + zdf - 2, zds + zdf - 3, zds + zdf - 4};
 #pragma unroll
-    for (int c = 0; c < 6; c++) {
-      const double *pw = P + I.pw + (size_t)planes[c] * wn * 2;
-      for (long q = threadIdx.x; q < wn; q += kThreads) {
-        v[6 + 2 * c] += pw[q * 2];
-        v[7 + 2 * c] += pw[q * 2 + 1];
-      }
-    }
+    for (int q = 0; q < 6; q++) chunk(I.pw + (long long)planes[q] * wn * 2, wn, 6 + 2 * q);
 #pragma unroll
-    for (int c = 0; c < kFinComp; c++) sh[c][threadIdx.x] = v[c];
+    for (int q = 0; q < kFinComp; q++) sh[q][threadIdx.x] = v[q];
     __syncthreads();
     for (int o = kThreads / 2; o > 0; o >>= 1) {
       if (threadIdx.x < o)
 #pragma unroll
-        for (int c = 0; c < kFinComp; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + o];
+        for (int q = 0; q < kFinComp; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
       __syncthreads();
     }
+    double *l2 = I.part + I.pl2;
     if (threadIdx.x == 0) {
-      double S[kFinComp];
-      for (int c = 0; c < kFinComp; c++) S[c] = sh[c][0];
-      DevState &X = state[I.slot];
-      DevLog r;
-      r.force = X.force;
-      r.momentum = X.momentum;
-      r.denst = X.denst;
-      r.flowrate = X.momentum * I.flow_scale / X.denst;
-      const double *U = S + 6;  // (U, D) per plane: lower k = 1, 2, 3; upper zdf-2, zdf-3, zdf-4
-      const double stdown = ((-2. * U[0] + 3. * U[2] - U[4]) / I.norm2) * (I.mu * (U[1] / I.norm2));
-      const double stup = (-(2. * U[6] - 3. * U[8] + U[10]) / I.norm2) * (I.mu * (U[11] / I.norm2));
-      r.stup = stup;
-      r.stdown = stdown;
-      r.stress = 0.5 * (stup + stdown);
-      r.pgrad = X.force * I.pgrad_scale;
-      log[(size_t)I.slot * kLogRows + (size_t)(D.step % kLogRows)] = r;
-      const double mom = (I.g3 * S[0] + 0.5 * I.g3 * S[4] + S[2]) / I.norm;
-      const double den = (I.g3 * S[1] + 0.5 * I.g3 * S[5] + S[3] + I.den_offset) / I.norm;
-      X.momentum = mom;
-      X.denst = den;
-      X.force = I.cfr ? I.ub - mom : I.gconst;
-      // xcomputations.c:548-556 (history rotation); exchange.c / fexchange.c (pointer swaps)
-      const int t = D.hpp;
-      D.hpp = D.hp;
-      D.hp = D.hn;
-      D.hn = t;
-      D.cc ^= 1;
-      D.cf ^= (I.gr & 1);
-      D.step += 1;
-      D.remaining -= 1;
-      dyn[I.slot] = D;
+      for (int q = 0; q < kFinComp; q++) l2[c * kFinComp + q] = sh[q][0];
+      __threadfence();
+      last = atomicAdd(count + I.slot, 1u) == (unsigned)(kFinChunks - 1);
+    }
+    __syncthreads();
+    if (last) {
+      __threadfence();
+      if (threadIdx.x < kFinComp) {
+        const volatile double *L = l2;
+        double a = 0.;
+        for (int q = 0; q < kFinChunks; q++) a += L[q * kFinComp + threadIdx.x];
+        sh[threadIdx.x][0] = a;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        double S[kFinComp];
+        for (int q = 0; q < kFinComp; q++) S[q] = sh[q][0];
+        DevState &X = state[I.slot];
+        DevLog r;
+        r.force = X.force;
+        r.momentum = X.momentum;
+        r.denst = X.denst;
+        r.flowrate = X.momentum * I.flow_scale / X.denst;
+        const double *U = S + 6;  // (U, D) per plane: lower k = 1, 2, 3; upper zdf-2, zdf-3, zdf-4
+        const double stdown = ((-2. * U[0] + 3. * U[2] - U[4]) / I.norm2) * (I.mu * (U[1] / I.norm2));
+        const double stup = (-(2. * U[6] - 3. * U[8] + U[10]) / I.norm2) * (I.mu * (U[11] / I.norm2));
+        r.stup = stup;
+        r.stdown = stdown;
+        r.stress = 0.5 * (stup + stdown);
+        r.pgrad = X.force * I.pgrad_scale;
+        log[(size_t)I.slot * kLogRows + (size_t)(D.step % kLogRows)] = r;
+        const double mom = (I.g3 * S[0] + 0.5 * I.g3 * S[4] + S[2]) / I.norm;
+        const double den = (I.g3 * S[1] + 0.5 * I.g3 * S[5] + S[3] + I.den_offset) / I.norm;
+        X.momentum = mom;
+        X.denst = den;
+        X.force = I.cfr ? I.ub - mom : I.gconst;
+        // xcomputations.c:548-556 (history rotation); exchange.c / fexchange.c (pointer swaps)
+        const int t = D.hpp;
+        D.hpp = D.hp;
+        D.hp = D.hn;
+        D.hn = t;
+        D.cc ^= 1;
+        D.cf ^= (I.gr & 1);
+        D.step += 1;
+        D.remaining -= 1;
+        dyn[I.slot] = D;
+        count[I.slot] = 0u;
+      }
     }
     __syncthreads();
   }
@@ -502,8 +556,10 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   c[PH_EXTRACT] = 2 * I.ny * I.egx;
   c[PH_FBULK] = 2 * (I.zds - 3) * fb;
   c[PH_FEDGE] = 6 * fb;
-  c[PH_IFACE] = 2 * I.igroups * I.igx * I.igy;
+  c[PH_ICORNER] = 2 * 23 * I.igx * I.igy;
+  c[PH_IEVAL] = 2 * I.nyf * ((I.nxf + kThreads - 1) / kThreads);
   c[PH_INJECT] = 2 * I.ny * I.egx;
+  c[PH_FINAL] = kFinChunks;
 }
 
 int query_grids(int gr, Grids *g) {
@@ -515,9 +571,10 @@ int query_grids(int gr, Grids *g) {
   rc |= occupancy_grid(b_extract, &g->extract);
   rc |= occupancy_grid(b_fine<1, true>, &g->fbulk);
   rc |= occupancy_grid(b_fine<3, false>, &g->fedge);
-  if (gr == 2) rc |= occupancy_grid(b_iface<2>, &g->iface);
-  else if (gr == 3) rc |= occupancy_grid(b_iface<3>, &g->iface);
-  else rc |= occupancy_grid(b_iface<4>, &g->iface);
+  rc |= occupancy_grid(b_icorner, &g->icorner);
+  if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
+  else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
+  else rc |= occupancy_grid(b_ieval<4>, &g->ieval);
   rc |= occupancy_grid(b_inject, &g->inject);
   rc |= occupancy_grid(b_final, &g->final_);
   return rc;
@@ -553,9 +610,10 @@ static TimeW time_weights(int sub, int gr) {
 
 static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, cudaStream_t s) {
   const TimeW tw = time_weights(sub, gr);
-  if (gr == 2) b_iface<2><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
-  else if (gr == 3) b_iface<3><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
-  else b_iface<4><<<g.iface, kThreads, 0, s>>>(m, dyn, sub, tw);
+  b_icorner<<<g.icorner, kThreads, 0, s>>>(m, dyn, sub, tw);
+  if (gr == 2) b_ieval<2><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else if (gr == 3) b_ieval<3><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else b_ieval<4><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
 }
 
 // One coarse step of every resident instance on two streams, with the
@@ -564,8 +622,8 @@ static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g
 //   aux: [start] fine(1), [iface(1)] fine(2) ..., inject
 // The statistics read the state fine(2) and iface(2) overwrite; both follow
 // iface(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject.
-void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, int gr, const Grids &g, cudaStream_t s,
-                 cudaStream_t aux, cudaEvent_t *ev) {
+void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev) {
   cudaEventRecord(ev[0], s);
   cudaStreamWaitEvent(aux, ev[0], 0);
   b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
@@ -585,7 +643,7 @@ void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, int gr, c
   b_inject<<<g.inject, kThreads, 0, aux>>>(m, dyn);
   cudaEventRecord(ev[9], aux);
   cudaStreamWaitEvent(s, ev[9], 0);
-  b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log);
+  b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log, count);
 }
 
 }  // namespace batch

@@ -69,7 +69,7 @@ struct dns_handle {
   DevLog *dlog = nullptr;              // kLogCap rows
   DevLog *hlog = nullptr;              // pinned mirror
   double *stats_acc = nullptr;         // [nz_profile][16]
-  double *iface_mac = nullptr;         // interface rho, u at fine nodes [2][4][nyf][nxf]
+  double *iface_mac = nullptr;         // FP64: interface rho, u [2][4][nyf][nxf]; FP32: corner data
   unsigned int *fin_counter = nullptr; // finalize's block counter
   cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
   cudaStream_t hip = nullptr;          // interface transfers (highest priority)
@@ -232,7 +232,8 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   PartialLayout pl = partial_layout(d, s);
   const long long nc = 19LL * g->nzc * g->ny * g->nx, nf = 19LL * 2 * p->zds * g->nyf * g->nxf;
   const long long esz = p->precision == DNS_FP32 ? 4 : 8;  // bytes per stored population
-  g->device_bytes = esz * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + 8LL * g->nyf * g->nxf) +
+  const long long mac = esz == 4 ? 2LL * 23 * g->ny * g->nx * 4 : 8LL * g->nyf * g->nxf;  // elements of esz
+  g->device_bytes = esz * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + mac) +
                     8 * (pl.total + 16LL * g->nz_profile) +
                     (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
   return DNS_OK;
@@ -333,7 +334,9 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   if ((rc = alloc((void **)&h->state, sizeof(DevState)))) return rc;
   if ((rc = alloc((void **)&h->dlog, kLogCap * sizeof(DevLog)))) return rc;
   if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * 16 * 8))) return rc;
-  if ((rc = alloc((void **)&h->iface_mac, 8ull * g.nyf * g.nxf * esz))) return rc;
+  // FP64: interface rho, u at fine nodes; FP32: corner values and derivatives (float4)
+  const size_t mac_bytes = esz == 4 ? 2ull * 23 * g.ny * g.nx * 16 : 8ull * g.nyf * g.nxf * esz;
+  if ((rc = alloc((void **)&h->iface_mac, mac_bytes))) return rc;
   if ((rc = alloc((void **)&h->fin_counter, 256))) return rc;
   cudaMemset(h->fin_counter, 0, 256);
   if (cudaMallocHost((void **)&h->hlog, kLogCap * sizeof(DevLog)) != cudaSuccess) {

@@ -34,10 +34,6 @@ constexpr int kThreads = 128;
 #ifndef DNS_F32_FUSED
 #define DNS_F32_FUSED 1
 #endif
-// population groups per (tile, wall) of the interface transfer (1..19)
-#ifndef DNS_F32_IFACE_GROUPS
-#define DNS_F32_IFACE_GROUPS 2
-#endif
 
 __device__ __forceinline__ int wrapf(int v, int n) {
   v %= n;
@@ -295,39 +291,26 @@ __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size
 }
 
 // ------------------------------------------------------------------ interface
-// Coarse-to-fine transfer of one tile of interface cells (ctfdtransfer_opt.c,
-// tinterpolate_hrmt.c, derivative.c, bcucof_opt.c).  Per field: the three
-// history levels are combined with the Hermite-in-time weights, the fourth-order
-// x, y and cross derivatives are formed at the tile's cell corners, and every
-// fine node of the tile is evaluated from its cell's bicubic patch.  The patch
-// with unit spacing matching value, d/dx, d/dy and d2/dxdy at the four corners
-// is the tensor product of the cubic Hermite basis
-//   h00(t) = 2t^3 - 3t^2 + 1, h01(t) = -2t^3 + 3t^2, h10(t) = t^3 - 2t^2 + t, h11(t) = t^3 - t^2,
-// so p(t, u) = sum_{a,b in 0,1} [h0a(t) h0b(u) V + h1a(t) h0b(u) Dx + h0a(t) h1b(u) Dy + h1a(t) h1b(u) Dxy]
-// at corner (a, b): the same polynomial as the 16 coefficients of the
-// reference's bicubic map, evaluated in 20 multiply-adds per node instead of
-// 256 + 16.  The FP32 form keeps its own rounding order (it is compared with
-// the FP64 oracle within a tolerance, not bit for bit).
+// Coarse-to-fine transfer (ctfdtransfer_opt.c, tinterpolate_hrmt.c,
+// derivative.c, bcucof_opt.c) in two fully parallel passes per substep:
 //
-// Tile: TX x TY coarse cells; the fine tile is GR*TX (<= 64) columns wide and
-// thread t evaluates fine column (t & 63) of rows (t >> 6) + 2r, r < NR.
-template <int GR>
-struct IfTile;
-template <>
-struct IfTile<2> {
-  static constexpr int TX = 32, TY = 8;
-};
-template <>
-struct IfTile<3> {
-  static constexpr int TX = 21, TY = 6;
-};
-template <>
-struct IfTile<4> {
-  static constexpr int TX = 16, TY = 4;
-};
-
+//  1. corner data: for every (tile, wall, field) the three history levels are
+//     combined with the Hermite-in-time weights and the fourth-order x, y and
+//     cross derivatives formed in shared memory; each coarse interface node
+//     gets C = (value, d/dx, d/dy, d2/dxdy) as one float4 [2][23][ny][nx].
+//  2. evaluation: one thread per fine interface node reads its cell's four
+//     corners per field and evaluates the bicubic patch as the tensor product
+//     of the cubic Hermite basis
+//       h00(t) = 2t^3 - 3t^2 + 1, h01(t) = -2t^3 + 3t^2, h10(t) = t^3 - 2t^2 + t, h11(t) = t^3 - t^2,
+//       p(t, u) = sum_{a,b in 0,1} [h0a(t) h0b(u) V + h1a(t) h0b(u) Dx + h0a(t) h1b(u) Dy + h1a(t) h1b(u) Dxy],
+//     the polynomial the reference's 16-coefficient map gives at unit spacing
+//     (20 multiply-adds per node instead of 256 + 16); then
+//     f_a = feq_a(rho^, u^) + fac fneq^_a into the wall's interface plane.
+// The FP32 form keeps its own rounding order (it is compared with the FP64
+// oracle within a tolerance, not bit for bit).
 struct IfParams32 {
   const float *hn, *hp, *hpp;  // history slots of levels n, p, pp: [2 walls][23][ny][nx]
+  float4 *corner;              // corner data [2 walls][23][ny][nx]
   float *fdst;                 // fine lattice receiving the interface planes
   int nx, ny, nxf, nyf, zds;
   float an, ap, app;           // Hermite-in-time weights of levels n, p, pp
@@ -335,8 +318,8 @@ struct IfParams32 {
 };
 
 // launch parameters of one substep's transfer (substep s of GR: time s/GR)
-inline IfParams32 iface_params32(const float *hn, const float *hp, const float *hpp, float *fdst, const Dims &d,
-                                 int substep, double omega_c, double omega_f) {
+inline IfParams32 iface_params32(const float *hn, const float *hp, const float *hpp, float4 *corner, float *fdst,
+                                 const Dims &d, int substep, double omega_c, double omega_f) {
   // value = h00 p + h10 (n - pp)/2 + h01 n + h11 (3n - 4p + pp)/2 (tinterpolate_hrmt.c:28-34),
   // gathered per level
   const double t = (double)substep / (double)d.gr, t2 = t * t, t3 = t2 * t;
@@ -345,6 +328,7 @@ inline IfParams32 iface_params32(const float *hn, const float *hp, const float *
   P.hn = hn;
   P.hp = hp;
   P.hpp = hpp;
+  P.corner = corner;
   P.fdst = fdst;
   P.nx = d.nx;
   P.ny = d.ny;
@@ -358,102 +342,65 @@ inline IfParams32 iface_params32(const float *hn, const float *hp, const float *
   return P;
 }
 
-template <int GR>
-struct IfSmem32 {
-  static constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY;
-  float V[TY + 5][TX + 5];
-  float DY[TY + 1][TX + 5];
-  float4 C[TY + 1][TX + 1];  // value, d/dx, d/dy, d2/dxdy at the cell corners
+// pass 1 tile: CTX x CTY interface nodes
+constexpr int CTX = 32, CTY = 8;
+struct IfCornerSmem {
+  float V[CTY + 4][CTX + 4];
+  float DY[CTY][CTX + 4];
 };
 
-// Staging of one field: the thread's share of the tile-plus-halo values is
-// prefetched into registers (offsets into a history plane precomputed once per
-// tile, with the periodic wrap), written as the time-interpolated value, and
-// the corner derivatives are formed in shared memory.
-template <int GR>
-struct IfStage {
-  static constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, QX = TX + 5, QY = TY + 5;
-  static constexpr int NV = (QX * QY + kThreads - 1) / kThreads;
-  int off[NV];                    // offset into a history plane, -1: no slot
-  float vn[NV], vp[NV], vpp[NV];  // prefetched levels n, p, pp
-  __device__ __forceinline__ void init(const IfParams32 &P, int i0, int j0) {
+__device__ __forceinline__ void iface_corner_tile32(IfCornerSmem &S, const IfParams32 &P, int tx, int ty, int w,
+                                                    int field) {
+  constexpr int QX = CTX + 4, QY = CTY + 4;
+  const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
+  const int i0 = tx * CTX, j0 = ty * CTY;
+  const size_t plane = (size_t)P.ny * P.nx, fo = ((size_t)w * 23 + field) * plane;
+  // the last substep (t = 1) is level n alone
+  const bool one = P.ap == 0.f && P.app == 0.f;
+  const float *hn = P.hn + fo, *hp = P.hp + fo, *hpp = P.hpp + fo;
 #pragma unroll
-    for (int s = 0; s < NV; s++) {
-      const int q = threadIdx.x + s * kThreads;
-      off[s] = -1;
-      if (q < QX * QY) {
-        const int pi = q % QX, pj = q / QX;
-        off[s] = wrapf(j0 - 2 + pj, P.ny) * P.nx + wrapf(i0 - 2 + pi, P.nx);
-      }
+  for (int s = 0; s < (QX * QY + kThreads - 1) / kThreads; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    if (q < QX * QY) {
+      const int pi = q % QX, pj = q / QX;
+      const int g = wrapf(j0 - 2 + pj, P.ny) * P.nx + wrapf(i0 - 2 + pi, P.nx);
+      S.V[pj][pi] = one ? __ldg(hn + g) : P.an * __ldg(hn + g) + P.ap * __ldg(hp + g) + P.app * __ldg(hpp + g);
     }
   }
-  __device__ __forceinline__ void prefetch(const float *__restrict__ hn, const float *__restrict__ hp,
-                                           const float *__restrict__ hpp) {
+  __syncthreads();
 #pragma unroll
-    for (int s = 0; s < NV; s++)
-      if (off[s] >= 0) {
-        vn[s] = __ldg(hn + off[s]);
-        vp[s] = __ldg(hp + off[s]);
-        vpp[s] = __ldg(hpp + off[s]);
-      }
-  }
-  __device__ __forceinline__ void build(IfSmem32<GR> &S, const IfParams32 &P) {
-    const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
-    float *V = &S.V[0][0];
-#pragma unroll
-    for (int s = 0; s < NV; s++)
-      if (off[s] >= 0) V[threadIdx.x + s * kThreads] = P.an * vn[s] + P.ap * vp[s] + P.app * vpp[s];
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < (QX * (TY + 1) + kThreads - 1) / kThreads; s++) {
-      const int q = threadIdx.x + s * kThreads;
-      if (q < QX * (TY + 1)) {
-        const int pi = q % QX, r = q / QX;
-        S.DY[r][pi] = c2o3 * (S.V[r + 3][pi] - S.V[r + 1][pi]) - c1o12 * (S.V[r + 4][pi] - S.V[r][pi]);
-      }
+  for (int s = 0; s < (QX * CTY + kThreads - 1) / kThreads; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    if (q < QX * CTY) {
+      const int pi = q % QX, r = q / QX;
+      S.DY[r][pi] = c2o3 * (S.V[r + 3][pi] - S.V[r + 1][pi]) - c1o12 * (S.V[r + 4][pi] - S.V[r][pi]);
     }
-    __syncthreads();
-#pragma unroll
-    for (int s = 0; s < ((TX + 1) * (TY + 1) + kThreads - 1) / kThreads; s++) {
-      const int q = threadIdx.x + s * kThreads;
-      if (q < (TX + 1) * (TY + 1)) {
-        const int c = q % (TX + 1), r = q / (TX + 1);
-        const float dx =
-            c2o3 * (S.V[r + 2][c + 3] - S.V[r + 2][c + 1]) - c1o12 * (S.V[r + 2][c + 4] - S.V[r + 2][c]);
-        const float dxy = c2o3 * (S.DY[r][c + 3] - S.DY[r][c + 1]) - c1o12 * (S.DY[r][c + 4] - S.DY[r][c]);
-        S.C[r][c] = make_float4(S.V[r + 2][c + 2], dx, S.DY[r][c + 2], dxy);
-      }
-    }
-    __syncthreads();
   }
-};
+  __syncthreads();
+  float4 *out = P.corner + fo;
+#pragma unroll
+  for (int s = 0; s < CTX * CTY / kThreads; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    const int c = q % CTX, r = q / CTX;
+    if (i0 + c < P.nx && j0 + r < P.ny) {
+      const float dx = c2o3 * (S.V[r + 2][c + 3] - S.V[r + 2][c + 1]) - c1o12 * (S.V[r + 2][c + 4] - S.V[r + 2][c]);
+      const float dxy = c2o3 * (S.DY[r][c + 3] - S.DY[r][c + 1]) - c1o12 * (S.DY[r][c + 4] - S.DY[r][c]);
+      out[(size_t)(j0 + r) * P.nx + i0 + c] = make_float4(S.V[r + 2][c + 2], dx, S.DY[r][c + 2], dxy);
+    }
+  }
+  __syncthreads();  // the tile's shared memory may be reused by the next item
+}
 
 struct Herm {
   float a0, a1, b0, b1;  // h00, h01, h10, h11
 };
-__host__ __device__ constexpr float herm_c(int which, int j, int gr) {
-  return which == 0   ? 2.f * (float)(j * j * j) / (float)(gr * gr * gr) - 3.f * (float)(j * j) / (float)(gr * gr) + 1.f
-         : which == 1 ? -2.f * (float)(j * j * j) / (float)(gr * gr * gr) + 3.f * (float)(j * j) / (float)(gr * gr)
-         : which == 2 ? (float)(j * j * j) / (float)(gr * gr * gr) - 2.f * (float)(j * j) / (float)(gr * gr) +
-                            (float)j / (float)gr
-                      : (float)(j * j * j) / (float)(gr * gr * gr) - (float)(j * j) / (float)(gr * gr);
-}
-// basis at t = j / GR, j < GR <= 4: [GR - 2][j][h00 h01 h10 h11]
-#define DNS_HERM_ROW(j, g) {herm_c(0, j, g), herm_c(1, j, g), herm_c(2, j, g), herm_c(3, j, g)}
-#define DNS_HERM_GR(g) {DNS_HERM_ROW(0, g), DNS_HERM_ROW(1, g), DNS_HERM_ROW(2, g), DNS_HERM_ROW(3, g)}
-static __constant__ float c_herm[3][4][4] = {DNS_HERM_GR(2), DNS_HERM_GR(3), DNS_HERM_GR(4)};
-#undef DNS_HERM_GR
-#undef DNS_HERM_ROW
-template <int GR>
-__device__ __forceinline__ Herm herm_at(int j) {
-  return Herm{c_herm[GR - 2][j][0], c_herm[GR - 2][j][1], c_herm[GR - 2][j][2], c_herm[GR - 2][j][3]};
+__device__ __forceinline__ Herm herm_at(float t) {
+  const float t2 = t * t, t3 = t2 * t;
+  return Herm{2.f * t3 - 3.f * t2 + 1.f, -2.f * t3 + 3.f * t2, t3 - 2.f * t2 + t, t3 - t2};
 }
 
-// patch value at local cell (cx, cy) with basis hx (in x) and hy (in y)
-template <int GR>
-__device__ __forceinline__ float if_eval32(const IfSmem32<GR> &S, int cx, int cy, const Herm &hx, const Herm &hy) {
-  const float4 c00 = S.C[cy][cx], c10 = S.C[cy][cx + 1], c01 = S.C[cy + 1][cx], c11 = S.C[cy + 1][cx + 1];
-  // along x on the two corner rows: value part P and d/dy part Q
+__device__ __forceinline__ float patch32(const float4 &c00, const float4 &c10, const float4 &c01, const float4 &c11,
+                                         const Herm &hx, const Herm &hy) {
   const float p0 = hx.a0 * c00.x + hx.a1 * c10.x + hx.b0 * c00.y + hx.b1 * c10.y;
   const float q0 = hx.a0 * c00.z + hx.a1 * c10.z + hx.b0 * c00.w + hx.b1 * c10.w;
   const float p1 = hx.a0 * c01.x + hx.a1 * c11.x + hx.b0 * c01.y + hx.b1 * c11.y;
@@ -461,96 +408,32 @@ __device__ __forceinline__ float if_eval32(const IfSmem32<GR> &S, int cx, int cy
   return hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
 }
 
-// The NR node values of the thread's fine column (cell column cx, basis hx);
-// thread row group fy0 (0 or 1) takes fine rows fy0 + 2r.  For GR = 2 every
-// node of the column has jj = fy0 and cell row r, so each corner row's
-// x-pass is shared by two consecutive nodes.
+// pass 2: fine interface node (I, J) of wall w
 template <int GR>
-__device__ __forceinline__ void if_rowpass32(const IfSmem32<GR> &S, int cx, int cr, const Herm &hx, float &p,
-                                             float &q) {
-  const float4 c0 = S.C[cr][cx], c1 = S.C[cr][cx + 1];
-  p = hx.a0 * c0.x + hx.a1 * c1.x + hx.b0 * c0.y + hx.b1 * c1.y;
-  q = hx.a0 * c0.z + hx.a1 * c1.z + hx.b0 * c0.w + hx.b1 * c1.w;
-}
-
-template <int GR, int NR>
-__device__ __forceinline__ void if_eval_column32(const IfSmem32<GR> &S, int cx, int fy0, const Herm &hx,
-                                                 float (&val)[NR]) {
-  if constexpr (GR == 2) {
-    const Herm hy = herm_at<2>(fy0);
-    float p0, q0;
-    if_rowpass32<GR>(S, cx, 0, hx, p0, q0);
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-      float p1, q1;
-      if_rowpass32<GR>(S, cx, r + 1, hx, p1, q1);
-      val[r] = hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
-      p0 = p1;
-      q0 = q1;
-    }
-  } else {
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
-      val[r] = if_eval32<GR>(S, cx, cy, hx, herm_at<GR>(jj));
-    }
-  }
-}
-
-// One tile, one wall, populations [a0, a1) (the macroscopic fields always):
-// f_a = feq_a(rho^, u^) + fac fneq^_a written into the wall's interface plane
-// (lower block plane zds-1 = k zdf-1, upper block plane zds = k 0).  The
-// next field's history values are in flight while the current one is
-// evaluated.  Requires blockDim.x == kThreads.
-template <int GR>
-__device__ __forceinline__ void iface_tile32(IfSmem32<GR> &S, const IfParams32 &P, int tx, int ty, int w, int a0,
-                                             int a1) {
-  constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, NR = GR * TY / 2;
-  const int i0 = tx * TX, j0 = ty * TY;
-  const int t = threadIdx.x, fx = t & 63, fy0 = (t >> 6) & 1;
-  const bool colok = fx < GR * TX && i0 + fx / GR < P.nx;
-  const int cx = colok ? fx / GR : 0, ii = colok ? fx - cx * GR : 0;  // in-bounds reads for idle lanes
-  const Herm hx = herm_at<GR>(ii);
-  const size_t plane = (size_t)P.ny * P.nx, fplane = (size_t)P.nyf * P.nxf;
-  const size_t wo = (size_t)w * 23 * plane;
-  const int pf = w == 0 ? P.zds - 1 : P.zds;
-  float *out = P.fdst + (size_t)pf * fplane;
-  const size_t fstride = (size_t)2 * P.zds * fplane;
-  IfStage<GR> st;
-  st.init(P, i0, j0);
-  st.prefetch(P.hn + wo, P.hp + wo, P.hpp + wo);
-  float mac[4][NR];
+__device__ __forceinline__ void iface_node32(const IfParams32 &P, int I, int J, int w) {
+  const int nx = P.nx, ny = P.ny;
+  const int ic = I / GR, ii = I - ic * GR, jc = J / GR, jj = J - jc * GR;
+  const int ic1 = ic + 1 == nx ? 0 : ic + 1, jc1 = jc + 1 == ny ? 0 : jc + 1;
+  const Herm hx = herm_at((float)ii * (1.f / GR)), hy = herm_at((float)jj * (1.f / GR));
+  const size_t plane = (size_t)ny * nx;
+  const float4 *C = P.corner + (size_t)w * 23 * plane;
+  const int o00 = jc * nx + ic, o10 = jc * nx + ic1, o01 = jc1 * nx + ic, o11 = jc1 * nx + ic1;
+  float m[4];
 #pragma unroll
   for (int b = 0; b < 4; b++) {
-    st.build(S, P);
-    // next field: macroscopic b + 1, or the first population of the group
-    const size_t nf = wo + (size_t)(b < 3 ? b + 1 : 4 + a0) * plane;
-    if (b < 3 || a0 < a1) st.prefetch(P.hn + nf, P.hp + nf, P.hpp + nf);
-    if_eval_column32<GR, NR>(S, cx, fy0, hx, mac[b]);
+    const float4 *Cb = C + (size_t)b * plane;
+    m[b] = patch32(__ldg(Cb + o00), __ldg(Cb + o10), __ldg(Cb + o01), __ldg(Cb + o11), hx, hy);
   }
-  float usq[NR];
+  const float dr = m[0], rho = 1.f + dr, u0 = m[1], u1 = m[2], u2 = m[3];
+  const float usq = u0 * u0 + u1 * u1 + u2 * u2;
+  const size_t fplane = (size_t)P.nyf * P.nxf, fstride = (size_t)2 * P.zds * fplane;
+  const int pf = w == 0 ? P.zds - 1 : P.zds;
+  float *out = P.fdst + (size_t)pf * fplane + (size_t)J * P.nxf + I;
 #pragma unroll
-  for (int r = 0; r < NR; r++) usq[r] = mac[1][r] * mac[1][r] + mac[2][r] * mac[2][r] + mac[3][r] * mac[3][r];
-  for (int a = a0; a < a1; a++) {
-    st.build(S, P);
-    if (a + 1 < a1) {
-      const size_t nf = wo + (size_t)(5 + a) * plane;
-      st.prefetch(P.hn + nf, P.hp + nf, P.hpp + nf);
-    }
-    const float ex = (float)ex_of(a), ey = (float)ey_of(a), ez = (float)ez_of(a), wa = w_of(a);
-    float *oa = out + (size_t)a * fstride;
-    float fv[NR];
-    if_eval_column32<GR, NR>(S, cx, fy0, hx, fv);
-#pragma unroll
-    for (int r = 0; r < NR; r++) {
-      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
-      if (colok && j0 + cy < P.ny) {
-        const float fneq = fv[r];
-        const float dr = mac[0][r], eu = ex * mac[1][r] + ey * mac[2][r] + ez * mac[3][r];
-        const float deq = wa * (dr + (1.f + dr) * (3.f * eu + 4.5f * eu * eu - 1.5f * usq[r]));
-        oa[(size_t)((j0 + cy) * GR + jj) * P.nxf + (i0 + cx) * GR + ii] = deq + P.fac * fneq;
-      }
-    }
+  for (int a = 0; a < 19; a++) {
+    const float4 *Ca = C + (size_t)(4 + a) * plane;
+    const float fneq = patch32(__ldg(Ca + o00), __ldg(Ca + o10), __ldg(Ca + o01), __ldg(Ca + o11), hx, hy);
+    out[(size_t)a * fstride] = deq_f32(a, dr, rho, u0, u1, u2, usq) + P.fac * fneq;
   }
 }
 

@@ -112,8 +112,9 @@ void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const Lau
 void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first, bool last,
                      bool stats, cudaStream_t stream);
-void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *mac, float *fdst, const Dims &d,
-                          int substep, double omega_c, double omega_f, cudaStream_t stream);
+// corner: scratch of 2 x 23 x ny x nx float4 (corner values and derivatives)
+void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *corner, float *fdst,
+                          const Dims &d, int substep, double omega_c, double omega_f, cudaStream_t stream);
 void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,
                        double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
 void launch_flow_sums_f32(const float *fc, const float *ff, DevState *st, double *partials, const PartialLayout &pl,

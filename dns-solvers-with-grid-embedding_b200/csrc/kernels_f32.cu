@@ -121,15 +121,17 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f
 }
 
 // ------------------------------------------------------------------ interface
-// one block per (tile, wall, population group)
-#ifndef DNS_F32_IFACE_MINB
-#define DNS_F32_IFACE_MINB 0
-#endif
+// pass 1: one block per (tile, wall, field); pass 2: one thread per fine node
+__global__ void __launch_bounds__(kThreads) iface_corner_f32(IfParams32 P) {
+  __shared__ IfCornerSmem S;
+  const int w = blockIdx.z / 23, field = blockIdx.z - w * 23;
+  iface_corner_tile32(S, P, blockIdx.x, blockIdx.y, w, field);
+}
+
 template <int GR>
-__global__ void __launch_bounds__(kThreads, DNS_F32_IFACE_MINB) iface_f32(IfParams32 P, int groups) {
-  __shared__ IfSmem32<GR> S;
-  const int w = blockIdx.z / groups, g = blockIdx.z - w * groups;
-  iface_tile32<GR>(S, P, blockIdx.x, blockIdx.y, w, 19 * g / groups, 19 * (g + 1) / groups);
+__global__ void __launch_bounds__(kThreads) iface_eval_f32(IfParams32 P) {
+  const int I = blockIdx.x * kThreads + threadIdx.x;
+  if (I < P.nxf) iface_node32<GR>(P, I, blockIdx.y, blockIdx.z);
 }
 
 // ------------------------------------------------------------------ injection
@@ -365,21 +367,14 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
 #undef FINE32_CASE
 }
 
-void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *mac, float *fdst, const Dims &d,
-                          int substep, double omega_c, double omega_f, cudaStream_t stream) {
-  (void)mac;
-  IfParams32 P = iface_params32(hn, hp, hpp, fdst, d, substep, omega_c, omega_f);
-  const int groups = DNS_F32_IFACE_GROUPS;
-  if (d.gr == 2) {
-    dim3 grid((d.nx + IfTile<2>::TX - 1) / IfTile<2>::TX, (d.ny + IfTile<2>::TY - 1) / IfTile<2>::TY, 2 * groups);
-    iface_f32<2><<<grid, kThreads, 0, stream>>>(P, groups);
-  } else if (d.gr == 3) {
-    dim3 grid((d.nx + IfTile<3>::TX - 1) / IfTile<3>::TX, (d.ny + IfTile<3>::TY - 1) / IfTile<3>::TY, 2 * groups);
-    iface_f32<3><<<grid, kThreads, 0, stream>>>(P, groups);
-  } else {
-    dim3 grid((d.nx + IfTile<4>::TX - 1) / IfTile<4>::TX, (d.ny + IfTile<4>::TY - 1) / IfTile<4>::TY, 2 * groups);
-    iface_f32<4><<<grid, kThreads, 0, stream>>>(P, groups);
-  }
+void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *corner, float *fdst,
+                          const Dims &d, int substep, double omega_c, double omega_f, cudaStream_t stream) {
+  IfParams32 P = iface_params32(hn, hp, hpp, reinterpret_cast<float4 *>(corner), fdst, d, substep, omega_c, omega_f);
+  dim3 gc((d.nx + CTX - 1) / CTX, (d.ny + CTY - 1) / CTY, 2 * 23), ge((d.nxf + kThreads - 1) / kThreads, d.nyf, 2);
+  iface_corner_f32<<<gc, kThreads, 0, stream>>>(P);
+  if (d.gr == 2) iface_eval_f32<2><<<ge, kThreads, 0, stream>>>(P);
+  else if (d.gr == 3) iface_eval_f32<3><<<ge, kThreads, 0, stream>>>(P);
+  else iface_eval_f32<4><<<ge, kThreads, 0, stream>>>(P);
 }
 
 void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,

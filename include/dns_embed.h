@@ -203,12 +203,10 @@ int dns_flow_sums_static(const dns_params *p, const double *fc, const double *ff
 typedef struct dns_batch dns_batch;
 
 /* Tile shape of one instance: threads per row along x (32, 64 or 128) and row
-   iterations per work item of the coarse and fine kernels, and the number of
-   population groups of the interface transfer (1..19). */
+   iterations per work item of the coarse (cw, cjb) and fine (fw, fjb) kernels. */
 typedef struct dns_tile {
   int cw, cjb;
   int fw, fjb;
-  int igroups;
 } dns_tile;
 
 typedef struct dns_batch_info {

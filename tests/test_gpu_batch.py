@@ -60,7 +60,7 @@ def test_batch_matches_single_fp32_channel(pkg, ref_configs):
     ch.set_sampling(2)
     la = ch.step(20)
     with pkg.Batch() as b:
-        i = b.add(p, steps=20, seed=SEED, uc=UC, amp=AMP, sample_every=2, tile=(128, 2, 128, 2, 2))
+        i = b.add(p, steps=20, seed=SEED, uc=UC, amp=AMP, sample_every=2, tile=(128, 2, 128, 2))
         b.run(20)
         for lvl in range(3):
             np.testing.assert_allclose(b.export_state(i, lvl), ch.export_state(lvl), rtol=0, atol=1e-7)
@@ -88,7 +88,7 @@ def test_batch_mix_invariance(pkg, ref_configs):
         c = mix.add(pc, steps=100, seed=9)
         mix.run(3)                                     # A joins two steps late
         a = mix.add(pa, steps=12, seed=7, sample_every=3)
-        d = mix.add(pd, steps=4, seed=11, tile=(32, 1, 32, 4, 1))
+        d = mix.add(pd, steps=4, seed=11, tile=(32, 1, 32, 4))
         assert mix.run(7) == 2                         # b and d are spent
         mix.remove(b)
         e = mix.add(pb, steps=30, seed=5)              # reuses b's slot
@@ -115,7 +115,7 @@ def test_batch_rejects_mixed_gratio_and_bad_tiles(pkg, ref_configs):
             b.add(params_for(pkg, ref_configs["t_gr4"], "cfr"), steps=1)
         assert e.value.code == pkg.DNS_EINVAL
         with pytest.raises(pkg.DnsError):
-            b.add(params_for(pkg, ref_configs["t_noslip"], "cfr"), steps=1, tile=(48, 2, 128, 2, 2))
+            b.add(params_for(pkg, ref_configs["t_noslip"], "cfr"), steps=1, tile=(48, 2, 128, 2))
 
 
 def test_batch_autotune_sets_table(pkg, ref_configs):
