@@ -344,16 +344,17 @@ __global__ void __launch_bounds__(kThreads) b_icorner(const Mix *__restrict__ M,
     local /= I.igx;
     const int ty = local % I.igy;
     local /= I.igy;
-    const int wall = local / 23, field = local - wall * 23;
+    const int wall = local / kCornerFieldGroups, g = local - wall * kCornerFieldGroups;
     if (threadIdx.x == 0) iface_params_of(P, I, D, sub, tw);
     __syncthreads();
-    iface_corner_tile32(S, P, tx, ty, wall, field);  // ends with a barrier
+    iface_corner_tile32(S, P, tx, ty, wall, corner_field(g), corner_field(g + 1));  // ends with a barrier
   }
 }
 
 template <int GR>
 __global__ void __launch_bounds__(kThreads) b_ieval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
                                                     TimeW tw) {
+  __shared__ IfEvalSmem<GR> S;
   __shared__ IfParams32 P;
   const int n = M->n;
   const int *st = M->start[PH_IEVAL];
@@ -367,15 +368,16 @@ __global__ void __launch_bounds__(kThreads) b_ieval(const Mix *__restrict__ M, c
       w = past(w, st[s + 1], gridDim.x);
       continue;
     }
-    const int local = w - st[s];
-    const int gx = (I.nxf + kThreads - 1) / kThreads;
-    const int row = local / gx, bx = local - row * gx;
-    const int wall = row / I.nyf, J = row - wall * I.nyf;
-    __syncthreads();  // the previous item is done with P
+    int local = w - st[s];
+    const int gx = (I.nx + IfTile<GR>::TX - 1) / IfTile<GR>::TX, gy = (I.ny + IfTile<GR>::TY - 1) / IfTile<GR>::TY;
+    const int tx = local % gx;
+    local /= gx;
+    const int ty = local % gy;
+    local /= gy;
+    const int wall = local / kEvalPopGroups, g = local - wall * kEvalPopGroups;
     if (threadIdx.x == 0) iface_params_of(P, I, D, sub, tw);
     __syncthreads();
-    const int Ii = bx * kThreads + threadIdx.x;
-    if (Ii < P.nxf) iface_node32<GR>(P, Ii, J, wall);
+    iface_eval_tile32<GR>(S, P, tx, ty, wall, 19 * g / kEvalPopGroups, 19 * (g + 1) / kEvalPopGroups);  // ends with a barrier
   }
 }
 
@@ -556,8 +558,10 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   c[PH_EXTRACT] = 2 * I.ny * I.egx;
   c[PH_FBULK] = 2 * (I.zds - 3) * fb;
   c[PH_FEDGE] = 6 * fb;
-  c[PH_ICORNER] = 2 * 23 * I.igx * I.igy;
-  c[PH_IEVAL] = 2 * I.nyf * ((I.nxf + kThreads - 1) / kThreads);
+  c[PH_ICORNER] = 2 * kCornerFieldGroups * I.igx * I.igy;
+  const int etx = I.gr == 2 ? IfTile<2>::TX : (I.gr == 3 ? IfTile<3>::TX : IfTile<4>::TX);
+  const int ety = I.gr == 2 ? IfTile<2>::TY : (I.gr == 3 ? IfTile<3>::TY : IfTile<4>::TY);
+  c[PH_IEVAL] = 2 * kEvalPopGroups * ((I.nx + etx - 1) / etx) * ((I.ny + ety - 1) / ety);
   c[PH_INJECT] = 2 * I.ny * I.egx;
   c[PH_FINAL] = kFinChunks;
 }

@@ -342,53 +342,77 @@ inline IfParams32 iface_params32(const float *hn, const float *hp, const float *
   return P;
 }
 
-// pass 1 tile: CTX x CTY interface nodes
+// pass 1 tile: CTX x CTY interface nodes; a work item covers a group of fields
 constexpr int CTX = 32, CTY = 8;
+constexpr int kCornerFieldGroups = 3;  // fields [0, 8), [8, 16), [16, 23)
+__host__ __device__ constexpr int corner_field(int g) { return g * 8 < 23 ? g * 8 : 23; }
 struct IfCornerSmem {
   float V[CTY + 4][CTX + 4];
   float DY[CTY][CTX + 4];
 };
 
+// Fields [f0, f1) of one (tile, wall): the next field's history values are
+// loaded into registers while the current one is differentiated.
 __device__ __forceinline__ void iface_corner_tile32(IfCornerSmem &S, const IfParams32 &P, int tx, int ty, int w,
-                                                    int field) {
-  constexpr int QX = CTX + 4, QY = CTY + 4;
+                                                    int f0, int f1) {
+  constexpr int QX = CTX + 4, QY = CTY + 4, NV = (QX * QY + kThreads - 1) / kThreads;
   const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
   const int i0 = tx * CTX, j0 = ty * CTY;
-  const size_t plane = (size_t)P.ny * P.nx, fo = ((size_t)w * 23 + field) * plane;
+  const size_t plane = (size_t)P.ny * P.nx;
   // the last substep (t = 1) is level n alone
   const bool one = P.ap == 0.f && P.app == 0.f;
-  const float *hn = P.hn + fo, *hp = P.hp + fo, *hpp = P.hpp + fo;
+  int off[NV];
+  float vn[NV], vp[NV], vpp[NV];
 #pragma unroll
-  for (int s = 0; s < (QX * QY + kThreads - 1) / kThreads; s++) {
+  for (int s = 0; s < NV; s++) {
     const int q = threadIdx.x + s * kThreads;
-    if (q < QX * QY) {
-      const int pi = q % QX, pj = q / QX;
-      const int g = wrapf(j0 - 2 + pj, P.ny) * P.nx + wrapf(i0 - 2 + pi, P.nx);
-      S.V[pj][pi] = one ? __ldg(hn + g) : P.an * __ldg(hn + g) + P.ap * __ldg(hp + g) + P.app * __ldg(hpp + g);
-    }
+    off[s] = -1;
+    vn[s] = vp[s] = vpp[s] = 0.f;
+    if (q < QX * QY) off[s] = wrapf(j0 - 2 + q / QX, P.ny) * P.nx + wrapf(i0 - 2 + q % QX, P.nx);
   }
-  __syncthreads();
+  auto fetch = [&](int f) {
+    const size_t fo = ((size_t)w * 23 + f) * plane;
 #pragma unroll
-  for (int s = 0; s < (QX * CTY + kThreads - 1) / kThreads; s++) {
-    const int q = threadIdx.x + s * kThreads;
-    if (q < QX * CTY) {
-      const int pi = q % QX, r = q / QX;
-      S.DY[r][pi] = c2o3 * (S.V[r + 3][pi] - S.V[r + 1][pi]) - c1o12 * (S.V[r + 4][pi] - S.V[r][pi]);
-    }
-  }
-  __syncthreads();
-  float4 *out = P.corner + fo;
+    for (int s = 0; s < NV; s++)
+      if (off[s] >= 0) {
+        vn[s] = __ldg(P.hn + fo + off[s]);
+        if (!one) {
+          vp[s] = __ldg(P.hp + fo + off[s]);
+          vpp[s] = __ldg(P.hpp + fo + off[s]);
+        }
+      }
+  };
+  fetch(f0);
+  float *V = &S.V[0][0];
+  for (int f = f0; f < f1; f++) {
 #pragma unroll
-  for (int s = 0; s < CTX * CTY / kThreads; s++) {
-    const int q = threadIdx.x + s * kThreads;
-    const int c = q % CTX, r = q / CTX;
-    if (i0 + c < P.nx && j0 + r < P.ny) {
-      const float dx = c2o3 * (S.V[r + 2][c + 3] - S.V[r + 2][c + 1]) - c1o12 * (S.V[r + 2][c + 4] - S.V[r + 2][c]);
-      const float dxy = c2o3 * (S.DY[r][c + 3] - S.DY[r][c + 1]) - c1o12 * (S.DY[r][c + 4] - S.DY[r][c]);
-      out[(size_t)(j0 + r) * P.nx + i0 + c] = make_float4(S.V[r + 2][c + 2], dx, S.DY[r][c + 2], dxy);
+    for (int s = 0; s < NV; s++)
+      if (off[s] >= 0) V[threadIdx.x + s * kThreads] = one ? vn[s] : P.an * vn[s] + P.ap * vp[s] + P.app * vpp[s];
+    if (f + 1 < f1) fetch(f + 1);
+    __syncthreads();
+#pragma unroll
+    for (int s = 0; s < (QX * CTY + kThreads - 1) / kThreads; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      if (q < QX * CTY) {
+        const int pi = q % QX, r = q / QX;
+        S.DY[r][pi] = c2o3 * (S.V[r + 3][pi] - S.V[r + 1][pi]) - c1o12 * (S.V[r + 4][pi] - S.V[r][pi]);
+      }
     }
+    __syncthreads();
+    float4 *out = P.corner + ((size_t)w * 23 + f) * plane;
+#pragma unroll
+    for (int s = 0; s < CTX * CTY / kThreads; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      const int c = q % CTX, r = q / CTX;
+      if (i0 + c < P.nx && j0 + r < P.ny) {
+        const float dx =
+            c2o3 * (S.V[r + 2][c + 3] - S.V[r + 2][c + 1]) - c1o12 * (S.V[r + 2][c + 4] - S.V[r + 2][c]);
+        const float dxy = c2o3 * (S.DY[r][c + 3] - S.DY[r][c + 1]) - c1o12 * (S.DY[r][c + 4] - S.DY[r][c]);
+        out[(size_t)(j0 + r) * P.nx + i0 + c] = make_float4(S.V[r + 2][c + 2], dx, S.DY[r][c + 2], dxy);
+      }
+    }
+    __syncthreads();  // V and DY are rewritten for the next field (or the next item)
   }
-  __syncthreads();  // the tile's shared memory may be reused by the next item
 }
 
 struct Herm {
@@ -399,42 +423,149 @@ __device__ __forceinline__ Herm herm_at(float t) {
   return Herm{2.f * t3 - 3.f * t2 + 1.f, -2.f * t3 + 3.f * t2, t3 - 2.f * t2 + t, t3 - t2};
 }
 
-__device__ __forceinline__ float patch32(const float4 &c00, const float4 &c10, const float4 &c01, const float4 &c11,
-                                         const Herm &hx, const Herm &hy) {
-  const float p0 = hx.a0 * c00.x + hx.a1 * c10.x + hx.b0 * c00.y + hx.b1 * c10.y;
-  const float q0 = hx.a0 * c00.z + hx.a1 * c10.z + hx.b0 * c00.w + hx.b1 * c10.w;
-  const float p1 = hx.a0 * c01.x + hx.a1 * c11.x + hx.b0 * c01.y + hx.b1 * c11.y;
-  const float q1 = hx.a0 * c01.z + hx.a1 * c11.z + hx.b0 * c01.w + hx.b1 * c11.w;
-  return hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+// pass 2 tile: TX x TY interface cells; the fine tile is GR*TX (<= 64) columns
+// wide and thread t evaluates fine column (t & 63) of rows (t >> 6) + 2r.
+template <int GR>
+struct IfTile;
+template <>
+struct IfTile<2> {
+  static constexpr int TX = 32, TY = 8;
+};
+template <>
+struct IfTile<3> {
+  static constexpr int TX = 21, TY = 6;
+};
+template <>
+struct IfTile<4> {
+  static constexpr int TX = 16, TY = 4;
+};
+constexpr int kEvalStages = 4;     // corner tiles in flight
+constexpr int kEvalPopGroups = 2;  // population groups per (tile, wall)
+
+template <int GR>
+struct IfEvalSmem {
+  static constexpr int CW = IfTile<GR>::TX + 1, CH = IfTile<GR>::TY + 1;
+  float4 C[kEvalStages][CH][CW];
+};
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
 }
 
-// pass 2: fine interface node (I, J) of wall w
 template <int GR>
-__device__ __forceinline__ void iface_node32(const IfParams32 &P, int I, int J, int w) {
-  const int nx = P.nx, ny = P.ny;
-  const int ic = I / GR, ii = I - ic * GR, jc = J / GR, jj = J - jc * GR;
-  const int ic1 = ic + 1 == nx ? 0 : ic + 1, jc1 = jc + 1 == ny ? 0 : jc + 1;
-  const Herm hx = herm_at((float)ii * (1.f / GR)), hy = herm_at((float)jj * (1.f / GR));
-  const size_t plane = (size_t)ny * nx;
-  const float4 *C = P.corner + (size_t)w * 23 * plane;
-  const int o00 = jc * nx + ic, o10 = jc * nx + ic1, o01 = jc1 * nx + ic, o11 = jc1 * nx + ic1;
-  float m[4];
+__device__ __forceinline__ void if_rowpass32(const float4 (&C)[IfTile<GR>::TY + 1][IfTile<GR>::TX + 1], int cx,
+                                             int cr, const Herm &hx, float &p, float &q) {
+  const float4 c0 = C[cr][cx], c1 = C[cr][cx + 1];
+  p = hx.a0 * c0.x + hx.a1 * c1.x + hx.b0 * c0.y + hx.b1 * c1.y;
+  q = hx.a0 * c0.z + hx.a1 * c1.z + hx.b0 * c0.w + hx.b1 * c1.w;
+}
+
+// the NR node values of the thread's fine column (cell column cx, basis hx);
+// for GR = 2 all NR nodes have jj = fy0 and cell row r, so each corner row's
+// x-pass serves two consecutive nodes
+template <int GR, int NR>
+__device__ __forceinline__ void if_column32(const float4 (&C)[IfTile<GR>::TY + 1][IfTile<GR>::TX + 1], int cx, int fy0,
+                                           const Herm &hx, float (&val)[NR]) {
+  if constexpr (GR == 2) {
+    const Herm hy = herm_at(0.5f * (float)fy0);
+    float p0, q0;
+    if_rowpass32<GR>(C, cx, 0, hx, p0, q0);
 #pragma unroll
-  for (int b = 0; b < 4; b++) {
-    const float4 *Cb = C + (size_t)b * plane;
-    m[b] = patch32(__ldg(Cb + o00), __ldg(Cb + o10), __ldg(Cb + o01), __ldg(Cb + o11), hx, hy);
+    for (int r = 0; r < NR; r++) {
+      float p1, q1;
+      if_rowpass32<GR>(C, cx, r + 1, hx, p1, q1);
+      val[r] = hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+      p0 = p1;
+      q0 = q1;
+    }
+  } else {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
+      const Herm hy = herm_at((float)jj * (1.f / GR));
+      float p0, q0, p1, q1;
+      if_rowpass32<GR>(C, cx, cy, hx, p0, q0);
+      if_rowpass32<GR>(C, cx, cy + 1, hx, p1, q1);
+      val[r] = hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+    }
   }
-  const float dr = m[0], rho = 1.f + dr, u0 = m[1], u1 = m[2], u2 = m[3];
-  const float usq = u0 * u0 + u1 * u1 + u2 * u2;
+}
+
+// One (tile, wall) and populations [a0, a1) (the macroscopic fields always):
+// the corner tiles of successive fields stream into shared memory through a
+// cp.async ring while earlier ones are evaluated.  blockDim.x == kThreads.
+template <int GR>
+__device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfParams32 &P, int tx, int ty, int w,
+                                                  int a0, int a1) {
+  constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, NR = GR * TY / 2;
+  constexpr int CW = TX + 1, CH = TY + 1, NC = CW * CH, NCS = (NC + kThreads - 1) / kThreads;
+  const int i0 = tx * TX, j0 = ty * TY;
+  const int t = threadIdx.x, fx = t & 63, fy0 = (t >> 6) & 1;
+  const bool colok = fx < GR * TX && i0 + fx / GR < P.nx;
+  const int cx = colok ? fx / GR : 0, ii = colok ? fx - cx * GR : 0;  // idle lanes read in bounds
+  const Herm hx = herm_at((float)ii * (1.f / GR));
+  const size_t plane = (size_t)P.ny * P.nx;
+  int goff[NCS];
+#pragma unroll
+  for (int s = 0; s < NCS; s++) {
+    const int c = t + s * kThreads;
+    goff[s] = c < NC ? wrapf(j0 + c / CW, P.ny) * P.nx + wrapf(i0 + c % CW, P.nx) : -1;
+  }
+  const int nf = 4 + (a1 - a0);
+  auto issue = [&](int k) {
+    if (k < nf) {
+      const int f = k < 4 ? k : 4 + a0 + (k - 4);
+      const float4 *src = P.corner + ((size_t)w * 23 + f) * plane;
+      float4 *dst = &S.C[k % kEvalStages][0][0];
+#pragma unroll
+      for (int s = 0; s < NCS; s++)
+        if (goff[s] >= 0) cp_async16(dst + t + s * kThreads, src + goff[s]);
+    }
+    cp_async_commit();
+  };
+#pragma unroll
+  for (int k = 0; k < kEvalStages - 1; k++) issue(k);
+  float mac[4][NR];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    cp_async_wait<kEvalStages - 2>();
+    __syncthreads();
+    issue(k + kEvalStages - 1);
+    if_column32<GR, NR>(S.C[k % kEvalStages], cx, fy0, hx, mac[k]);
+  }
+  float usq[NR];
+#pragma unroll
+  for (int r = 0; r < NR; r++) usq[r] = mac[1][r] * mac[1][r] + mac[2][r] * mac[2][r] + mac[3][r] * mac[3][r];
   const size_t fplane = (size_t)P.nyf * P.nxf, fstride = (size_t)2 * P.zds * fplane;
   const int pf = w == 0 ? P.zds - 1 : P.zds;
-  float *out = P.fdst + (size_t)pf * fplane + (size_t)J * P.nxf + I;
+  float *out = P.fdst + (size_t)pf * fplane;
+  for (int k = 4; k < nf; k++) {
+    cp_async_wait<kEvalStages - 2>();
+    __syncthreads();
+    issue(k + kEvalStages - 1);
+    const int a = a0 + (k - 4);
+    float fv[NR];
+    if_column32<GR, NR>(S.C[k % kEvalStages], cx, fy0, hx, fv);
+    const float ex = (float)ex_of(a), ey = (float)ey_of(a), ez = (float)ez_of(a), wa = w_of(a);
+    float *oa = out + (size_t)a * fstride;
 #pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const float4 *Ca = C + (size_t)(4 + a) * plane;
-    const float fneq = patch32(__ldg(Ca + o00), __ldg(Ca + o10), __ldg(Ca + o01), __ldg(Ca + o11), hx, hy);
-    out[(size_t)a * fstride] = deq_f32(a, dr, rho, u0, u1, u2, usq) + P.fac * fneq;
+    for (int r = 0; r < NR; r++) {
+      const int fy = fy0 + 2 * r, cy = fy / GR, jj = fy - cy * GR;
+      if (colok && j0 + cy < P.ny) {
+        const float dr = mac[0][r], eu = ex * mac[1][r] + ey * mac[2][r] + ez * mac[3][r];
+        const float deq = wa * (dr + (1.f + dr) * (3.f * eu + 4.5f * eu * eu - 1.5f * usq[r]));
+        oa[(size_t)((j0 + cy) * GR + jj) * P.nxf + (i0 + cx) * GR + ii] = deq + P.fac * fv[r];
+      }
+    }
   }
+  cp_async_wait<0>();
+  __syncthreads();  // the ring may be reused by the next item
 }
 
 }  // namespace f32

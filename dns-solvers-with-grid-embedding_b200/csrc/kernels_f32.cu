@@ -121,17 +121,19 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f
 }
 
 // ------------------------------------------------------------------ interface
-// pass 1: one block per (tile, wall, field); pass 2: one thread per fine node
+// pass 1: one block per (tile, wall, field group); pass 2: one block per
+// (tile, wall, population group)
 __global__ void __launch_bounds__(kThreads) iface_corner_f32(IfParams32 P) {
   __shared__ IfCornerSmem S;
-  const int w = blockIdx.z / 23, field = blockIdx.z - w * 23;
-  iface_corner_tile32(S, P, blockIdx.x, blockIdx.y, w, field);
+  const int w = blockIdx.z / kCornerFieldGroups, g = blockIdx.z - w * kCornerFieldGroups;
+  iface_corner_tile32(S, P, blockIdx.x, blockIdx.y, w, corner_field(g), corner_field(g + 1));
 }
 
 template <int GR>
 __global__ void __launch_bounds__(kThreads) iface_eval_f32(IfParams32 P) {
-  const int I = blockIdx.x * kThreads + threadIdx.x;
-  if (I < P.nxf) iface_node32<GR>(P, I, blockIdx.y, blockIdx.z);
+  __shared__ IfEvalSmem<GR> S;
+  const int w = blockIdx.z / kEvalPopGroups, g = blockIdx.z - w * kEvalPopGroups;
+  iface_eval_tile32<GR>(S, P, blockIdx.x, blockIdx.y, w, 19 * g / kEvalPopGroups, 19 * (g + 1) / kEvalPopGroups);
 }
 
 // ------------------------------------------------------------------ injection
@@ -370,11 +372,16 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
 void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *corner, float *fdst,
                           const Dims &d, int substep, double omega_c, double omega_f, cudaStream_t stream) {
   IfParams32 P = iface_params32(hn, hp, hpp, reinterpret_cast<float4 *>(corner), fdst, d, substep, omega_c, omega_f);
-  dim3 gc((d.nx + CTX - 1) / CTX, (d.ny + CTY - 1) / CTY, 2 * 23), ge((d.nxf + kThreads - 1) / kThreads, d.nyf, 2);
+  dim3 gc((d.nx + CTX - 1) / CTX, (d.ny + CTY - 1) / CTY, 2 * kCornerFieldGroups);
   iface_corner_f32<<<gc, kThreads, 0, stream>>>(P);
-  if (d.gr == 2) iface_eval_f32<2><<<ge, kThreads, 0, stream>>>(P);
-  else if (d.gr == 3) iface_eval_f32<3><<<ge, kThreads, 0, stream>>>(P);
-  else iface_eval_f32<4><<<ge, kThreads, 0, stream>>>(P);
+#define DNS_EVAL_LAUNCH(G)                                                                            \
+  iface_eval_f32<G><<<dim3((d.nx + IfTile<G>::TX - 1) / IfTile<G>::TX, (d.ny + IfTile<G>::TY - 1) / IfTile<G>::TY, \
+                           2 * kEvalPopGroups),                                                        \
+                      kThreads, 0, stream>>>(P)
+  if (d.gr == 2) DNS_EVAL_LAUNCH(2);
+  else if (d.gr == 3) DNS_EVAL_LAUNCH(3);
+  else DNS_EVAL_LAUNCH(4);
+#undef DNS_EVAL_LAUNCH
 }
 
 void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,
