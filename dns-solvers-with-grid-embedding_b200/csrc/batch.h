@@ -34,7 +34,8 @@ enum Phase {
   PH_CEDGE,      // coarse planes 0, 1, zdc-2, zdc-1
   PH_EXTRACT,    // interface history planes k = 1 and zdc-2
   PH_FBULK,      // fine planes k = 2..zdf-3 of both blocks
-  PH_FEDGE,      // the remaining fine planes
+  PH_FEDGE,      // the wall-adjacent fine planes (lower k = 1, upper k = zdf-2)
+  PH_FADJ,       // the fine planes next to the interfaces (lower zdf-2, zdf-1; upper 0, 1)
   PH_ICORNER,    // interface corner data: tiles x walls x fields
   PH_IEVAL,      // interface evaluation: fine rows x walls
   PH_INJECT,     // fine-to-coarse injection rows
@@ -91,7 +92,7 @@ constexpr int kCornerTX = 32, kCornerTY = 8;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
-  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, icorner, ieval, inject, final_;
+  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, fadj, icorner, ieval, inject, final_;
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)

@@ -233,17 +233,20 @@ __global__ void __launch_bounds__(kThreads) b_extract(const Mix *__restrict__ M,
 }
 
 // ------------------------------------------------------------------ fine
-__device__ __forceinline__ int fine_plane(bool bulk, int q, int zds) {
-  if (bulk) return q < zds - 3 ? q + 1 : zds + 2 + (q - (zds - 3));
-  // edge planes: lower k = 1, zdf-2, zdf-1; upper k = 0, 1, zdf-2
-  return q < 3 ? (q == 0 ? 0 : zds - 3 + q) : (q < 5 ? zds + (q - 3) : 2 * zds - 1);
+// device plane of item plane q: KIND 1 bulk (k = 2..zdf-3 of both blocks),
+// KIND 2 interface-adjacent (lower k = zdf-2, zdf-1; upper k = 0, 1),
+// KIND 0 wall-adjacent (lower k = 1, upper k = zdf-2)
+__device__ __forceinline__ int fine_plane(int kind, int q, int zds) {
+  if (kind == 1) return q < zds - 3 ? q + 1 : zds + 2 + (q - (zds - 3));
+  if (kind == 2) return zds - 2 + q;
+  return q == 0 ? 0 : 2 * zds - 1;
 }
 
-template <int MODE, bool BULK>
-__global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
+template <int MODE, int KIND>
+__global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
     b_fine(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state, int sub) {
   const int n = M->n;
-  const int *st = M->start[BULK ? PH_FBULK : PH_FEDGE];
+  const int *st = M->start[KIND == 1 ? PH_FBULK : (KIND == 2 ? PH_FADJ : PH_FEDGE)];
   const int total = st[n];
   int s = 0;
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -258,7 +261,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
     const int gxy = I.fgx * I.fgy;
     const int q = local / gxy, rem = local - q * gxy, by = rem / I.fgx, bx = rem - by * I.fgx;
     const int zds = I.zds, zdf = I.zdf, gr = I.gr;
-    const int p = fine_plane(BULK, q, zds);
+    const int p = fine_plane(KIND, q, zds);
     const bool upper = p >= zds;
     const int k = upper ? p - zds : p + 1;
     const int kwall = upper ? zdf - 1 : 0;
@@ -275,7 +278,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
     double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
     double sacc[9];
     float wz[3] = {0.f, 0.f, 0.f};
-    if (BULK) {
+    if (KIND) {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const int kd = k + c - 1;
@@ -289,9 +292,21 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
       float fa[19];
       const size_t idx0 = ((size_t)p * I.nyf + j) * I.nxf + i;
       load19f(src, idx0, pstride, fa);
-      if (BULK)
+      if (KIND == 1)
         fine_bulk_f32<MODE>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc, wacc,
                             sacc);
+      else if (KIND == 2 && !upper && k == zdf - 1)
+        fine_bulk_f32<MODE, 2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                               wacc, sacc);
+      else if (KIND == 2 && upper && k == 0)
+        fine_bulk_f32<MODE, -2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                                wacc, sacc);
+      else if (KIND == 2 && !upper)
+        fine_bulk_f32<MODE, 1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                               wacc, sacc);
+      else if (KIND == 2)
+        fine_bulk_f32<MODE, -1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                                wacc, sacc);
       else
         fine_node_f32<MODE>(fa, i, j, p, k, upper, kwall, d, om, Gf, I.wflag, dst, pstride, wall_sum_plane,
                             wall_rho_plane, acc, wacc, sacc);
@@ -557,7 +572,8 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   c[PH_CEDGE] = 4 * cb;
   c[PH_EXTRACT] = 2 * I.ny * I.egx;
   c[PH_FBULK] = 2 * (I.zds - 3) * fb;
-  c[PH_FEDGE] = 6 * fb;
+  c[PH_FEDGE] = 2 * fb;
+  c[PH_FADJ] = 4 * fb;
   c[PH_ICORNER] = 2 * kCornerFieldGroups * I.igx * I.igy;
   const int etx = I.gr == 2 ? IfTile<2>::TX : (I.gr == 3 ? IfTile<3>::TX : IfTile<4>::TX);
   const int ety = I.gr == 2 ? IfTile<2>::TY : (I.gr == 3 ? IfTile<3>::TY : IfTile<4>::TY);
@@ -573,8 +589,9 @@ int query_grids(int gr, Grids *g) {
   rc |= occupancy_grid(b_coarse<true>, &g->cbulk);
   rc |= occupancy_grid(b_coarse<false>, &g->cedge);
   rc |= occupancy_grid(b_extract, &g->extract);
-  rc |= occupancy_grid(b_fine<1, true>, &g->fbulk);
-  rc |= occupancy_grid(b_fine<3, false>, &g->fedge);
+  rc |= occupancy_grid(b_fine<1, 1>, &g->fbulk);
+  rc |= occupancy_grid(b_fine<3, 0>, &g->fedge);
+  rc |= occupancy_grid(b_fine<3, 2>, &g->fadj);
   rc |= occupancy_grid(b_icorner, &g->icorner);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
@@ -586,24 +603,19 @@ int query_grids(int gr, Grids *g) {
 
 static void launch_fine(const Mix *m, Dyn *dyn, DevState *state, int mode, int sub, const Grids &g,
                         cudaStream_t s) {
+#define DNS_BFINE(M)                                                      \
+  case M:                                                                 \
+    b_fine<M, 1><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);        \
+    b_fine<M, 2><<<g.fadj, kThreads, 0, s>>>(m, dyn, state, sub);         \
+    b_fine<M, 0><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);        \
+    break;
   switch (mode) {
-    case 0:
-      b_fine<0, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
-      b_fine<0, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
-      break;
-    case 1:
-      b_fine<1, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
-      b_fine<1, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
-      break;
-    case 2:
-      b_fine<2, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
-      b_fine<2, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
-      break;
-    default:
-      b_fine<3, true><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);
-      b_fine<3, false><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);
-      break;
+    DNS_BFINE(0)
+    DNS_BFINE(1)
+    DNS_BFINE(2)
+    DNS_BFINE(3)
   }
+#undef DNS_BFINE
 }
 
 static TimeW time_weights(int sub, int gr) {

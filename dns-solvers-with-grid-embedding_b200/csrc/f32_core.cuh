@@ -239,7 +239,13 @@ __device__ __forceinline__ void fine_node_f32(float (&f)[19], int i, int j, int 
 // Bulk planes (every push lands on a fluid plane of the same block: no wall,
 // no interface): destinations from precomputed +-1 / +-row / +-plane offsets
 // with the periodic wrap folded in; encalc2 weights per destination plane.
-template <int MODE>
+// ZSKIP drops the pushes that land on or beyond the block's interface plane,
+// as the node rule's block-boundary test does (xfcomputations.c:843-897): the
+// interface plane of the destination belongs to the coarse-to-fine transfer,
+// which runs concurrently.  +1: e_z > 0 (lower k = zdf-2); +2: e_z >= 0
+// (lower k = zdf-1, the interface plane); -1: e_z < 0 (upper k = 1);
+// -2: e_z <= 0 (upper k = 0, the interface plane).
+template <int MODE, int ZSKIP = 0>
 __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
                                               float Gf, float *__restrict__ dst, size_t pstride, const float (&wz)[3],
                                               bool wall_sum_plane, bool wall_rho_plane, double (&acc)[2],
@@ -268,6 +274,9 @@ __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size
   float mom = 0.f, den = 0.f;
 #pragma unroll
   for (int a = 0; a < 19; a++) {
+    if ((ZSKIP == 1 && ez_of(a) > 0) || (ZSKIP == 2 && ez_of(a) >= 0) || (ZSKIP == -1 && ez_of(a) < 0) ||
+        (ZSKIP == -2 && ez_of(a) <= 0))
+      continue;
     const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
                     (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
 #if DNS_F32_FUSED

@@ -62,17 +62,19 @@ __global__ void __launch_bounds__(kThreads) extract_f32(const float *__restrict_
 }
 
 // ------------------------------------------------------------------ fine
-// The fine step is two launches: BULK over planes k = 2..zdf-3 of both blocks
-// (every push regular) and the edge planes (wall-adjacent, interface, and the
-// planes next to them).  blockIdx.z indexes a list of planes; partial sums
-// are stored at the plane's own block index, so the layout does not change.
+// The fine step is three launches over lists of planes: KIND 1 (bulk) the
+// planes k = 2..zdf-3 of both blocks, where every push is regular; KIND 2 the
+// two planes next to each interface, regular but for the pushes that leave the
+// block; KIND 0 the two wall-adjacent planes (bounce-back / free-slip rules).
+// blockIdx.z indexes the list; partial sums are stored at the plane's own
+// block index, so the layout does not change.
 struct PlaneList {
   int n;
   int p[64];
 };
 
-template <int MODE, bool BULK>
-__global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f32(const float *__restrict__ src, float *__restrict__ dst,
+template <int MODE, int KIND>
+__global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f32(const float *__restrict__ src, float *__restrict__ dst,
                                                     const int8_t *__restrict__ wf, Dims d, int jb, float om,
                                                     const DevState *st, double *__restrict__ part,
                                                     double *__restrict__ wpart, double *__restrict__ spart,
@@ -92,7 +94,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
   double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
   float wz[3] = {0.f, 0.f, 0.f};
-  if (BULK) {
+  if (KIND) {
     // destination planes k - 1, k, k + 1 (encalc2.c:33-53, 86-107)
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -107,9 +109,21 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) fine_f
     float fa[19];
     const size_t idx0 = ((size_t)p * ny + j) * nx + i;
     load19f(src, idx0, pstride, fa);
-    if (BULK)
+    if (KIND == 1)
       fine_bulk_f32<MODE>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc, wacc,
                           sacc);
+    else if (KIND == 2 && !upper && k == zdf - 1)
+      fine_bulk_f32<MODE, 2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                             wacc, sacc);
+    else if (KIND == 2 && upper && k == 0)
+      fine_bulk_f32<MODE, -2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                              wacc, sacc);
+    else if (KIND == 2 && !upper)
+      fine_bulk_f32<MODE, 1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc, wacc,
+                             sacc);
+    else if (KIND == 2)
+      fine_bulk_f32<MODE, -1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
+                              wacc, sacc);
     else
       fine_node_f32<MODE>(fa, i, j, p, k, upper, kwall, d, om, Gf, wf, dst, pstride, wall_sum_plane,
                           wall_rho_plane, acc, wacc, sacc);
@@ -347,20 +361,23 @@ void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const Lau
 void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first, bool last,
                      bool stats, cudaStream_t stream) {
-  PlaneList bulk{}, edge{};
+  PlaneList bulk{}, edge{}, adj{};
   for (int p = 0; p < 2 * d.zds; p++) {
-    const int k = p >= d.zds ? p - d.zds : p + 1;
-    PlaneList &L = (k >= 2 && k <= d.zdf - 3) ? bulk : edge;
+    const bool upper = p >= d.zds;
+    const int k = upper ? p - d.zds : p + 1;
+    const bool wall = upper ? k == d.zdf - 2 : k == 1;
+    PlaneList &L = (k >= 2 && k <= d.zdf - 3) ? bulk : (wall ? edge : adj);
     L.p[L.n++] = p;
   }
   const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
   double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
   const float omf = (float)om;
-  dim3 gb(s.fgx, s.fgy, bulk.n), ge(s.fgx, s.fgy, edge.n), block(s.bx);
-#define FINE32_CASE(M)                                                                                         \
-  case M:                                                                                                      \
-    if (bulk.n) fine_f32<M, true><<<gb, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, bulk); \
-    fine_f32<M, false><<<ge, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, edge);        \
+  dim3 gb(s.fgx, s.fgy, bulk.n), ge(s.fgx, s.fgy, edge.n), ga(s.fgx, s.fgy, adj.n), block(s.bx);
+#define FINE32_CASE(M)                                                                                       \
+  case M:                                                                                                    \
+    if (bulk.n) fine_f32<M, 1><<<gb, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, bulk); \
+    fine_f32<M, 2><<<ga, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, adj);            \
+    fine_f32<M, 0><<<ge, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, edge);           \
     break;
   switch (mode) {
     FINE32_CASE(0) FINE32_CASE(1) FINE32_CASE(2) FINE32_CASE(3) FINE32_CASE(4) FINE32_CASE(5) FINE32_CASE(6)
