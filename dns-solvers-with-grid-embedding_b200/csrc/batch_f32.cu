@@ -264,7 +264,6 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
     const int p = fine_plane(KIND, q, zds);
     const bool upper = p >= zds;
     const int k = upper ? p - zds : p + 1;
-    const int kwall = upper ? zdf - 1 : 0;
     const int lw = log2i(I.fw), tx = threadIdx.x & (I.fw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
     const int i = bx * I.fw + tx;
     const Dims d = dims_of(I);
@@ -278,7 +277,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
     double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
     double sacc[9];
     float wz[3] = {0.f, 0.f, 0.f};
-    if (KIND) {
+    {
 #pragma unroll
       for (int c = 0; c < 3; c++) {
         const int kd = k + c - 1;
@@ -307,9 +306,12 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
       else if (KIND == 2)
         fine_bulk_f32<MODE, -1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
                                 wacc, sacc);
+      else if (!upper)
+        fine_wall_f32<MODE, false>(fa, i, j, idx0, d, om, Gf, I.wflag, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
+                                   acc, wacc, sacc);
       else
-        fine_node_f32<MODE>(fa, i, j, p, k, upper, kwall, d, om, Gf, I.wflag, dst, pstride, wall_sum_plane,
-                            wall_rho_plane, acc, wacc, sacc);
+        fine_wall_f32<MODE, true>(fa, i, j, idx0, d, om, Gf, I.wflag, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
+                                  acc, wacc, sacc);
     }
     const size_t blk = ((size_t)p * I.fgy + by) * I.fgx + bx;
     if (MODE & 1) block_reduce32<2>(acc, I.part + I.pf + blk * 2);

@@ -182,60 +182,6 @@ __device__ __forceinline__ void coarse_bulk_f32(float (&f)[19], int i, int j, si
 }
 
 // ------------------------------------------------------------------ fine
-template <int MODE>
-__device__ __forceinline__ void fine_node_f32(float (&f)[19], int i, int j, int p, int k, bool upper, int kwall,
-                                              const Dims &d, float om, float Gf, const int8_t *__restrict__ wf,
-                                              float *__restrict__ dst, size_t pstride, bool wall_sum_plane,
-                                              bool wall_rho_plane, double (&acc)[2], double (&wacc)[2],
-                                              double (&sacc)[9]) {
-  const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
-  const Mac32 m = collide_f32(f, om, Gf);
-  if (MODE & 2) {
-    if (wall_sum_plane) wacc[0] += (double)m.u0;
-    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
-  }
-  if (MODE & 4) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
-  const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
-  const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
-  const bool wall_adjacent = upper ? (k == zdf - 2) : (k == 1);
-  const int8_t own = wall_adjacent ? wf[(size_t)j * nx + i] : (int8_t)-1;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    const int k2 = k + ez_of(a);
-    const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
-    const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
-    int pd, id, jd, ad, kd, exd;
-    if (k2 == kwall) {
-      const int8_t sld = wf[(size_t)j2 * nx + i2];
-      if (sld == -1 && own == -1) {
-        pd = p; id = i; jd = j; ad = opp_of(a); exd = -ex_of(a);
-      } else {
-        pd = p; id = i2; jd = j2; ad = mir_of(a); exd = ex_of(a);
-      }
-      kd = k;
-    } else {
-      if (!upper && k2 >= zdf - 1) continue;
-      if (upper && k2 <= 0) continue;
-      pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
-    }
-    (dst + (size_t)ad * pstride)[(unsigned)((pd * ny + jd) * nx + id)] = f[a];
-    if (MODE & 1) {
-      const float wgt = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
-                               : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
-      den += wgt * f[a];
-      if (exd > 0) mom += wgt * f[a];
-      if (exd < 0) mom -= wgt * f[a];
-    }
-  }
-  acc[0] += mom;
-  acc[1] += den;
-}
-
 // Bulk planes (every push lands on a fluid plane of the same block: no wall,
 // no interface): destinations from precomputed +-1 / +-row / +-plane offsets
 // with the periodic wrap folded in; encalc2 weights per destination plane.
@@ -293,6 +239,74 @@ __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size
       den += wgt * f[a];
       if (ex_of(a) > 0) mom += wgt * f[a];
       if (ex_of(a) < 0) mom -= wgt * f[a];
+    }
+  }
+  acc[0] += mom;
+  acc[1] += den;
+}
+
+// Wall-adjacent planes (lower k = 1, upper k = zdf-2): the regular pushes as
+// in the bulk planes; the five populations heading into the wall plane follow
+// the node rule (xfcomputations.c:226-240): half-way bounce-back onto the
+// node itself when both the destination column and the node's own column are
+// solid (flag -1), else specular reflection into the destination column.
+template <int MODE, bool UPPER>
+__device__ __forceinline__ void fine_wall_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
+                                              float Gf, const int8_t *__restrict__ wf, float *__restrict__ dst,
+                                              size_t pstride, const float (&wz)[3], bool wall_sum_plane,
+                                              bool wall_rho_plane, double (&acc)[2], double (&wacc)[2],
+                                              double (&sacc)[9]) {
+  const int nx = d.nxf, ny = d.nyf;
+  const Mac32 m = macro_f32(f);
+  if (MODE & 2) {
+    if (wall_sum_plane) wacc[0] += (double)m.u0;
+    if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
+  }
+  if (MODE & 4) {
+    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
+    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
+    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  }
+  const int plane = ny * nx;
+  const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
+  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+  const unsigned u0 = (unsigned)idx0, c0 = (unsigned)(j * nx + i);
+  const int8_t own = __ldg(wf + c0);
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int coff = (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) + (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
+    {
+      const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+      float dn = f[a] - om * (f[a] - deq);
+      if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * Gf;
+      f[a] = dn;
+    }
+    if ((UPPER && ez_of(a) > 0) || (!UPPER && ez_of(a) < 0)) {
+      const int8_t sld = __ldg(wf + (c0 + (unsigned)coff));  // 32-bit wrap before the pointer add
+      int exd;
+      if (sld == -1 && own == -1) {
+        (dst + (size_t)opp_of(a) * pstride)[u0] = f[a];
+        exd = -ex_of(a);
+      } else {
+        (dst + (size_t)mir_of(a) * pstride)[u0 + (unsigned)coff] = f[a];
+        exd = ex_of(a);
+      }
+      if (MODE & 1) {
+        const float wgt = wz[1];  // stays on the node's plane
+        den += wgt * f[a];
+        if (exd > 0) mom += wgt * f[a];
+        if (exd < 0) mom -= wgt * f[a];
+      }
+    } else {
+      const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + coff;
+      (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
+      if (MODE & 1) {
+        const float wgt = wz[ez_of(a) + 1];
+        den += wgt * f[a];
+        if (ex_of(a) > 0) mom += wgt * f[a];
+        if (ex_of(a) < 0) mom -= wgt * f[a];
+      }
     }
   }
   acc[0] += mom;

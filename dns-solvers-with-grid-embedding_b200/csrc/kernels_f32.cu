@@ -85,7 +85,6 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
   const int p = pls.p[blockIdx.z];
   const bool upper = p >= zds;
   const int k = upper ? p - zds : p + 1;
-  const int kwall = upper ? zdf - 1 : 0;
   const size_t pstride = (size_t)P * ny * nx;
   const float Gf = (float)((1. / (double)gr) * st->force);
   const bool wall_sum_plane =
@@ -94,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
   double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
   float wz[3] = {0.f, 0.f, 0.f};
-  if (KIND) {
+  {
     // destination planes k - 1, k, k + 1 (encalc2.c:33-53, 86-107)
 #pragma unroll
     for (int q = 0; q < 3; q++) {
@@ -124,9 +123,12 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
     else if (KIND == 2)
       fine_bulk_f32<MODE, -1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
                               wacc, sacc);
+    else if (!upper)
+      fine_wall_f32<MODE, false>(fa, i, j, idx0, d, om, Gf, wf, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
+                                 acc, wacc, sacc);
     else
-      fine_node_f32<MODE>(fa, i, j, p, k, upper, kwall, d, om, Gf, wf, dst, pstride, wall_sum_plane,
-                          wall_rho_plane, acc, wacc, sacc);
+      fine_wall_f32<MODE, true>(fa, i, j, idx0, d, om, Gf, wf, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
+                                acc, wacc, sacc);
   }
   const size_t blk = ((size_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce32<2>(acc, part + blk * 2);
