@@ -13,6 +13,15 @@ seeded synthetic initial state.  The state (2.1 GB) is far larger than L2.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
+Beside the FP64 line the same JSON carries three FP32 legs run by the
+batched engine: ``fp32`` (the production channel as a batch of one),
+``batched`` (96 independent channels of uneven size, wall pattern and Re_tau
+drawn from a seed, 2000 steps each, against the same channels run one after
+another in FP64) and ``served`` (Poisson request streams at 2, 10 and 50 per
+second with step budgets of 1000-10000, admitted against a 150 GB budget:
+p50/p99 latency and aggregate MLUPS, against the same requests served one at a
+time by the FP64 form).
+
 N > 1 runs under torchrun: every rank advances its own independent channel
 (replicas, weak scaling); the reported value is the whole job's updates over
 the slowest rank's device time.  ``--impl reference`` times the reference's own
@@ -21,6 +30,7 @@ CPU routines (compiled from its sources, oracle/_ref) on the host cores.
 from __future__ import annotations
 
 import argparse
+import importlib
 import json
 import os
 import statistics
@@ -30,6 +40,8 @@ import tempfile
 import threading
 import time
 from pathlib import Path
+
+import numpy as np
 
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
@@ -189,13 +201,120 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+def timed_batch_run(torch, b, n):
+    """Device time (ms) of b.run(n), CUDA events on the batch's stream."""
+    s = torch.cuda.ExternalStream(b.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    b.run(n)
+    e1.record(s)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1)
+
+
+def fp64_ms_per_step(pkg, torch, inst, cache, steps=8, device=0):
+    """FP64 plain form, one channel alone: device ms per coarse step (cached per grid shape)."""
+    key = (inst.nx, inst.ny, inst.nz)
+    if key not in cache:
+        p = inst.params(pkg)
+        p.device = device
+        ch = pkg.Channel(p)
+        st = torch.cuda.Stream()
+        ch.set_stream(st.cuda_stream)
+        ch.init_seeded(inst.seed, 0.05, 0.005)
+        ch.step(3, log=False)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        ch.step(steps, log=True)
+        e1.record(st)
+        torch.cuda.synchronize()
+        cache[key] = e0.elapsed_time(e1) / steps
+        ch.close()
+    return cache[key]
+
+
+def bench_batched(pkg, torch, args, peak, fp64_cache):
+    """Config 4: n channels of uneven size / pattern / Re_tau in one batch."""
+    W = importlib.import_module(PKG + ".workloads")
+    insts = W.batched_instances(args.c4_instances, steps=args.c4_steps)
+    b = pkg.Batch()
+    ids = [b.add(x.params(pkg), steps=x.steps, seed=x.seed) for x in insts]
+    U = sum(x.updates_per_step() for x in insts)
+    held = sum(b.info(i).device_bytes for i in ids)
+    b.run(args.warmup)
+    before = [b.info(i).steps_done for i in ids]
+    ms = timed_batch_run(torch, b, args.c4_steps - args.warmup)
+    steps = args.c4_steps - args.warmup
+    # work actually done: an instance that stops (non-finite wall stress) does no more
+    done = [b.info(i).steps_done - s0 for i, s0 in zip(ids, before)]
+    work = sum(x.updates_per_step() * d for x, d in zip(insts, done))
+    value = work / (ms * 1e-3) / 1e6
+    failed = sum(1 for i in ids if b.info(i).status != 0)
+    b.close()
+    # the same channels one after another in FP64 (device ms per step each)
+    seq_ms = sum(fp64_ms_per_step(pkg, torch, x, fp64_cache) for x in insts)
+    v64 = U / (seq_ms * 1e-3) / 1e6
+    return {
+        "value": value, "unit": "MLUPS", "dtype": "f32 (deviation storage, FP64 reductions)",
+        "instances": len(insts), "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+        "updates_per_step": U, "device_bytes": held, "failed_instances": failed,
+        "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak,
+        "re_tau_drawn_range": [min(x.re_tau for x in insts), max(x.re_tau for x in insts)],
+        "re_tau_run_range": [min(x.re_tau_run for x in insts), max(x.re_tau_run for x in insts)],
+        "gas_fraction_range": [min(x.gas_fraction for x in insts), max(x.gas_fraction for x in insts)],
+        "fp64_sequential": {"value": v64, "unit": "MLUPS", "ms_per_step_all": seq_ms,
+                            "how": "each channel alone in the FP64 plain form, 8 timed steps after 3 warm-up "
+                                   "(device time per grid shape), summed"},
+        "over_fp64_sequential": value / v64,
+        "workload": "96 channels drawn from seed 4: Nx {64,128,192,256}, Ny {32,48,64} (Ny/8 coarse cells "
+                    "embedded 2:1 per wall), Nz {64,96,128}, Re_tau U[180,395], ridges or posts, pitch "
+                    "{16,24,32} fine cells, gas fraction U[0.5,0.9]; the run's Re_tau capped at 3.5 wall units "
+                    "per fine cell (BGK diverges beyond ~4 on these grids)",
+    }
+
+
+def bench_served(pkg, torch, args, peak, fp64_cache):
+    """Config 5: Poisson request streams served by continuous batching."""
+    W = importlib.import_module(PKG + ".workloads")
+    S = importlib.import_module(PKG + ".serve")
+    out = {"budget_bytes": 150e9, "requests_per_rate": args.c5_requests, "group_steps": 32,
+           "note": "latency = completion - arrival on the host clock; FP64 one-at-a-time latencies are a "
+                   "first-come-first-served queue over the measured FP64 device time per step of each "
+                   "request's grid times its budget", "rates": {}}
+    for rate in args.c5_rates:
+        reqs = W.request_stream(rate, args.c5_requests, seed=7)
+        srv = S.Server(pkg, hbm_budget=150e9, group=32, sample_every=20)
+        t0 = time.perf_counter()
+        recs = srv.run(reqs)
+        span = time.perf_counter() - t0
+        srv.batch.close()
+        lat = S.latency_summary(recs)
+        mlups = srv.updates / span / 1e6
+        services = [x.steps * fp64_ms_per_step(pkg, torch, x, fp64_cache) * 1e-3 for x in reqs]
+        l64 = S.fifo_latencies([x.arrival for x in reqs], services)
+        work = sum(x.steps * x.updates_per_step() for x in reqs)
+        end64 = float(np.max(np.array([x.arrival for x in reqs]) + l64))
+        ok = [r for r in recs if r.status == 0]
+        out["rates"][str(rate)] = {
+            **lat, "aggregate_mlups": mlups, "hbm_frac": mlups * 1e6 * 152 / 1e9 / peak, "makespan_s": span,
+            "peak_resident_bytes": srv.peak_used,
+            "fp64_one_at_a_time": {"p50_s": float(np.percentile(l64, 50)), "p99_s": float(np.percentile(l64, 99)),
+                                   "aggregate_mlups": work / end64 / 1e6, "makespan_s": end64},
+            "slip_length_median": float(np.median([r.result["slip_length"] for r in ok])) if ok else None,
+            "drag_reduction_median_pct": float(np.median([r.result["drag_reduction_pct"] for r in ok])) if ok
+            else None,
+        }
+    return out
+
+
+PKG = "dns-solvers-with-grid-embedding_b200"
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
 
-    import importlib
-
-    pkg = importlib.import_module("dns-solvers-with-grid-embedding_b200")
+    pkg = importlib.import_module(PKG)
     torch.cuda.set_device(local_rank)
     dist = None
     if world > 1:
@@ -306,34 +425,26 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "log_tail": {"force": float(log[-1, 1]), "flowrate": float(log[-1, 4]), "stress": float(log[-1, 7])},
     }
-    # ---- the FP32 deviation-storage form on the same workload (same GPU)
+    # ---- the FP32 deviation-storage form on the same workload (same GPU), run
+    # by the batched engine as a batch of one
+    fp64_cache = {}
     if not args.no_fp32:
         ch.close()
-        p32 = pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank, precision=pkg.FP32)
-        c32 = pkg.Channel(p32)
-        c32.set_stream(stream.cuda_stream)
-        c32.init_seeded(42 + rank, 0.05, 0.005)
-        c32.step(args.warmup, log=False)
-        torch.cuda.synchronize()
-        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s0.record(stream)
-        c32.step(args.steps, log=True)
-        s1.record(stream)
-        torch.cuda.synchronize()
-        ms32 = s0.elapsed_time(s1)
-        c32.set_profiling(True)
-        c32.step(prof_steps, log=False)
-        kt32 = c32.kernel_times()
-        c32.close()
-        f32_ms, f32_n = kt32["fine"]
-        ach32 = fine_nodes * 2 * 19 * 4 / (f32_ms / f32_n * 1e-3) / 1e9 if f32_n else None
+        b1 = pkg.Batch(local_rank)
+        b1.add(pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank), steps=10 ** 9, seed=42 + rank)
+        b1.run(args.warmup)
+        ms32 = timed_batch_run(torch, b1, args.steps)
+        b1.close()
         v32 = U * args.steps * world / (ms32 * 1e-3) / 1e6
-        line["fp32"] = {"value": v32, "unit": "MLUPS", "ms_per_step": ms32 / args.steps, "dtype": "f32 (deviation)",
+        line["fp32"] = {"value": v32, "unit": "MLUPS", "ms_per_step": ms32 / args.steps,
+                        "dtype": "f32 (deviation storage, FP64 reductions)", "engine": "batched, one instance",
                         "over_fp64": v32 / value,
-                        "roofline": {"bound": "hbm", "kernel": "fine_kernel", "achieved": ach32, "peak": peak,
-                                     "unit": "GB/s", "frac": (ach32 / peak) if ach32 else None},
-                        "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak,
-                        "kernel_ms_per_step": {k: (v[0] / prof_steps) for k, v in kt32.items()}}
+                        "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak}
+    if world == 1 and not args.no_batched:
+        line["batched"] = bench_batched(pkg, torch, args, peak, fp64_cache)
+        line["batched"]["over_fp64_plain"] = line["batched"]["value"] / value
+    if world == 1 and not args.no_served:
+        line["served"] = bench_served(pkg, torch, args, peak, fp64_cache)
     if world == 1 and not args.no_cpu_baseline:
         m_ = CONFIGS[args.config][0]
         secs = reference_cpu(args.config, args.cpu_steps, 1)
@@ -362,6 +473,12 @@ def main():
     ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--c4-instances", type=int, default=96)
+    ap.add_argument("--c4-steps", type=int, default=2000)
+    ap.add_argument("--c5-requests", type=int, default=16)
+    ap.add_argument("--c5-rates", type=float, nargs="+", default=[2.0, 10.0, 50.0])
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))

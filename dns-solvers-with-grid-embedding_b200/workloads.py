@@ -1,0 +1,190 @@
+"""Parametric channel workloads for the batched and served forms.
+
+A *channel instance* is one grid-embedded channel: coarse grid Nx (stream) x
+Ny (wall-normal) x Nz (span) with a 2:1 fine level over the Ny/8 coarse cells
+next to each wall, a wall pattern (streamwise ridges or square posts of a given
+pitch and gas fraction) and a friction Reynolds number.  In the reference's
+parameters (src/definitions.h) that is xdv = Nx, ydv = Nz, gratio = 2,
+zds = 2 Ny / 8 fine planes per block and zdv = Ny - zds + 3 coarse planes, so
+the fine-unit channel height is H = 2 Ny - 1 (dns-q-mgrd-all-patterns-xyc.c:155).
+
+The flow is driven at constant flow rate (encalc2) with the reference's bulk
+velocity ub = 0.0866034 (definitions.h:35); the bulk Reynolds number on the
+full height follows from the target Re_tau through Dean's correlation
+Re_tau = 0.175 (Re_b / 2)^(7/8), which the reference validates against.
+
+Resolution cap.  The drawn Re_tau (uniform in [180, 395]) is kept on the
+instance, but the run uses min(Re_tau, 3.5 H / 2): a fine-grid spacing of at
+most 3.5 wall units.  The BGK scheme (the reference's) diverges on these grids
+beyond about 4 wall units: with the drawn values, every one of the 81 batched
+channels at 4.12 wall units or more (relaxation time tau_f <= 0.504) produced
+a non-finite wall stress within 300-1700 steps, from the specified seeded
+start and from a start at the target flow rate alike, and every channel at
+4.1 or less ran its 2000 steps.  The reference's own runs use < 2 wall units.
+
+The quantities a solve returns (mean velocity profile, slip length, drag
+reduction) are computed here on the host from the instance's on-device
+statistics and log:
+  - slip length b = U_s / (dU/dz)|_w per wall, with U_s and the wall gradient
+    from the quadratic through the first three fine planes (z = 0.5, 1.5, 2.5
+    fine units from the wall): U_s = (15 U1 - 10 U2 + 3 U3) / 8 and
+    dU/dz = -2 U1 + 3 U2 - U3 (the stencil wshearstr.c:67-100 uses);
+  - drag reduction DR = 100 (Cf0 - Cf) / Cf0 with Cf = tau_w / (ub^2 / 2) from
+    the logged wall shear stress and flow rate (TKE-budget/postprocessing/
+    CFriction.c:33-59 forms Cf the same way) and the no-slip reference
+    Cf0 = 0.073 Re_b^(-1/4) (Dean) in place of that file's constant, which
+    belongs to one Reynolds number.
+The reference itself computes neither on the fly, so these definitions are
+this project's; nothing in the reference pins them.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+
+UB = 0.0866034
+SEED, UC, AMP = 42, 0.05, 0.005  # seeded initial state: laminar profile + Philox noise
+DPLUS_CAP = 3.5  # largest fine-grid spacing in wall units a run is given
+
+NX_CHOICES = (64, 128, 192, 256)
+NY_CHOICES = (32, 48, 64)
+NZ_CHOICES = (64, 96, 128)
+PITCH_CHOICES = (16, 24, 32)
+
+
+def reb_from_retau(re_tau: float) -> float:
+    """Bulk Reynolds number (full height) from Dean's correlation."""
+    return 2.0 * (re_tau / 0.175) ** (8.0 / 7.0)
+
+
+@dataclass
+class Instance:
+    nx: int
+    ny: int  # wall-normal coarse cells
+    nz: int  # spanwise
+    pattern: str  # "RSLIP" ridges or "PSLIP" posts
+    pitch: int  # fine cells
+    gas: int  # slip width per pitch, fine cells
+    re_tau: float
+    seed: int = SEED
+    steps: int = 2000
+    arrival: float = 0.0  # seconds after the stream starts (served form)
+    macros: dict = field(default_factory=dict)
+
+    @property
+    def zds(self) -> int:
+        return 2 * self.ny // 8
+
+    @property
+    def gas_fraction(self) -> float:
+        """Realised gas (slip) area fraction of the wall pattern."""
+        g = self.gas / self.pitch
+        return g if self.pattern == "RSLIP" else 1.0 - (1.0 - g) ** 2
+
+    @property
+    def height(self) -> int:
+        """Fine-unit channel height H = NZs - 2 = 2 Ny - 1."""
+        return 2 * self.ny - 1
+
+    @property
+    def re_tau_run(self) -> float:
+        """Re_tau the run uses: the drawn value, capped at DPLUS_CAP wall units per fine cell."""
+        return min(self.re_tau, DPLUS_CAP * self.height / 2.0)
+
+    @property
+    def rebs(self) -> float:
+        return reb_from_retau(self.re_tau_run)
+
+    def params(self, pkg, precision=None):
+        kw = dict(xdv=self.nx, ydv=self.nz, zdv=self.ny - self.zds + 3, zds=self.zds, gratio=2, Rebs=self.rebs,
+                  ub=UB, CFL=0.1, pattern=self.pattern, gyplussize=self.gas, wyplussize=self.pitch - self.gas,
+                  gxplussize=self.gas, wxplussize=self.pitch - self.gas, forcing=pkg.FORCING_CFR)
+        if precision is not None:
+            kw["precision"] = precision
+        kw.update(self.macros)
+        return pkg.make_params(**kw)
+
+    def updates_per_step(self) -> int:
+        nxf, nyf = 2 * self.nx, 2 * self.nz
+        return self.nx * self.nz * (self.ny - self.zds + 3) + 2 * 2 * nxf * nyf * self.zds
+
+
+def _gas_width(pattern: str, pitch: int, gf: float) -> int:
+    # ridges: slip width = GF pitch; posts (slip where x OR y in the gap):
+    # solid post side w with (w / pitch)^2 = 1 - GF
+    if pattern == "RSLIP":
+        g = int(round(gf * pitch))
+    else:
+        g = pitch - int(round(pitch * math.sqrt(1.0 - gf)))
+    return min(max(g, 1), pitch - 1)
+
+
+def draw_instance(rng: np.random.Generator, seed: int, steps: int) -> Instance:
+    nx = int(rng.choice(NX_CHOICES))
+    ny = int(rng.choice(NY_CHOICES))
+    nz = int(rng.choice(NZ_CHOICES))
+    re_tau = float(rng.uniform(180.0, 395.0))
+    pattern = "RSLIP" if rng.random() < 0.5 else "PSLIP"
+    pitch = int(rng.choice(PITCH_CHOICES))
+    gf = float(rng.uniform(0.5, 0.9))
+    return Instance(nx, ny, nz, pattern, pitch, _gas_width(pattern, pitch, gf), re_tau, seed=seed, steps=steps)
+
+
+def batched_instances(n: int = 96, seed: int = 4, steps: int = 2000) -> list[Instance]:
+    """The batched workload: n independent channels drawn from seed."""
+    rng = np.random.default_rng(seed)
+    return [draw_instance(rng, SEED + q, steps) for q in range(n)]
+
+
+def request_stream(rate: float, n: int, seed: int = 5, budget=(1000, 10000)) -> list[Instance]:
+    """The served workload: n requests with Poisson arrivals at `rate` per
+    second, grids and walls drawn as in the batched workload, step budgets
+    uniform in [budget[0], budget[1]]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for q in range(n):
+        t += float(rng.exponential(1.0 / rate))
+        inst = draw_instance(rng, SEED + q, int(rng.integers(budget[0], budget[1] + 1)))
+        inst.arrival = t
+        out.append(inst)
+    return out
+
+
+# ------------------------------------------------------------------ results
+def slip_length(stats: np.ndarray, zdf: int) -> tuple[float, float]:
+    """(lower, upper) slip length in fine units from the mean profile
+    stats[1] (U per composite-profile plane; lower fine planes are indices
+    1..zdf-1 at z = k - 1/2, the upper wall's first planes are the last ones)."""
+    U = stats[1]
+    nz = U.shape[0]
+
+    def one(u1, u2, u3):
+        us = (15.0 * u1 - 10.0 * u2 + 3.0 * u3) / 8.0
+        g = -2.0 * u1 + 3.0 * u2 - u3
+        return us / g if g != 0 else float("nan")
+
+    low = one(U[1], U[2], U[3])
+    # upper wall: profile index nz - 2 is the fluid plane next to the wall
+    up = one(U[nz - 2], U[nz - 3], U[nz - 4])
+    return low, up
+
+
+def drag_reduction(log: np.ndarray, rebs: float, first: int = 0) -> tuple[float, float]:
+    """(Cf, DR percent) from the per-step log rows [first:] (columns time,
+    force, momentum, denst, flowrate, stup, stdown, stress, pgrad)."""
+    rows = log[first:]
+    ub = float(np.mean(rows[:, 2] / rows[:, 3]))  # momentum / mass = bulk velocity
+    cf = float(np.mean(rows[:, 7])) / (0.5 * ub * ub)
+    cf0 = 0.073 * rebs ** -0.25
+    return cf, 100.0 * (cf0 - cf) / cf0
+
+
+def solve_result(inst: Instance, stats: np.ndarray, log: np.ndarray, zdf: int) -> dict:
+    """The answer to one parametric solve."""
+    lo, up = slip_length(stats, zdf)
+    cf, dr = drag_reduction(log, inst.rebs, first=len(log) // 2)
+    return {"z": stats[0].tolist(), "U": stats[1].tolist(), "slip_length": 0.5 * (lo + up),
+            "slip_length_walls": (lo, up), "cf": cf, "drag_reduction_pct": dr}
