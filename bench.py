@@ -268,8 +268,9 @@ def bench_batched(pkg, torch, args, peak, fp64_cache):
         "over_fp64_sequential": value / v64,
         "workload": "96 channels drawn from seed 4: Nx {64,128,192,256}, Ny {32,48,64} (Ny/8 coarse cells "
                     "embedded 2:1 per wall), Nz {64,96,128}, Re_tau U[180,395], ridges or posts, pitch "
-                    "{16,24,32} fine cells, gas fraction U[0.5,0.9]; the run's Re_tau capped at 3.5 wall units "
-                    "per fine cell (BGK diverges beyond ~4 on these grids)",
+                    "{16,24,32} fine cells, gas fraction U[0.5,0.9]; the run's Re_tau capped at 1.75 / 2.5 / "
+                    "2.75 wall units per fine cell for Ny 32 / 48 / 64 (the BGK scheme diverges beyond that on "
+                    "these grids, in FP64 as in FP32)",
     }
 
 

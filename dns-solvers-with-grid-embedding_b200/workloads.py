@@ -14,13 +14,16 @@ full height follows from the target Re_tau through Dean's correlation
 Re_tau = 0.175 (Re_b / 2)^(7/8), which the reference validates against.
 
 Resolution cap.  The drawn Re_tau (uniform in [180, 395]) is kept on the
-instance, but the run uses min(Re_tau, 3.5 H / 2): a fine-grid spacing of at
-most 3.5 wall units.  The BGK scheme (the reference's) diverges on these grids
-beyond about 4 wall units: with the drawn values, every one of the 81 batched
-channels at 4.12 wall units or more (relaxation time tau_f <= 0.504) produced
-a non-finite wall stress within 300-1700 steps, from the specified seeded
-start and from a start at the target flow rate alike, and every channel at
-4.1 or less ran its 2000 steps.  The reference's own runs use < 2 wall units.
+instance, but the run uses min(Re_tau, c(Ny) H / 2): a fine-grid spacing of
+at most c(Ny) wall units, c = 1.75 for Ny = 32, 2.5 for Ny = 48, 2.75 for
+Ny = 64.  The reference's BGK scheme diverges on these grids beyond that
+(measured on B200 with this library, FP64 form = the reference's arithmetic
+and FP32 batched form alike, which diverge within ~1% of the same step):
+over 10000 steps, Ny = 32 ran at 2.0 wall units and diverged at 2.5
+(after 1400-2700 steps), Ny = 48 ran at 3.0 and diverged at 3.5, Ny = 64 ran
+at 3.0 and diverged once at 3.5; uncapped, 81 of the 96 drawn channels
+diverged within 2000 steps; capped, none of them did in 3000.  The
+reference's own production runs use under 2 wall units.
 
 The quantities a solve returns (mean velocity profile, slip length, drag
 reduction) are computed here on the host from the instance's on-device
@@ -46,7 +49,11 @@ import numpy as np
 
 UB = 0.0866034
 SEED, UC, AMP = 42, 0.05, 0.005  # seeded initial state: laminar profile + Philox noise
-DPLUS_CAP = 3.5  # largest fine-grid spacing in wall units a run is given
+DPLUS_CAP = {32: 1.75, 48: 2.5, 64: 2.75}  # largest fine-grid spacing (wall units) per Ny
+
+
+def dplus_cap(ny: int) -> float:
+    return DPLUS_CAP[ny] if ny in DPLUS_CAP else (1.75 if ny <= 32 else (2.5 if ny <= 48 else 2.75))
 
 NX_CHOICES = (64, 128, 192, 256)
 NY_CHOICES = (32, 48, 64)
@@ -90,8 +97,8 @@ class Instance:
 
     @property
     def re_tau_run(self) -> float:
-        """Re_tau the run uses: the drawn value, capped at DPLUS_CAP wall units per fine cell."""
-        return min(self.re_tau, DPLUS_CAP * self.height / 2.0)
+        """Re_tau the run uses: the drawn value, capped at dplus_cap(ny) wall units per fine cell."""
+        return min(self.re_tau, dplus_cap(self.ny) * self.height / 2.0)
 
     @property
     def rebs(self) -> float:

@@ -25,7 +25,7 @@ def test_batched_draw_is_seeded_and_in_range():
         assert 180 <= x.re_tau <= 395 and x.pattern in ("RSLIP", "PSLIP")
         assert 0.4 < x.gas_fraction < 0.95
         assert x.zds == x.ny // 4
-        assert x.re_tau_run <= W.DPLUS_CAP * x.height / 2 + 1e-9 and x.re_tau_run <= x.re_tau
+        assert x.re_tau_run <= W.dplus_cap(x.ny) * x.height / 2 + 1e-9 and x.re_tau_run <= x.re_tau
     assert {x.pattern for x in a} == {"RSLIP", "PSLIP"}
 
 
