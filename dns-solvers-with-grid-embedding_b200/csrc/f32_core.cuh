@@ -441,6 +441,15 @@ __device__ __forceinline__ void iface_corner_tile32(IfCornerSmem &S, const IfPar
 struct Herm {
   float a0, a1, b0, b1;  // h00, h01, h10, h11
 };
+
+// e_x, e_y, e_z, w of each population, for loops over a run-time population
+#define DNS_POP_ROW(a) {(float)ex_of(a), (float)ey_of(a), (float)ez_of(a), w_of(a)}
+static __constant__ float c_pop[19][4] = {
+    DNS_POP_ROW(0),  DNS_POP_ROW(1),  DNS_POP_ROW(2),  DNS_POP_ROW(3),  DNS_POP_ROW(4),
+    DNS_POP_ROW(5),  DNS_POP_ROW(6),  DNS_POP_ROW(7),  DNS_POP_ROW(8),  DNS_POP_ROW(9),
+    DNS_POP_ROW(10), DNS_POP_ROW(11), DNS_POP_ROW(12), DNS_POP_ROW(13), DNS_POP_ROW(14),
+    DNS_POP_ROW(15), DNS_POP_ROW(16), DNS_POP_ROW(17), DNS_POP_ROW(18)};
+#undef DNS_POP_ROW
 __device__ __forceinline__ Herm herm_at(float t) {
   const float t2 = t * t, t3 = t2 * t;
   return Herm{2.f * t3 - 3.f * t2 + 1.f, -2.f * t3 + 3.f * t2, t3 - 2.f * t2 + t, t3 - t2};
@@ -489,23 +498,55 @@ __device__ __forceinline__ void if_rowpass32(const float4 (&C)[IfTile<GR>::TY + 
   q = hx.a0 * c0.z + hx.a1 * c1.z + hx.b0 * c0.w + hx.b1 * c1.w;
 }
 
-// the NR node values of the thread's fine column (cell column cx, basis hx);
-// for GR = 2 all NR nodes have jj = fy0 and cell row r, so each corner row's
-// x-pass serves two consecutive nodes
-template <int GR, int NR>
-__device__ __forceinline__ void if_column32(const float4 (&C)[IfTile<GR>::TY + 1][IfTile<GR>::TX + 1], int cx, int fy0,
-                                           const Herm &hx, float (&val)[NR]) {
-  if constexpr (GR == 2) {
-    const Herm hy = herm_at(0.5f * (float)fy0);
+// GR = 2, a warp's nodes all at sub-position (II, JJ) of their cells: the
+// Hermite basis is (1, 0, 0, 0) at t = 0 and (1/2, 1/2, 1/8, -1/8) at t = 1/2,
+// so II = 0 needs no x-pass and JJ = 0 no y-pass; cell row r is node r.
+template <int II, int JJ, int NR, int CH, int CW>
+__device__ __forceinline__ void if_col2(const float4 (&C)[CH][CW], int cx, float (&val)[NR]) {
+  auto xpass = [&](int r, float &p, float &q) {
+    const float4 c0 = C[r][cx];
+    if (II == 0) {
+      p = c0.x;
+      q = c0.z;
+    } else {
+      const float4 c1 = C[r][cx + 1];
+      p = 0.5f * (c0.x + c1.x) + 0.125f * (c0.y - c1.y);
+      q = 0.5f * (c0.z + c1.z) + 0.125f * (c0.w - c1.w);
+    }
+  };
+  if (JJ == 0) {
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      float p, q;
+      xpass(r, p, q);
+      val[r] = p;
+    }
+  } else {
     float p0, q0;
-    if_rowpass32<GR>(C, cx, 0, hx, p0, q0);
+    xpass(0, p0, q0);
 #pragma unroll
     for (int r = 0; r < NR; r++) {
       float p1, q1;
-      if_rowpass32<GR>(C, cx, r + 1, hx, p1, q1);
-      val[r] = hy.a0 * p0 + hy.a1 * p1 + hy.b0 * q0 + hy.b1 * q1;
+      xpass(r + 1, p1, q1);
+      val[r] = 0.5f * (p0 + p1) + 0.125f * (q0 - q1);
       p0 = p1;
       q0 = q1;
+    }
+  }
+}
+
+// the NR node values of the thread's fine column (cell column cx, basis hx;
+// for GR = 2 the sub-position ii and jj = fy0 are warp-uniform)
+template <int GR, int NR>
+__device__ __forceinline__ void if_column32(const float4 (&C)[IfTile<GR>::TY + 1][IfTile<GR>::TX + 1], int cx, int ii,
+                                           int fy0, const Herm &hx, float (&val)[NR]) {
+  constexpr int CH = IfTile<GR>::TY + 1, CW = IfTile<GR>::TX + 1;
+  if constexpr (GR == 2) {
+    switch (ii * 2 + fy0) {
+      case 0: if_col2<0, 0, NR, CH, CW>(C, cx, val); break;
+      case 1: if_col2<0, 1, NR, CH, CW>(C, cx, val); break;
+      case 2: if_col2<1, 0, NR, CH, CW>(C, cx, val); break;
+      default: if_col2<1, 1, NR, CH, CW>(C, cx, val); break;
     }
   } else {
 #pragma unroll
@@ -529,7 +570,10 @@ __device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfPar
   constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, NR = GR * TY / 2;
   constexpr int CW = TX + 1, CH = TY + 1, NC = CW * CH, NCS = (NC + kThreads - 1) / kThreads;
   const int i0 = tx * TX, j0 = ty * TY;
-  const int t = threadIdx.x, fx = t & 63, fy0 = (t >> 6) & 1;
+  // GR = 2: lanes take consecutive cells and a warp one sub-position ii, so
+  // the fine column is 2 cx + ii; otherwise lanes take consecutive fine columns
+  const int t = threadIdx.x, fy0 = (t >> 6) & 1;
+  const int fx = GR == 2 ? 2 * (t & 31) + ((t >> 5) & 1) : (t & 63);
   const bool colok = fx < GR * TX && i0 + fx / GR < P.nx;
   const int cx = colok ? fx / GR : 0, ii = colok ? fx - cx * GR : 0;  // idle lanes read in bounds
   const Herm hx = herm_at((float)ii * (1.f / GR));
@@ -560,7 +604,7 @@ __device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfPar
     cp_async_wait<kEvalStages - 2>();
     __syncthreads();
     issue(k + kEvalStages - 1);
-    if_column32<GR, NR>(S.C[k % kEvalStages], cx, fy0, hx, mac[k]);
+    if_column32<GR, NR>(S.C[k % kEvalStages], cx, ii, fy0, hx, mac[k]);
   }
   float usq[NR];
 #pragma unroll
@@ -574,8 +618,8 @@ __device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfPar
     issue(k + kEvalStages - 1);
     const int a = a0 + (k - 4);
     float fv[NR];
-    if_column32<GR, NR>(S.C[k % kEvalStages], cx, fy0, hx, fv);
-    const float ex = (float)ex_of(a), ey = (float)ey_of(a), ez = (float)ez_of(a), wa = w_of(a);
+    if_column32<GR, NR>(S.C[k % kEvalStages], cx, ii, fy0, hx, fv);
+    const float ex = c_pop[a][0], ey = c_pop[a][1], ez = c_pop[a][2], wa = c_pop[a][3];
     float *oa = out + (size_t)a * fstride;
 #pragma unroll
     for (int r = 0; r < NR; r++) {
