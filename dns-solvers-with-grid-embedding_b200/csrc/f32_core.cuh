@@ -26,13 +26,10 @@ namespace f32 {
 
 constexpr int kThreads = 128;
 // minimum resident blocks asked of the register allocator for the bulk-plane
-// kernels (0: compiler's choice); fused: collide each population right before
-// its store so collided values die as they are written
+// kernels (0: compiler's choice).  The fine bulk and wall kernels collide each
+// population right before its store, so collided values die as they are written.
 #ifndef DNS_F32_BULK_MINB
 #define DNS_F32_BULK_MINB 6
-#endif
-#ifndef DNS_F32_FUSED
-#define DNS_F32_FUSED 1
 #endif
 
 __device__ __forceinline__ int wrapf(int v, int n) {
@@ -167,18 +164,51 @@ __device__ __forceinline__ void coarse_bulk_f32(float (&f)[19], int i, int j, si
   // each population array holds fewer than 2^31 floats: 32-bit offsets from
   // the population's (thread-uniform) base
   const unsigned u0 = (unsigned)idx0;
-  float mom = 0.f, den = 0.f;
 #pragma unroll
   for (int a = 0; a < 19; a++) {
     const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
                     (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
     (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
-    den += f[a];
-    if (ex_of(a) > 0) mom += f[a];
-    if (ex_of(a) < 0) mom -= f[a];
   }
-  acc[0] += mom;
-  acc[1] += den;
+  // every push of a bulk node lands on a plane of equal flow-rate weight, so
+  // the partials are the node's post-collision moments: the collision keeps
+  // mass and momentum and the force adds rho G to sum e_x f (sum e_x^2 B = 1)
+  acc[0] += (double)(m.rho * m.u0 + m.rho * G);
+  acc[1] += (double)m.drho;
+}
+
+// the pushes of one bulk node (fused collision); ACC: accumulate the flow-rate
+// partials per destination plane weight
+template <bool ACC, int ZSKIP>
+__device__ __forceinline__ void fine_push_f32(float (&f)[19], const Mac32 &m, float om, float Gf,
+                                              float *__restrict__ dst, size_t pstride, unsigned u0, int plane, int dxm,
+                                              int dxp, int dym, int dyp, const float (&wz)[3], double (&acc)[2]) {
+  float mom = 0.f, den = 0.f;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    if ((ZSKIP == 1 && ez_of(a) > 0) || (ZSKIP == 2 && ez_of(a) >= 0) || (ZSKIP == -1 && ez_of(a) < 0) ||
+        (ZSKIP == -2 && ez_of(a) <= 0))
+      continue;
+    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
+                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
+    {
+      const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+      float dn = f[a] - om * (f[a] - deq);
+      if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * Gf;
+      f[a] = dn;
+    }
+    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
+    if (ACC) {
+      const float wgt = wz[ez_of(a) + 1];
+      den += wgt * f[a];
+      if (ex_of(a) > 0) mom += wgt * f[a];
+      if (ex_of(a) < 0) mom -= wgt * f[a];
+    }
+  }
+  if (ACC) {
+    acc[0] += mom;
+    acc[1] += den;
+  }
 }
 
 // ------------------------------------------------------------------ fine
@@ -197,11 +227,7 @@ __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size
                                               bool wall_sum_plane, bool wall_rho_plane, double (&acc)[2],
                                               double (&wacc)[2], double (&sacc)[9]) {
   const int nx = d.nxf, ny = d.nyf;
-#if DNS_F32_FUSED
   const Mac32 m = macro_f32(f);
-#else
-  const Mac32 m = collide_f32(f, om, Gf);
-#endif
   if (MODE & 2) {
     if (wall_sum_plane) wacc[0] += (double)m.u0;
     if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
@@ -217,32 +243,17 @@ __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size
   // each population array holds fewer than 2^31 floats: 32-bit offsets from
   // the population's (thread-uniform) base
   const unsigned u0 = (unsigned)idx0;
-  float mom = 0.f, den = 0.f;
-#pragma unroll
-  for (int a = 0; a < 19; a++) {
-    if ((ZSKIP == 1 && ez_of(a) > 0) || (ZSKIP == 2 && ez_of(a) >= 0) || (ZSKIP == -1 && ez_of(a) < 0) ||
-        (ZSKIP == -2 && ez_of(a) <= 0))
-      continue;
-    const int off = (ez_of(a) > 0 ? plane : (ez_of(a) < 0 ? -plane : 0)) + (ey_of(a) > 0 ? dyp : (ey_of(a) < 0 ? dym : 0)) +
-                    (ex_of(a) > 0 ? dxp : (ex_of(a) < 0 ? dxm : 0));
-#if DNS_F32_FUSED
-    {
-      const float deq = deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
-      float dn = f[a] - om * (f[a] - deq);
-      if (ex_of(a) != 0) dn += (float)ex_of(a) * bi_of(a) * m.rho * Gf;
-      f[a] = dn;
-    }
-#endif
-    (dst + (size_t)a * pstride)[u0 + (unsigned)off] = f[a];
-    if (MODE & 1) {
-      const float wgt = wz[ez_of(a) + 1];
-      den += wgt * f[a];
-      if (ex_of(a) > 0) mom += wgt * f[a];
-      if (ex_of(a) < 0) mom -= wgt * f[a];
-    }
+  // planes whose three destination planes weigh the same: the flow-rate
+  // partials are the node's post-collision moments (as in coarse_bulk_f32)
+  const bool wuni = ZSKIP == 0 && wz[0] == wz[1] && wz[1] == wz[2];
+  if ((MODE & 1) && wuni) {
+    acc[0] += (double)(wz[1] * (m.rho * m.u0 + m.rho * Gf));
+    acc[1] += (double)(wz[1] * m.drho);
   }
-  acc[0] += mom;
-  acc[1] += den;
+  if ((MODE & 1) && !wuni)
+    fine_push_f32<true, ZSKIP>(f, m, om, Gf, dst, pstride, u0, plane, dxm, dxp, dym, dyp, wz, acc);
+  else
+    fine_push_f32<false, ZSKIP>(f, m, om, Gf, dst, pstride, u0, plane, dxm, dxp, dym, dyp, wz, acc);
 }
 
 // Wall-adjacent planes (lower k = 1, upper k = zdf-2): the regular pushes as
