@@ -104,6 +104,7 @@ def lib() -> C.CDLL:
         "dns_get_geometry": (I, [P, C.POINTER(Geometry)]),
         "dns_load_restart": (I, [P, C.c_char_p, I]),
         "dns_write_restart": (I, [P, C.c_char_p, I]),
+        "dns_write_fields": (I, [P, C.c_char_p, I]),
         "dns_init_seeded": (I, [P, C.c_uint64, D, D]),
         "dns_export_state": (I, [P, I, P]),
         "dns_import_state": (I, [P, I, P]),
@@ -216,6 +217,10 @@ class Channel:
 
     def write_restart(self, directory, cntr: int):
         _check(lib().dns_write_restart(self.h, str(directory).encode(), cntr), "dns_write_restart")
+
+    def write_fields(self, directory, cntr: int):
+        """vel-{c,slf,suf} / den-{c,slf,suf} field files (the reference's vel_print)."""
+        _check(lib().dns_write_fields(self.h, str(directory).encode(), cntr), "dns_write_fields")
 
     def _level_shape(self, level: int):
         g = self.geom

@@ -730,6 +730,87 @@ extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
   return DNS_OK;
 }
 
+// ---------------------------------------------------------------- field output
+// vel_print.c:15-275 (called by main at :1342): per level, u = (sum E f) / rho
+// and rho = sum f of the post-stream state, summed in population order, zero
+// where rho <= 0; vel-* (nx, ny, nz, 3) and den-* (nx, ny, nz), C order,
+// native doubles.  The moments are formed on the device (4 of the 19 values per
+// node cross to the host); the wall planes, kept on the host, are done here.
+extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
+  if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  const size_t nmax = std::max((size_t)g.nx * g.ny * g.nzc, (size_t)g.nxf * g.nyf * g.zdf);
+  double *dvel = nullptr, *dden = nullptr;
+  if (cudaMalloc(&dvel, nmax * 3 * 8) != cudaSuccess) return fail(DNS_ENOMEM, "field staging");
+  if (cudaMalloc(&dden, nmax * 8) != cudaSuccess) {
+    cudaFree(dvel);
+    return fail(DNS_ENOMEM, "field staging");
+  }
+  std::vector<double> vel(nmax * 3), den(nmax);
+  static const double EX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0};
+  static const double EY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+  static const double EZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+  const char *names[3] = {"c", "slf", "suf"};
+  int rc = DNS_OK;
+  for (int lv = 0; lv < 3 && rc == DNS_OK; lv++) {
+    const int nx = lv == 0 ? g.nx : g.nxf, ny = lv == 0 ? g.ny : g.nyf, nz = lv == 0 ? g.nzc : g.zdf;
+    const size_t n = (size_t)nx * ny * nz;
+    const int P = lv == 0 ? g.nzc : 2 * zds, p0 = lv == 2 ? zds : 0, np = lv == 0 ? g.nzc : zds;
+    const int k0 = lv == 1 ? 1 : 0;
+    if (is_f32(h))
+      launch_fields_f32(F(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f]), dvel, dden, nx, ny, P, p0, np, nz, k0,
+                        h->stream);
+    else
+      launch_fields_f64(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f], dvel, dden, nx, ny, P, p0, np, nz, k0,
+                        h->stream);
+    cudaError_t e = cudaMemcpyAsync(vel.data(), dvel, n * 3 * 8, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(den.data(), dden, n * 8, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) {
+      rc = fail(DNS_ECUDA, cudaGetErrorString(e));
+      break;
+    }
+    if (lv > 0) {
+      const std::vector<double> &wall = lv == 1 ? h->wall_lo : h->wall_hi;
+      const int kw = lv == 1 ? 0 : g.zdf - 1;
+      for (size_t c = 0; c < (size_t)nx * ny; c++) {
+        const double *f = wall.data() + c * 19;
+        double ux = 0., uy = 0., uz = 0., dens = 0.;
+        for (int a = 0; a < 19; a++) {
+          ux += EX[a] * f[a];
+          uy += EY[a] * f[a];
+          uz += EZ[a] * f[a];
+          dens += f[a];
+        }
+        if (dens > 0.) {
+          ux /= dens;
+          uy /= dens;
+          uz /= dens;
+        } else {
+          ux = uy = uz = dens = 0.;
+        }
+        const size_t o = c * nz + kw;
+        vel[o * 3] = ux;
+        vel[o * 3 + 1] = uy;
+        vel[o * 3 + 2] = uz;
+        den[o] = dens;
+      }
+    }
+    char base[16];
+    std::snprintf(base, sizeof base, "vel-%s", names[lv]);
+    rc = write_file(cname(dir, base, cntr), vel.data(), n * 3, 1);
+    if (rc == DNS_OK) {
+      std::snprintf(base, sizeof base, "den-%s", names[lv]);
+      rc = write_file(cname(dir, base, cntr), den.data(), n, 1);
+    }
+  }
+  cudaFree(dvel);
+  cudaFree(dden);
+  return rc;
+}
+
 // ---------------------------------------------------------------- stepping
 // Precision dispatch for one launch of each kernel.  Buffers are addressed by
 // ping-pong index; history slots by ring index.

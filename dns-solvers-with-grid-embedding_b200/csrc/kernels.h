@@ -98,6 +98,12 @@ void finalize_flow_sums(DevState *st, const double *pairs, long npairs, const Di
 double encalc2_weight_sum(const Dims &d);
 void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint64_t seed, double uc, double amp,
                      cudaStream_t stream);
+// vel_print field records of np device planes p0.. into vel[i][j][k][3] and
+// den[i][j][k] (nz_aos planes, device plane p0 + q at k = k0_aos + q)
+void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream);
+void launch_fields_f32(const float *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);

@@ -337,6 +337,37 @@ __global__ void aos_to_dev_kernel(const double *__restrict__ aos, float *__restr
   }
 }
 
+// ------------------------------------------------------------------ field output
+// f = w + d in FP64, then the moments in population order as the FP64 form
+__global__ void fields_f32_kernel(const float *__restrict__ soa, double *__restrict__ vel, double *__restrict__ den,
+                                  int nx, int ny, int P, int p0, int nz_aos, int k0_aos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= nx) return;
+  const size_t stride = (size_t)P * ny * nx, s = ((size_t)(p0 + q) * ny + j) * nx + i;
+  double dens = 0., mx = 0., my = 0., mz = 0.;
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const double f = (a == 0 ? 1. / 3. : (a <= 6 ? 1. / 18. : 1. / 36.)) + (double)soa[s + (size_t)a * stride];
+    dens += f;
+    mx += (double)ex_of(a) * f;
+    my += (double)ey_of(a) * f;
+    mz += (double)ez_of(a) * f;
+  }
+  double ux = 0., uy = 0., uz = 0.;
+  if (dens > 0.) {
+    ux = mx / dens;
+    uy = my / dens;
+    uz = mz / dens;
+  } else {
+    dens = 0.;
+  }
+  const size_t o = ((size_t)i * ny + j) * nz_aos + k0_aos + q;
+  vel[o * 3 + 0] = ux;
+  vel[o * 3 + 1] = uy;
+  vel[o * 3 + 2] = uz;
+  den[o] = dens;
+}
+
 }  // namespace
 
 // ====================================================================== host
@@ -434,6 +465,12 @@ void launch_aos_to_dev_f32(const double *aos, float *soa, int nx, int ny, int P,
                            int k0_aos, cudaStream_t stream) {
   dim3 grid((nx + 127) / 128, ny, np), block(128);
   aos_to_dev_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_fields_f32(const float *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  fields_f32_kernel<<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
 }
 
 }  // namespace dns

@@ -803,6 +803,33 @@ __global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__rest
   for (int a = 0; a < 19; a++) soa[s + (size_t)a * stride] = o[a];
 }
 
+// ------------------------------------------------------------------ field output
+// vel_print.c:86-125: per node u = (sum E f) / rho, rho = sum f, both summed in
+// population order (moments_f64 is that order); zero where rho <= 0
+__global__ void fields_kernel(const double *__restrict__ soa, double *__restrict__ vel, double *__restrict__ den,
+                              int nx, int ny, int P, int p0, int nz_aos, int k0_aos) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= nx) return;
+  const size_t stride = (size_t)P * ny * nx;
+  double f[19];
+  load19(soa, ((size_t)(p0 + q) * ny + j) * nx + i, stride, f);
+  double dens, mx, my, mz;
+  moments_f64(f, dens, mx, my, mz);
+  double ux = 0., uy = 0., uz = 0.;
+  if (dens > 0.) {
+    ux = mx / dens;
+    uy = my / dens;
+    uz = mz / dens;
+  } else {
+    dens = 0.;
+  }
+  const size_t o = ((size_t)i * ny + j) * nz_aos + k0_aos + q;
+  vel[o * 3 + 0] = ux;
+  vel[o * 3 + 1] = uy;
+  vel[o * 3 + 2] = uz;
+  den[o] = dens;
+}
+
 }  // namespace
 
 // ====================================================================== host
@@ -1024,6 +1051,12 @@ void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, in
                        cudaStream_t stream) {
   dim3 grid((nx + 127) / 128, ny, np), block(128);
   aos_to_soa_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
+                       int k0_aos, cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  fields_kernel<<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
 }
 
 }  // namespace dns

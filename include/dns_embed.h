@@ -129,6 +129,11 @@ int dns_export_state(dns_handle *h, int level, double *aos_out);
 int dns_import_state(dns_handle *h, int level, const double *aos_in);
 /* Interface history [3 levels n,p,pp][2 walls lower,upper][xdv][ydv][23]. */
 int dns_export_history(dns_handle *h, double *out);
+/* Field output as the reference's vel_print.c:15-275 (main :1342): vel-c,
+   vel-slf, vel-suf (nx, ny, nz, 3) and den-c, den-slf, den-suf (nx, ny, nz),
+   counter cntr, of the post-stream state; the FP64 form writes the
+   reference's bytes. */
+int dns_write_fields(dns_handle *h, const char *dir, int cntr);
 /* Force the next step will use (encalc2 of the current state in CFR mode). */
 int dns_get_force(dns_handle *h, double *force);
 

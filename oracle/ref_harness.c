@@ -22,9 +22,11 @@
  * [ftemp | f] in global C order (i, j, k, a); lbf-uin / lbf-lin hold the
  * [n | p | pp] interface history (i, j, 23); force holds force[0].
  *
- * usage: ref_harness INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY]
+ * usage: ref_harness INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY] [FIELDS]
  * (INDIR "-" starts from rest instead of reading restart files; CNTR_OUT < 0
- *  skips the restart output, for timing)
+ *  skips the restart output, for timing; FIELDS = 1 also writes the
+ *  reference's vel-* / den-* field files of the final state with its own
+ *  vel_print, as main does at :1342)
  * The step loop time (MPI_Wtime, as main's t2-t4) is printed as
  *   "harness_seconds <s>".
  */
@@ -130,6 +132,7 @@ int main(int argc, char **argv) {
   /* strtod parses hex floats, so the force can be passed bit-exactly */
   double gconst = argc > 7 ? strtod(argv[7], NULL) : 0.0;
   long stats_every = argc > 8 ? atol(argv[8]) : 0;
+  int fields = argc > 9 ? atoi(argv[9]) : 0;
 
   int dims[2] = {XDIM, YDIM}, period[2] = {1, 1};
   MPI_Init(&argc, &argv);
@@ -318,6 +321,7 @@ cold_start:
   write_history(fn, V.uin, V.uinp, V.uinpp, xdc, ydc);
   snprintf(fn, sizeof fn, "lbf-lin.%.4d", cout);
   write_history(fn, V.lin, V.linp, V.linpp, xdc, ydc);
+  if (fields) V = vel_print(xdf, ydf, zdf, xdc, ydc, zdc, V, (long)cout);
   MPI_Finalize();
   return 0;
 }

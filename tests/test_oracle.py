@@ -193,3 +193,47 @@ def test_laminar_profile_known_answer(port, ref_configs):
     exact = 6.0 * ub * zeta * (1.0 - zeta)
     used = slice(1, nz - 1)
     assert np.max(np.abs(st[0, used] - exact[used])) < 0.05 * ub
+
+
+def _moments_seq(f):
+    """vel_print's per-node sums, sequential in population order (Python floats are IEEE doubles)."""
+    EX = (0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0)
+    EY = (0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1)
+    EZ = (0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1)
+    ux = uy = uz = d = 0.0
+    for a in range(19):
+        v = float(f[a])
+        ux += EX[a] * v
+        uy += EY[a] * v
+        uz += EZ[a] * v
+        d += v
+    if d > 0.0:
+        return ux / d, uy / d, uz / d, d
+    return 0.0, 0.0, 0.0, 0.0
+
+
+def test_reference_field_files_layout(ref_configs, tmp_path):
+    """The reference's own vel_print (through the harness) writes, per level,
+    (nx, ny, nz, 3) velocities and (nx, ny, nz) densities of the post-stream
+    state, each node's sums in population order: pins the layout that
+    dns_write_fields reproduces."""
+    name = "t_ridges"
+    exe = ref_binary(name)
+    if exe is None:
+        pytest.skip("compiled reference not available")
+    m = ref_configs[name]
+    subprocess.run([str(exe), "-", "0", str(tmp_path), "5", "3", "const", (1e-5).hex(), "0", "1"], check=True,
+                   capture_output=True)
+    gr = m["gratio"]
+    shapes = {"c": (m["xdv"], m["ydv"], m["zdv"]), "slf": (gr * m["xdv"], gr * m["ydv"], m["zds"] + 1),
+              "suf": (gr * m["xdv"], gr * m["ydv"], m["zds"] + 1)}
+    for lv, (nx, ny, nz) in shapes.items():
+        lat = np.fromfile(tmp_path / f"lbf-{lv}.0005", dtype=np.float64)[: nx * ny * nz * 19].reshape(nx, ny, nz, 19)
+        vel = np.fromfile(tmp_path / f"vel-{lv}.0005", dtype=np.float64).reshape(nx, ny, nz, 3)
+        den = np.fromfile(tmp_path / f"den-{lv}.0005", dtype=np.float64).reshape(nx, ny, nz)
+        for i in range(nx):
+            for j in range(ny):
+                for k in range(nz):
+                    ux, uy, uz, d = _moments_seq(lat[i, j, k])
+                    assert (vel[i, j, k, 0], vel[i, j, k, 1], vel[i, j, k, 2], den[i, j, k]) == (ux, uy, uz, d), \
+                        (lv, i, j, k)
