@@ -233,30 +233,59 @@ def fp64_ms_per_step(pkg, torch, inst, cache, steps=8, device=0):
     return cache[key]
 
 
-def bench_batched(pkg, torch, args, peak, fp64_cache):
-    """Config 4: n channels of uneven size / pattern / Re_tau in one batch."""
+def max_over_ranks(torch, dist, x: float) -> float:
+    """The largest x over all ranks (x itself without a process group)."""
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(torch, dist, x: float) -> float:
+    if dist is None:
+        return x
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def bench_batched(pkg, torch, args, peak, fp64_cache, rank=0, world=1, dist=None, device=0):
+    """Config 4: n channels of uneven size / pattern / Re_tau in one batch per
+    GPU; with N GPUs each rank takes its shard (workloads.shard), the value is
+    all ranks' node updates over the slowest rank's device time."""
     W = importlib.import_module(PKG + ".workloads")
-    insts = W.batched_instances(args.c4_instances, steps=args.c4_steps)
-    b = pkg.Batch()
-    ids = [b.add(x.params(pkg), steps=x.steps, seed=x.seed) for x in insts]
-    U = sum(x.updates_per_step() for x in insts)
+    everything = W.batched_instances(args.c4_instances, steps=args.c4_steps)
+    mine = W.shard(everything, world)[rank]
+    insts = [everything[q] for q in mine]
+    b = pkg.Batch(device)
+    ids = []
+    for x in insts:
+        p = x.params(pkg)
+        p.device = device
+        ids.append(b.add(p, steps=x.steps, seed=x.seed))
+    U = sum_over_ranks(torch, dist, sum(x.updates_per_step() for x in insts))
     held = sum(b.info(i).device_bytes for i in ids)
     b.run(args.warmup)
     before = [b.info(i).steps_done for i in ids]
-    ms = timed_batch_run(torch, b, args.c4_steps - args.warmup)
+    if dist is not None:
+        dist.barrier()
+    ms = max_over_ranks(torch, dist, timed_batch_run(torch, b, args.c4_steps - args.warmup))
     steps = args.c4_steps - args.warmup
     # work actually done: an instance that stops (non-finite wall stress) does no more
     done = [b.info(i).steps_done - s0 for i, s0 in zip(ids, before)]
-    work = sum(x.updates_per_step() * d for x, d in zip(insts, done))
+    work = sum_over_ranks(torch, dist, sum(x.updates_per_step() * d for x, d in zip(insts, done)))
     value = work / (ms * 1e-3) / 1e6
-    failed = sum(1 for i in ids if b.info(i).status != 0)
+    failed = int(sum_over_ranks(torch, dist, sum(1 for i in ids if b.info(i).status != 0)))
     b.close()
-    # the same channels one after another in FP64 (device ms per step each)
-    seq_ms = sum(fp64_ms_per_step(pkg, torch, x, fp64_cache) for x in insts)
+    # the same channels one after another in FP64 (device ms per step each),
+    # every rank its own shard
+    seq_ms = max_over_ranks(torch, dist, sum(fp64_ms_per_step(pkg, torch, x, fp64_cache, device=device)
+                                               for x in insts))
     v64 = U / (seq_ms * 1e-3) / 1e6
     return {
         "value": value, "unit": "MLUPS", "dtype": "f32 (deviation storage, FP64 reductions)",
-        "instances": len(insts), "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
+        "instances": len(everything), "gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
         "updates_per_step": U, "device_bytes": held, "failed_instances": failed,
         "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak,
         "re_tau_drawn_range": [min(x.re_tau for x in insts), max(x.re_tau for x in insts)],
@@ -392,6 +421,14 @@ def run_ours(args, rank, world, local_rank):
         e2e_ms = float(t.item())
     e2e = U * args.steps * world / (e2e_ms * 1e-3) / 1e6
 
+    # ---- batched channels sharded over the GPUs (every rank takes part)
+    batched_multi = None
+    if world > 1 and not args.no_batched:
+        ch.close()
+        peak_, _ = measured_peak()
+        batched_multi = bench_batched(pkg, torch, args, peak_, {}, rank=rank, world=world, dist=dist,
+                                      device=local_rank)
+
     if rank != 0:
         if dist:
             dist.barrier()
@@ -430,7 +467,7 @@ def run_ours(args, rank, world, local_rank):
     # by the batched engine as a batch of one
     fp64_cache = {}
     if not args.no_fp32:
-        ch.close()
+        ch.close()  # (idempotent)
         b1 = pkg.Batch(local_rank)
         b1.add(pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank), steps=10 ** 9, seed=42 + rank)
         b1.run(args.warmup)
@@ -443,6 +480,10 @@ def run_ours(args, rank, world, local_rank):
                         "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak}
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(pkg, torch, args, peak, fp64_cache)
+    if batched_multi is not None:
+        line["batched"] = batched_multi
+        line["batched"]["whole_step_hbm_frac"] /= world  # of N GPUs' bandwidth
+    if "batched" in line:
         line["batched"]["over_fp64_plain"] = line["batched"]["value"] / value
     if world == 1 and not args.no_served:
         line["served"] = bench_served(pkg, torch, args, peak, fp64_cache)

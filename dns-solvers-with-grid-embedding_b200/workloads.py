@@ -145,6 +145,21 @@ def batched_instances(n: int = 96, seed: int = 4, steps: int = 2000) -> list[Ins
     return [draw_instance(rng, SEED + q, steps) for q in range(n)]
 
 
+def shard(instances: list[Instance], world: int) -> list[list[int]]:
+    """Split independent channels across `world` GPUs: longest-processing-time
+    first on node updates x steps (ties by index), each to the least loaded
+    rank.  Deterministic, so every rank computes the same assignment without
+    communicating.  Returns the instance indices of each rank, ascending."""
+    load = [0] * world
+    out: list[list[int]] = [[] for _ in range(world)]
+    order = sorted(range(len(instances)), key=lambda q: (-instances[q].updates_per_step() * instances[q].steps, q))
+    for q in order:
+        r = min(range(world), key=lambda x: (load[x], x))
+        out[r].append(q)
+        load[r] += instances[q].updates_per_step() * instances[q].steps
+    return [sorted(x) for x in out]
+
+
 def request_stream(rate: float, n: int, seed: int = 5, budget=(1000, 10000)) -> list[Instance]:
     """The served workload: n requests with Poisson arrivals at `rate` per
     second, grids and walls drawn as in the batched workload, step budgets
