@@ -46,6 +46,7 @@ class Params(C.Structure):
         ("gyplussize", C.c_int), ("wyplussize", C.c_int), ("gxplussize", C.c_int), ("wxplussize", C.c_int),
         ("pattern", C.c_int), ("XDIM", C.c_int), ("YDIM", C.c_int), ("ITER", C.c_long),
         ("forcing", C.c_int), ("force_const", C.c_double), ("precision", C.c_int), ("device", C.c_int),
+        ("xdu", C.c_int), ("ydu", C.c_int), ("zdu", C.c_int),
     ]
 
 
@@ -104,6 +105,7 @@ def lib() -> C.CDLL:
         "dns_get_geometry": (I, [P, C.POINTER(Geometry)]),
         "dns_load_restart": (I, [P, C.c_char_p, I]),
         "dns_write_restart": (I, [P, C.c_char_p, I]),
+        "dns_load_uniform": (I, [P, C.c_char_p, I]),
         "dns_write_fields": (I, [P, C.c_char_p, I]),
         "dns_init_seeded": (I, [P, C.c_uint64, D, D]),
         "dns_export_state": (I, [P, I, P]),
@@ -214,6 +216,10 @@ class Channel:
 
     def load_restart(self, directory, cntr: int):
         _check(lib().dns_load_restart(self.h, str(directory).encode(), cntr), "dns_load_restart")
+
+    def load_uniform(self, directory, cntr: int):
+        """Mode -i start from the uniform-grid file lbf.cntr in directory."""
+        _check(lib().dns_load_uniform(self.h, str(directory).encode(), cntr), "dns_load_uniform")
 
     def write_restart(self, directory, cntr: int):
         _check(lib().dns_write_restart(self.h, str(directory).encode(), cntr), "dns_write_restart")

@@ -150,6 +150,9 @@ extern "C" int dns_params_default(dns_params *p) {
   p->force_const = 0.0;
   p->precision = DNS_FP64;
   p->device = 0;
+  p->xdu = 512;
+  p->ydu = 256;
+  p->zdu = 221;
   return DNS_OK;
 }
 
@@ -185,6 +188,9 @@ extern "C" int dns_params_from_definitions(const char *path, dns_params *p) {
     else if (n == "gxplussize") inum(p->gxplussize);
     else if (n == "wxplussize") inum(p->wxplussize);
     else if (n == "XDIM") inum(p->XDIM);
+    else if (n == "xdu") inum(p->xdu);
+    else if (n == "ydu") inum(p->ydu);
+    else if (n == "zdu") inum(p->zdu);
     else if (n == "YDIM") inum(p->YDIM);
     else if (n == "ITER") p->ITER = val[0] ? std::strtol(val, nullptr, 10) : 1;
     else if (n == "RSLIP") p->pattern = DNS_PATTERN_RSLIP;
@@ -862,6 +868,109 @@ static void rotate_history(dns_handle *h) {
   h->hpp = h->hp;
   h->hp = h->hn;
   h->hn = t;
+}
+
+// ---------------------------------------------------------------- mode -i start
+// dns-q-mgrd-all-patterns-xyc.c:978-997: init (every node the rest equilibrium,
+// before the wall flags exist), initializer (uniform grid -> coarse and both
+// fine blocks), inter_init (interface history from the coarse state).  The
+// uniform state is the first half of lbf.cntr, [xdu][ydu][zdu + 2][19]; the
+// second half (the uniform solver's scratch lattice) is not needed.  Each level
+// is interpolated on the device into reference AoS order and then imported like
+// a restart level.  The history is the extraction of the coarse planes k = 1
+// and zdc - 2 (inter_init.c:150-226) on all three levels: the reference copies
+// only 19 of every 23 fields into levels p and pp (inter_init.c:237-248) and
+// writes the upper plane's density and velocity into the lower history
+// (inter_init.c:202-205); neither slip is reproduced.
+extern "C" int dns_load_uniform(dns_handle *h, const char *dir, int cntr) {
+  if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
+  const dns_params &p = h->p;
+  if (p.xdu < 1 || p.ydu < 1 || p.zdu < 1) return fail(DNS_EINVAL, "xdu, ydu and zdu must be positive");
+  CUDA_TRY(cudaSetDevice(p.device));
+  const dns_geometry &g = h->g;
+  const int zd = p.zdu + 2;
+  const size_t nuni = 19ull * p.xdu * p.ydu * zd;
+  const std::string fn = cname(dir, "lbf", cntr);
+  {
+    FILE *fp = std::fopen(fn.c_str(), "rb");
+    if (!fp) return fail(DNS_EIO, "cannot open " + fn);
+    const bool ok = std::fseek(fp, 0, SEEK_END) == 0 && std::ftell(fp) >= (long)(nuni * 8);
+    std::fclose(fp);
+    if (!ok) return fail(DNS_EIO, fn + " is shorter than one (xdu, ydu, zdu + 2, 19) lattice");
+  }
+  std::vector<double> host(nuni);
+  int rc = read_file(fn, host.data(), nuni);
+  if (rc) return rc;
+  const size_t nlev = std::max(19ull * g.nx * g.ny * g.nzc, 19ull * g.nxf * g.nyf * g.zdf);
+  double *uni = nullptr, *lev = nullptr;
+  int *bad = nullptr;
+  auto release = [&]() {
+    cudaFree(uni);
+    cudaFree(lev);
+    cudaFree(bad);
+  };
+  if (cudaMalloc(&uni, nuni * 8) != cudaSuccess || cudaMalloc(&lev, nlev * 8) != cudaSuccess ||
+      cudaMalloc(&bad, sizeof(int)) != cudaSuccess) {
+    release();
+    return fail(DNS_ENOMEM, "uniform-grid staging");
+  }
+  cudaError_t e = cudaMemcpyAsync(uni, host.data(), nuni * 8, cudaMemcpyHostToDevice, h->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(bad, 0, sizeof(int), h->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+  if (e != cudaSuccess) {
+    release();
+    return fail(DNS_ECUDA, cudaGetErrorString(e));
+  }
+  host.clear();
+  host.shrink_to_fit();
+  // initializer.c:43-45 and main :443-444, the uniform grid's relaxation rate
+  const double dxf = 2. / ((double)(g.nzs - 2.));
+  const double dxc = g.gr * dxf;
+  const double dxr = 2. / ((double)(zd - 2.));
+  const double omega_u = 1. / ((3. / p.Rebs) * p.ub * (zd - 2.) + 0.5);
+  std::vector<double> aos(nlev);
+  for (int level = 0; level < 3 && rc == DNS_OK; level++) {
+    UniformMap m;
+    m.level = level;
+    m.nxl = level == 0 ? g.nx : g.nxf;
+    m.nyl = level == 0 ? g.ny : g.nyf;
+    m.nzl = level == 0 ? g.nzc : g.zdf;
+    m.xu = p.xdu;
+    m.yu = p.ydu;
+    m.zd = zd;
+    m.gr = g.gr;
+    m.zdf = g.zdf;
+    m.zdc = g.nzc;
+    m.dxf = dxf;
+    m.dxc = dxc;
+    m.dxr = dxr;
+    m.fac = level == 0 ? (dxr / dxc) * (omega_u / g.omega_c) : (dxr / dxf) * (omega_u / g.omega_f);
+    const size_t n = 19ull * m.nxl * m.nyl * m.nzl;
+    launch_uniform_interp_f64(uni, m, lev, bad, h->stream);
+    int flag = 0;
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpyAsync(aos.data(), lev, n * 8, cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&flag, bad, sizeof(int), cudaMemcpyDeviceToHost, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (e != cudaSuccess) rc = fail(DNS_ECUDA, cudaGetErrorString(e));
+    else if (flag) rc = fail(DNS_EINVAL, "the uniform grid (xdu, ydu, zdu) does not cover the embedded grid");
+    else rc = import_level(h, level, aos.data());
+  }
+  release();
+  if (rc) return rc;
+  // inter_init: level n from the new coarse state, then p = pp = n
+  h->hn = 0;
+  h->hp = 1;
+  h->hpp = 2;
+  L_extract(h, h->cur_c, 0, h->stream);
+  CUDA_TRY(cudaGetLastError());
+  const size_t hbytes = hslot_elems(h) * (is_f32(h) ? 4 : 8);
+  char *hist = reinterpret_cast<char *>(h->hist);
+  CUDA_TRY(cudaMemcpyAsync(hist + hbytes, hist, hbytes, cudaMemcpyDeviceToDevice, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(hist + 2 * hbytes, hist, hbytes, cudaMemcpyDeviceToDevice, h->stream));
+  h->ss = 0;
+  h->tm = cntr;
+  return refresh_flow(h, p.forcing == DNS_FORCING_CFR ? 0.0 : p.force_const);
 }
 
 // One coarse step on two (or three) streams.  The interface transfer of

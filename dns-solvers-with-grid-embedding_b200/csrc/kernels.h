@@ -104,6 +104,20 @@ void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int 
                        int k0_aos, cudaStream_t stream);
 void launch_fields_f32(const float *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);
+// Mode -i start: one level of the embedded grid interpolated from a uniform-grid
+// state.  uni is the uniform state in reference AoS order [xu][yu][zd][19]; out
+// receives the level in reference AoS order [nxl][nyl][nzl][19] (wall plane of a
+// fine block = the rest equilibrium w_a).  *bad is set when a stencil index
+// leaves the reference's two-deep halo in x or y, or the grid in z (those
+// nodes are not read).  level: 0 coarse, 1 lower fine, 2 upper fine.
+struct UniformMap {
+  int level, nxl, nyl, nzl;  // output level extents (nzl = zdc or zdf)
+  int xu, yu, zd;            // uniform grid: xdu, ydu, zdu + 2
+  int gr, zdf, zdc;
+  double dxf, dxc, dxr;      // node spacings as the reference's initializer forms them
+  double fac;                // (dxr / dx_level) (omega / omega_level), the f^neq rescaling
+};
+void launch_uniform_interp_f64(const double *uni, const UniformMap &m, double *out, int *bad, cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);

@@ -1059,4 +1059,130 @@ void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int 
   fields_kernel<<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
 }
 
+// ------------------------------------------------------------------ mode -i start
+// Uniform grid -> embedded grid (initializer.c:303-533, the pass over the first half,
+// sp_interpolate_qd.c:22-45): tri-quadratic Lagrange interpolation of all 19
+// populations at the level's node, then f = feq + fac (f_int - feq) with feq of
+// the interpolated moments.  Every expression is the reference's, in its order
+// (this unit is built without fused multiply-add).  The reference reads the
+// uniform state into an array with a two-deep ghost layer below and four above
+// in x and y, filled periodically; the periodic wrap here reads the same values
+// wherever that halo reaches.
+namespace {
+
+__device__ __forceinline__ int wrap_periodic(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+
+// 0.5 d (d - 1) F0 - (d - 1)(d + 1) F1 + 0.5 (d + 1) d F2  (sp_interpolate_qd.c:34,41,44)
+__device__ __forceinline__ double lagrange3(double d, double f0, double f1, double f2) {
+  return 0.5 * d * (d - 1.) * f0 - (d - 1.) * (d + 1.) * f1 + 0.5 * (d + 1.) * d * f2;
+}
+
+__global__ void __launch_bounds__(128) uniform_interp_kernel(const double *__restrict__ uni, UniformMap m,
+                                                             double *__restrict__ out, int *__restrict__ bad) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long nodes = (long long)m.nxl * m.nyl * m.nzl;
+  if (t >= nodes) return;
+  const int k = (int)(t % m.nzl);
+  const int j = (int)((t / m.nzl) % m.nyl);
+  const int i = (int)(t / ((long long)m.nzl * m.nyl));
+  double *o = out + t * 19;
+  const bool wall = (m.level == 1 && k == 0) || (m.level == 2 && k == m.zdf - 1);
+  if (wall) {
+    // init.c:18-53 runs before the wall flags exist in mode -i: rest equilibrium
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      const int c = wclass_of(a);
+      o[a] = c == 0 ? 1. / 3. : (c == 1 ? 1. / 18. : 1. / 36.);
+    }
+    return;
+  }
+  const double dxf = m.dxf, dxc = m.dxc, dxr = m.dxr;
+  const int GR = m.gr, zdf = m.zdf, zdc = m.zdc;
+  int iref, jref, kref, k0;
+  double dx, dy, dz;
+  if (m.level == 1) {  // initializer.c:326-399
+    iref = (int)floor((i + 0.5) * (dxf / dxr) - 0.5);
+    jref = (int)floor((j + 0.5) * (dxf / dxr) - 0.5);
+    kref = (int)floor((k - 0.5) * (dxf / dxr) + 0.5);
+    dx = (i + 0.5) * dxf - (iref + 0.5) * dxr;
+    dy = (j + 0.5) * dxf - (jref + 0.5) * dxr;
+    if (kref == 0) {
+      k0 = kref;
+      dz = -dxr + (k - 0.5) * dxf + 0.5 * dxr - kref * dxr;
+    } else {
+      k0 = kref - 1;
+      dz = (k - 0.5) * dxf + 0.5 * dxr - kref * dxr;
+    }
+  } else if (m.level == 0) {  // initializer.c:402-468
+    iref = (int)floor((i + 0.5) * dxc / dxr - 0.5);
+    jref = (int)floor((j + 0.5) * dxc / dxr - 0.5);
+    kref = (int)floor(0.5 + (k * GR + (zdf - GR - 1 - 0.5)) * dxf / dxr);
+    dx = (i + 0.5) * dxc - (iref + 0.5) * dxr;
+    dy = (j + 0.5) * dxc - (jref + 0.5) * dxr;
+    k0 = kref - 1;
+    dz = (k * GR + (zdf - GR - 1 - 0.5)) * dxf - (kref - 0.5) * dxr;
+  } else {  // initializer.c:470-533
+    iref = (int)floor((i + 0.5) * dxf / dxr - 0.5);
+    jref = (int)floor((j + 0.5) * dxf / dxr - 0.5);
+    kref = (int)floor(0.5 + (k + GR * (zdc - 3) + zdf - 1 - 0.5) * dxf / dxr);
+    dx = (i + 0.5) * dxf - (iref + 0.5) * dxr;
+    dy = (j + 0.5) * dxf - (jref + 0.5) * dxr;
+    k0 = kref - 1;
+    dz = (k + GR * (zdc - 3) + zdf - 1 - 0.5) * dxf - (kref - 0.5) * dxr;
+  }
+  dx = dx / dxr;
+  dy = dy / dxr;
+  dz = dz / dxr;
+  if (iref - 1 < -2 || iref + 1 > m.xu + 3 || jref - 1 < -2 || jref + 1 > m.yu + 3 || k0 < 0 || k0 + 2 >= m.zd) {
+    atomicOr(bad, 1);
+#pragma unroll
+    for (int a = 0; a < 19; a++) o[a] = __longlong_as_double(0x7ff8000000000000LL);
+    return;
+  }
+  // row offsets of the 3 x 3 stencil columns (ind[i] x jnd[j]), z-runs of 3 x 19 doubles
+  size_t col[3][3];
+#pragma unroll
+  for (int p = 0; p < 3; p++)
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+      col[p][q] = (((size_t)wrap_periodic(iref - 1 + p, m.xu) * m.yu + wrap_periodic(jref - 1 + q, m.yu)) * m.zd + k0) * 19;
+  double fi[19];
+#pragma unroll 1
+  for (int a = 0; a < 19; a++) {
+    double cy[3];
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      double cz[3];
+#pragma unroll
+      for (int q = 0; q < 3; q++) {
+        const double *u = uni + col[p][q] + a;
+        cz[q] = lagrange3(dz, __ldg(u), __ldg(u + 19), __ldg(u + 38));
+      }
+      cy[p] = lagrange3(dy, cz[0], cz[1], cz[2]);
+    }
+    fi[a] = lagrange3(dx, cy[0], cy[1], cy[2]);
+  }
+  double dens, mx, my, mz;
+  moments_f64(fi, dens, mx, my, mz);
+  const double u0 = mx / dens, u1 = my / dens, u2 = mz / dens;
+  const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+  const Weighted wr = weighted_rho(dens);
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int c = wclass_of(a);
+    const double feq = feq_f64(c == 0 ? wr.w0 : (c == 1 ? wr.w1 : wr.w2), proj_f64(a, u0, u1, u2), t15v);
+    o[a] = feq + m.fac * (fi[a] - feq);
+  }
+}
+
+}  // namespace
+
+void launch_uniform_interp_f64(const double *uni, const UniformMap &m, double *out, int *bad, cudaStream_t stream) {
+  const long long nodes = (long long)m.nxl * m.nyl * m.nzl;
+  uniform_interp_kernel<<<(unsigned)((nodes + 127) / 128), 128, 0, stream>>>(uni, m, out, bad);
+}
+
 }  // namespace dns

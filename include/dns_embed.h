@@ -64,6 +64,8 @@ typedef struct dns_params {
   double force_const;   /* coarse-unit body force g when forcing == DNS_FORCING_CONST */
   int precision;        /* enum dns_precision */
   int device;           /* CUDA device ordinal */
+  /* uniform grid of a mode -i start (definitions.h:103-109): xdu x ydu x (zdu + 2) */
+  int xdu, ydu, zdu;
 } dns_params;
 
 /* Derived sizes; computed on the host, no GPU needed. */
@@ -122,6 +124,19 @@ int dns_write_restart(dns_handle *h, const char *dir, int cntr);
    history [rho, u, 0...] on all three levels (the state inter_init.c builds).
    Replaces mode -s (init.c), which starts from rest. */
 int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double amp);
+/* Mode -i start (dns-q-mgrd-all-patterns-xyc.c:978-997): read the uniform-grid
+   state lbf.cntr (its first half, (xdu, ydu, zdu + 2, 19) in C order) from dir,
+   interpolate it onto the coarse and both fine grids by 3-D quadratic Lagrange
+   interpolation with the non-equilibrium part rescaled to each grid
+   (initializer.c:303-533, sp_interpolate_qd.c), and build the interface history
+   from the coarse state (inter_init.c), with levels p and pp equal to n and
+   each wall's history holding its own plane's moments (the reference copies 19
+   of every 23 fields into p and pp, inter_init.c:237-248, and writes the upper
+   plane's density and velocity into the lower history, inter_init.c:202-205).
+   DNS_EINVAL when a stencil would leave the reference's periodic halo (a
+   uniform grid too short for the channel); DNS_EIO when the file is missing or
+   shorter than one lattice. */
+int dns_load_uniform(dns_handle *h, const char *dir, int cntr);
 /* Post-stream state S in reference AoS order f[i][j][k][a] of the global domain:
    level 0 coarse (xdv, ydv, zdc, 19), 1 lower fine, 2 upper fine
    ((GR xdv), (GR ydv), zdf, 19).  out must hold that many doubles. */

@@ -46,7 +46,7 @@ from ref_configs import REF_CONFIGS  # noqa: E402
 
 # macros the configurations may set (reference src/definitions.h:34-119)
 VALUE_MACROS = ("Rebs", "ub", "zdv", "ydv", "xdv", "TSTR", "TEND", "CFL", "gratio", "zds",
-                "gyplussize", "wyplussize", "gxplussize", "wxplussize", "XDIM", "YDIM")
+                "gyplussize", "wyplussize", "gxplussize", "wxplussize", "XDIM", "YDIM", "xdu", "ydu", "zdu")
 PATTERNS = ("PSLIP", "RSLIP", "SSLIP")
 
 

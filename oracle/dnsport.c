@@ -637,6 +637,156 @@ void port_init_seeded(port_state *s, uint64_t seed, double uc, double amp, doubl
   s->force = force;
 }
 
+/* ------------------------------------------------------------ mode -i start */
+/* sp_interpolate_qd.c:22-45: quadratic Lagrange in z, then y, then x over the
+   3 x 3 x 3 stencil ind x jnd x knd of the uniform state u ([xu][yu][zd][19]);
+   x and y wrap periodically, which is what the reference's halo holds */
+static void qd_interp(const double *u, int xu, int yu, int zd, const int *ind, const int *jnd, const int *knd,
+                      double dx, double dy, double dz, double *ans) {
+  double cz[3][3][19], cy[3][19];
+  for (int i = 0; i < 3; i++)
+    for (int j = 0; j < 3; j++) {
+      int ii = ((ind[i] % xu) + xu) % xu, jj = ((jnd[j] % yu) + yu) % yu;
+      const double *col = u + ((size_t)ii * yu + jj) * zd * 19;
+      for (int a = 0; a < 19; a++)
+        cz[i][j][a] = 0.5 * dz * (dz - 1.) * col[knd[0] * 19 + a] - (dz - 1.) * (dz + 1.) * col[knd[1] * 19 + a] +
+                      0.5 * (dz + 1.) * dz * col[knd[2] * 19 + a];
+    }
+  for (int i = 0; i < 3; i++)
+    for (int a = 0; a < 19; a++)
+      cy[i][a] = 0.5 * dy * (dy - 1.) * cz[i][0][a] - (dy - 1.) * (dy + 1.) * cz[i][1][a] +
+                 0.5 * (dy + 1.) * dy * cz[i][2][a];
+  for (int a = 0; a < 19; a++)
+    ans[a] = 0.5 * dx * (dx - 1.) * cy[0][a] - (dx - 1.) * (dx + 1.) * cy[1][a] + 0.5 * (dx + 1.) * dx * cy[2][a];
+}
+
+/* interpolated populations -> feq + fac (f - feq) (initializer.c:372-395) */
+static void rescale_node(const double *fi, double fac, double *out) {
+  double dens, ux, uy, uz;
+  moments(fi, &dens, &ux, &uy, &uz);
+  double u0 = ux / dens, u1 = uy / dens, u2 = uz / dens;
+  double v = u0 * u0 + u1 * u1 + u2 * u2;
+  for (int a = 0; a < 19; a++) {
+    double feq = feq_of(a, dens, u0, u1, u2, v);
+    out[a] = feq + fac * (fi[a] - feq);
+  }
+}
+
+static int stencil_ok(const int *ind, const int *jnd, const int *knd, int xu, int yu, int zd) {
+  return ind[0] >= -2 && ind[2] <= xu + 3 && jnd[0] >= -2 && jnd[2] <= yu + 3 && knd[0] >= 0 && knd[2] < zd;
+}
+
+/* dns-q-mgrd-all-patterns-xyc.c:978-997 (mode -i): init.c before the wall flags
+   exist (every node w_a), initializer.c:303-533 (first half of lbf.TTTT onto the
+   post-stream lattices), inter_init.c (interface history from the coarse
+   state).  Two slips of inter_init are not reproduced: levels p and pp get all
+   23 fields of level n (the reference copies 19 of every 23, :237-248), and the
+   upper plane's density and velocity go to the upper history (the reference
+   writes them into the lower one, :202-205). */
+int port_init_uniform(port_state *s, const double *u, int xu, int yu, int zu) {
+  const int zd = zu + 2, GR = s->gr, zdf = s->zdf, zdc = s->zdc;
+  const double dxf = 2. / ((double)(s->nzs - 2.));
+  const double dxc = GR * dxf;
+  const double dxr = 2. / ((double)(zd - 2.));
+  double tau = (3. / s->c.Reb) * s->c.ub * (zd - 2.) + 0.5;
+  tau = 1. / tau;
+  const double tauf = s->omf, tauc = s->omc;
+  int ind[3], jnd[3], knd[3], iref, jref, kref;
+  double dx, dy, dz, fi[19];
+  size_t nc = (size_t)s->nx * s->ny * zdc * 19, nf = (size_t)s->nxf * s->nyf * zdf * 19;
+  for (int h = 0; h < 2; h++) {
+    for (size_t q = 0; q < nc; q++) s->fc[h][q] = WT[q % 19];
+    for (size_t q = 0; q < nf; q++) s->fl[h][q] = s->fu[h][q] = WT[q % 19];
+  }
+  /* lower fine block, k = 1..zdf-1 (initializer.c:326-399) */
+  for (int i = 0; i < s->nxf; i++)
+    for (int j = 0; j < s->nyf; j++)
+      for (int k = 1; k < zdf; k++) {
+        iref = (int)floor((i + 0.5) * (dxf / dxr) - 0.5);
+        jref = (int)floor((j + 0.5) * (dxf / dxr) - 0.5);
+        kref = (int)floor((k - 0.5) * (dxf / dxr) + 0.5);
+        ind[0] = iref - 1; ind[1] = iref; ind[2] = iref + 1;
+        jnd[0] = jref - 1; jnd[1] = jref; jnd[2] = jref + 1;
+        dx = (i + 0.5) * dxf - (iref + 0.5) * dxr;
+        dy = (j + 0.5) * dxf - (jref + 0.5) * dxr;
+        if (kref == 0) {
+          knd[0] = kref; knd[1] = kref + 1; knd[2] = kref + 2;
+          dz = -dxr + (k - 0.5) * dxf + 0.5 * dxr - kref * dxr;
+        } else {
+          knd[0] = kref - 1; knd[1] = kref; knd[2] = kref + 1;
+          dz = (k - 0.5) * dxf + 0.5 * dxr - kref * dxr;
+        }
+        dx = dx / dxr; dy = dy / dxr; dz = dz / dxr;
+        if (!stencil_ok(ind, jnd, knd, xu, yu, zd)) return -1;
+        qd_interp(u, xu, yu, zd, ind, jnd, knd, dx, dy, dz, fi);
+        rescale_node(fi, (dxr / dxf) * (tau / tauf), s->fl[0] + FIDX(s, i, j, k));
+      }
+  /* coarse grid, k = 0..zdc-1 (initializer.c:402-468) */
+  for (int i = 0; i < s->nx; i++)
+    for (int j = 0; j < s->ny; j++)
+      for (int k = 0; k < zdc; k++) {
+        iref = (int)floor((i + 0.5) * dxc / dxr - 0.5);
+        jref = (int)floor((j + 0.5) * dxc / dxr - 0.5);
+        kref = (int)floor(0.5 + (k * GR + (zdf - GR - 1 - 0.5)) * dxf / dxr);
+        ind[0] = iref - 1; ind[1] = iref; ind[2] = iref + 1;
+        jnd[0] = jref - 1; jnd[1] = jref; jnd[2] = jref + 1;
+        knd[0] = kref - 1; knd[1] = kref; knd[2] = kref + 1;
+        dx = (i + 0.5) * dxc - (iref + 0.5) * dxr;
+        dy = (j + 0.5) * dxc - (jref + 0.5) * dxr;
+        dz = (k * GR + (zdf - GR - 1 - 0.5)) * dxf - (kref - 0.5) * dxr;
+        dx = dx / dxr; dy = dy / dxr; dz = dz / dxr;
+        if (!stencil_ok(ind, jnd, knd, xu, yu, zd)) return -1;
+        qd_interp(u, xu, yu, zd, ind, jnd, knd, dx, dy, dz, fi);
+        rescale_node(fi, (dxr / dxc) * (tau / tauc), s->fc[0] + CIDX(s, i, j, k));
+      }
+  /* upper fine block, k = 0..zdf-2 (initializer.c:470-533) */
+  for (int i = 0; i < s->nxf; i++)
+    for (int j = 0; j < s->nyf; j++)
+      for (int k = 0; k < zdf - 1; k++) {
+        iref = (int)floor((i + 0.5) * dxf / dxr - 0.5);
+        jref = (int)floor((j + 0.5) * dxf / dxr - 0.5);
+        kref = (int)floor(0.5 + (k + GR * (zdc - 3) + zdf - 1 - 0.5) * dxf / dxr);
+        ind[0] = iref - 1; ind[1] = iref; ind[2] = iref + 1;
+        jnd[0] = jref - 1; jnd[1] = jref; jnd[2] = jref + 1;
+        knd[0] = kref - 1; knd[1] = kref; knd[2] = kref + 1;
+        dx = (i + 0.5) * dxf - (iref + 0.5) * dxr;
+        dy = (j + 0.5) * dxf - (jref + 0.5) * dxr;
+        dz = (k + GR * (zdc - 3) + zdf - 1 - 0.5) * dxf - (kref - 0.5) * dxr;
+        dx = dx / dxr; dy = dy / dxr; dz = dz / dxr;
+        if (!stencil_ok(ind, jnd, knd, xu, yu, zd)) return -1;
+        qd_interp(u, xu, yu, zd, ind, jnd, knd, dx, dy, dz, fi);
+        rescale_node(fi, (dxr / dxf) * (tau / tauf), s->fu[0] + FIDX(s, i, j, k));
+      }
+  memcpy(s->fl[1], s->fl[0], nf * sizeof(double));
+  memcpy(s->fu[1], s->fu[0], nf * sizeof(double));
+  /* inter_init.c:150-226 on the new coarse state, then all three levels */
+  s->hn = 0;
+  s->hp = 1;
+  s->hpp = 2;
+  for (int w = 0; w < 2; w++) {
+    int k = w == 0 ? 1 : zdc - 2;
+    for (int i = 0; i < s->nx; i++)
+      for (int j = 0; j < s->ny; j++) {
+        const double *f = s->fc[0] + CIDX(s, i, j, k);
+        double dens, ux, uy, uz;
+        moments(f, &dens, &ux, &uy, &uz);
+        double u0 = ux / dens, u1 = uy / dens, u2 = uz / dens;
+        double v = u0 * u0 + u1 * u1 + u2 * u2;
+        double *o = s->hist[0] + HIDX(s, w, i, j);
+        o[0] = dens;
+        o[1] = u0;
+        o[2] = u1;
+        o[3] = u2;
+        for (int a = 0; a < 19; a++) o[4 + a] = f[a] - feq_of(a, dens, u0, u1, u2, v);
+      }
+  }
+  size_t nh = (size_t)2 * s->nx * s->ny * 23;
+  memcpy(s->hist[1], s->hist[0], nh * sizeof(double));
+  memcpy(s->hist[2], s->hist[0], nh * sizeof(double));
+  s->force = s->cfr ? 0. : s->g;
+  return 0;
+}
+
 /* ------------------------------------------------------------ restart I/O */
 static int read_block(FILE *fp, double *dst, size_t n) { return fread(dst, sizeof(double), n, fp) == n ? 0 : -1; }
 

@@ -50,6 +50,10 @@ int port_save_restart(port_state *s, const char *dir, int cntr);
 /* seeded initial condition: rho = 1, laminar profile with centreline uc plus
    Philox4x32-10 uniform perturbations of amplitude amp; force[0] = force */
 void port_init_seeded(port_state *s, uint64_t seed, double uc, double amp, double force);
+/* mode -i start from a uniform-grid state u, the first half of lbf.TTTT in the
+   reference's order [xu][yu][zu + 2][19]; -1 when a stencil leaves the
+   reference's halo (x, y) or the uniform grid (z) */
+int port_init_uniform(port_state *s, const double *u, int xu, int yu, int zu);
 /* cfr != 0: constant flow rate (force from encalc2 every step); else fixed g */
 void port_set_forcing(port_state *s, int cfr, double g);
 /* advance n coarse steps; log (may be NULL) receives n entries */

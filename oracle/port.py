@@ -61,6 +61,8 @@ def lib() -> C.CDLL:
         L.port_save_restart.argtypes = [P, C.c_char_p, C.c_int]
         L.port_init_seeded.argtypes = [P, C.c_uint64, C.c_double, C.c_double, C.c_double]
         L.port_set_forcing.argtypes = [P, C.c_int, C.c_double]
+        L.port_init_uniform.restype = C.c_int
+        L.port_init_uniform.argtypes = [P, C.c_void_p, C.c_int, C.c_int, C.c_int]
         L.port_step.argtypes = [P, C.c_long, C.POINTER(PortLog)]
         L.port_export.restype = C.c_long
         L.port_export.argtypes = [P, C.c_int, C.c_void_p]
@@ -103,6 +105,13 @@ class Port:
     def init_seeded(self, seed=42, uc=0.05, amp=0.005, force=0.0):
         lib().port_init_seeded(self.h, seed, uc, amp, force)
 
+    def init_uniform(self, uni: np.ndarray):
+        """Mode -i start from the uniform-grid state uni[xdu, ydu, zdu + 2, 19]."""
+        u = np.ascontiguousarray(uni, dtype=np.float64)
+        xu, yu, zd, _ = u.shape
+        if lib().port_init_uniform(self.h, u.ctypes.data, xu, yu, zd - 2) != 0:
+            raise ValueError("the uniform grid does not cover the embedded grid")
+
     def set_forcing(self, cfr: bool, g: float = 0.0):
         lib().port_set_forcing(self.h, 1 if cfr else 0, g)
 
@@ -141,6 +150,50 @@ class Port:
         out = np.zeros(9 * nz)
         lib().port_plane_stats(self.h, out.ctypes.data)
         return out.reshape(9, nz)
+
+
+_EX = np.array([0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0], dtype=np.float64)
+_EY = np.array([0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1], dtype=np.float64)
+_EZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1], dtype=np.float64)
+_W = np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12, dtype=np.float64)
+
+
+def _uniform01(idx: np.ndarray, seed: int) -> np.ndarray:
+    """splitmix64 of (seed, idx) mapped to [0, 1): integer arithmetic and one
+    exact scaling, so the values are the same on every machine."""
+    with np.errstate(over="ignore"):
+        z = idx.astype(np.uint64) + np.uint64(seed) * np.uint64(0x9E3779B97F4A7C15) + np.uint64(0x9E3779B97F4A7C15)
+        z = (z ^ (z >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+        z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+        z = z ^ (z >> np.uint64(31))
+    return (z >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def uniform_state(xu: int, yu: int, zu: int, seed: int, uc: float = 0.05) -> np.ndarray:
+    """A uniform-grid state [xu, yu, zu + 2, 19] for mode -i starts: density
+    1 +- 0.005, laminar profile of centreline uc on the wall-normal node
+    positions (k - 1/2) / zu plus +-0.005 in each velocity component, the
+    equilibrium of that, plus +-5e-5 in every population.  Built from
+    additions and multiplications of hashed integers only."""
+    zd = zu + 2
+    n = xu * yu * zd
+    r = _uniform01(np.arange(n * 23, dtype=np.uint64), seed).reshape(xu, yu, zd, 23)
+    zeta = (np.arange(zd, dtype=np.float64) - 0.5) / zu
+    rho = 1.0 + 0.01 * (r[..., 0] - 0.5)
+    u0 = (4.0 * uc) * zeta * (1.0 - zeta) + 0.01 * (r[..., 1] - 0.5)
+    u1 = 0.01 * (r[..., 2] - 0.5)
+    u2 = 0.01 * (r[..., 3] - 0.5)
+    v = u0 * u0 + u1 * u1 + u2 * u2
+    f = np.empty((xu, yu, zd, 19))
+    for a in range(19):
+        eu = _EX[a] * u0 + _EY[a] * u1 + _EZ[a] * u2
+        f[..., a] = _W[a] * rho * (1.0 + 3.0 * eu + 4.5 * eu * eu - 1.5 * v) + 1e-4 * (r[..., 4 + a] - 0.5)
+    return f
+
+
+def write_uniform_file(path, first: np.ndarray, second: np.ndarray) -> None:
+    """lbf.TTTT of a uniform-grid run: [ftemp | f] in C order, native doubles."""
+    np.concatenate([first.reshape(-1), second.reshape(-1)]).astype(np.float64).tofile(path)
 
 
 def philox(ctr, key):

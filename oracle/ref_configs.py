@@ -37,8 +37,10 @@ def _tiny(**kw):
 
 
 REF_CONFIGS = {
-    "t_noslip": _tiny(main=True),
-    "t_ridges": _tiny(pattern="RSLIP", main=True),
+    # the two configurations with the unmodified main also carry a small uniform
+    # grid for its mode -i start
+    "t_noslip": _tiny(main=True, xdu=12, ydu=12, zdu=11),
+    "t_ridges": _tiny(pattern="RSLIP", main=True, xdu=12, ydu=12, zdu=11),
     "t_posts": _tiny(pattern="PSLIP"),
     "t_span": _tiny(pattern="SSLIP"),
     "t_gr4": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8),

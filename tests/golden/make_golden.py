@@ -6,7 +6,8 @@ compiled from the mounted reference sources) for N coarse steps, and record
 SHA-256 digests of the post-stream lattices and interface histories it writes,
 plus a few sampled values and the logged flow rate.  The tests check the CPU
 restatement against these digests on machines where the reference tree is not
-mounted.
+mounted.  A second file, ``uniform_golden.json``, holds the same digests for
+mode -i starts of the unmodified reference main from a uniform-grid file.
 
 Run from the repository root: ``python tests/golden/make_golden.py``.
 """
@@ -68,10 +69,46 @@ def run_case(name, mode, n):
     return out
 
 
+# mode -i starts: the unmodified reference main (``ref_main -i``) reads a
+# uniform-grid lbf.TSTR built by port.uniform_state and writes its restart at
+# the first iteration, before any step
+UNIFORM_CASES = [("t_noslip", 1, 2), ("t_ridges", 3, 4)]
+
+
+def run_uniform_case(name, seed_first, seed_second):
+    m = REF_CONFIGS[name]
+    xu, yu, zu, tstr = int(m["xdu"]), int(m["ydu"]), int(m["zdu"]), int(m["TSTR"])
+    p = port.Port(m)
+    out = {"config": name, "uniform": [xu, yu, zu], "seeds": [seed_first, seed_second], "cntr": tstr}
+    with tempfile.TemporaryDirectory() as d:
+        port.write_uniform_file(Path(d, f"lbf.{tstr:04d}"), port.uniform_state(xu, yu, zu, seed_first),
+                                port.uniform_state(xu, yu, zu, seed_second))
+        exe = ROOT / "oracle" / "_ref" / name / "ref_main"
+        subprocess.run([str(exe), "-i"], cwd=d, check=True, capture_output=True)
+        nx, ny, zdc, nxf, nyf, zdf = p.nx, p.ny, p.zdc, p.nxf, p.nyf, p.zdf
+        shapes = {"lbf-c": (nx, ny, zdc, 19), "lbf-slf": (nxf, nyf, zdf, 19), "lbf-suf": (nxf, nyf, zdf, 19)}
+        for fn, sh in shapes.items():
+            a = np.fromfile(Path(d, f"{fn}.{tstr:04d}"))
+            s = a[: a.size // 2].reshape(sh)
+            out[fn] = {"sha256": digest(s), "sum": float(s.sum())}
+        lin = np.fromfile(Path(d, f"lbf-lin.{tstr:04d}")).reshape(3, nx, ny, 23)
+        uin = np.fromfile(Path(d, f"lbf-uin.{tstr:04d}")).reshape(3, nx, ny, 23)
+        # level n: f^neq of the lower and upper planes; the density and velocity
+        # the reference writes into the lower history are the upper plane's
+        out["lin_fneq_n"] = digest(lin[0, ..., 4:])
+        out["uin_fneq_n"] = digest(uin[0, ..., 4:])
+        out["upper_moments_n"] = digest(lin[0, ..., :4])
+        out["force"] = float(np.fromfile(Path(d, f"force.{tstr:04d}"))[0])
+    return out
+
+
 def main():
     cases = [run_case(*c) for c in CASES]
     (Path(__file__).parent / "oracle_golden.json").write_text(json.dumps(cases, indent=1))
     print(f"wrote {len(cases)} cases")
+    uni = [run_uniform_case(*c) for c in UNIFORM_CASES]
+    (Path(__file__).parent / "uniform_golden.json").write_text(json.dumps(uni, indent=1))
+    print(f"wrote {len(uni)} uniform-start cases")
 
 
 if __name__ == "__main__":

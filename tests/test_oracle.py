@@ -13,6 +13,7 @@ import pytest
 from conftest import ROOT, ref_binary
 
 GOLDEN = json.loads((ROOT / "tests" / "golden" / "oracle_golden.json").read_text())
+UNIFORM_GOLDEN = json.loads((ROOT / "tests" / "golden" / "uniform_golden.json").read_text())
 
 
 def _digest(a):
@@ -237,3 +238,81 @@ def test_reference_field_files_layout(ref_configs, tmp_path):
                     ux, uy, uz, d = _moments_seq(lat[i, j, k])
                     assert (vel[i, j, k, 0], vel[i, j, k, 1], vel[i, j, k, 2], den[i, j, k]) == (ux, uy, uz, d), \
                         (lv, i, j, k)
+
+
+# ------------------------------------------------------------ mode -i start
+def _uniform_pair(port, m, tmp_path, seeds=(1, 2)):
+    xu, yu, zu, tstr = int(m["xdu"]), int(m["ydu"]), int(m["zdu"]), int(m["TSTR"])
+    first = port.uniform_state(xu, yu, zu, seeds[0])
+    port.write_uniform_file(tmp_path / f"lbf.{tstr:04d}", first, port.uniform_state(xu, yu, zu, seeds[1]))
+    p = port.Port(m)
+    p.set_forcing(True)
+    p.init_uniform(first)
+    return p, tstr
+
+
+@pytest.mark.parametrize("name", ["t_noslip", "t_ridges"])
+def test_port_uniform_start_matches_reference_main(port, ref_configs, tmp_path, name):
+    """Mode -i of the unmodified reference main (initializer + inter_init), its
+    restart written at the first iteration: the three post-stream lattices,
+    the f^neq history and the force are bit-identical.  Two slips of
+    inter_init are pinned as what they are: the reference's lower history
+    carries the upper plane's density and velocity (its upper one keeps
+    zeros), and its levels p and pp hold level n only where the flat index of
+    the halo-padded array is below the 19-field extent it copies."""
+    exe = ref_binary(name, "ref_main")
+    if exe is None:
+        pytest.skip("compiled reference main not available")
+    m = ref_configs[name]
+    p, tstr = _uniform_pair(port, m, tmp_path)
+    subprocess.run([str(exe), "-i"], cwd=tmp_path, check=True, capture_output=True)
+    for lvl, fn in enumerate(("lbf-c", "lbf-slf", "lbf-suf")):
+        a = np.fromfile(tmp_path / f"{fn}.{tstr:04d}")
+        np.testing.assert_array_equal(p.export(lvl).reshape(-1), a[: a.size // 2])
+    assert p.force() == np.fromfile(tmp_path / f"force.{tstr:04d}")[0]
+    h = p.history()
+    nx, ny = p.nx, p.ny
+    lin = np.fromfile(tmp_path / f"lbf-lin.{tstr:04d}").reshape(3, nx, ny, 23)
+    uin = np.fromfile(tmp_path / f"lbf-uin.{tstr:04d}").reshape(3, nx, ny, 23)
+    np.testing.assert_array_equal(h[0, 0, ..., 4:], lin[0, ..., 4:])
+    np.testing.assert_array_equal(h[0, 1, ..., 4:], uin[0, ..., 4:])
+    np.testing.assert_array_equal(h[0, 1, ..., :4], lin[0, ..., :4])
+    assert not uin[0, ..., :4].any()
+    # the restatement: p = pp = n in full
+    np.testing.assert_array_equal(h[1], h[0])
+    np.testing.assert_array_equal(h[2], h[0])
+    # the reference: inter_init.c:237-248 copies element q < 19 (xdc+5)(ydc+5)
+    # of the padded [xdc+5][ydc+5][23] array, xdc = xdv + 1, ydc = ydv + 1
+    i, j, b = np.meshgrid(np.arange(nx), np.arange(ny), np.arange(23), indexing="ij")
+    q = (i + 2) * (ny + 6) * 23 + (j + 2) * 23 + b
+    copied = q < 19 * (nx + 6) * (ny + 6)
+    for ref in (lin, uin):
+        for lvl in (1, 2):
+            np.testing.assert_array_equal(ref[lvl], np.where(copied, ref[0], 0.0))
+
+
+@pytest.mark.parametrize("case", UNIFORM_GOLDEN, ids=lambda c: c["config"])
+def test_port_uniform_start_golden(port, ref_configs, tmp_path, case):
+    """The restatement's mode -i start against digests of the reference main's."""
+    m = ref_configs[case["config"]]
+    assert [int(m["xdu"]), int(m["ydu"]), int(m["zdu"])] == case["uniform"]
+    p, _ = _uniform_pair(port, m, tmp_path, case["seeds"])
+    for lvl, fn in enumerate(("lbf-c", "lbf-slf", "lbf-suf")):
+        assert _digest(p.export(lvl)) == case[fn]["sha256"], fn
+    h = p.history()
+    assert _digest(h[0, 0, ..., 4:]) == case["lin_fneq_n"]
+    assert _digest(h[0, 1, ..., 4:]) == case["uin_fneq_n"]
+    assert _digest(h[0, 1, ..., :4]) == case["upper_moments_n"]
+    assert p.force() == case["force"]
+
+
+def test_port_uniform_start_rejects_short_grid(port, ref_configs):
+    """A uniform grid too short for the channel, whose stencils would leave
+    the reference's periodic halo in x or y, is refused."""
+    m = ref_configs["t_ridges"]
+    p = port.Port(m)
+    with pytest.raises(ValueError):
+        p.init_uniform(port.uniform_state(4, 12, 11, 1))
+    with pytest.raises(ValueError):
+        p.init_uniform(port.uniform_state(12, 4, 11, 1))
+    p.init_uniform(port.uniform_state(12, 12, 5, 1))   # a coarser wall-normal grid is fine
