@@ -46,7 +46,7 @@ class Params(C.Structure):
         ("gyplussize", C.c_int), ("wyplussize", C.c_int), ("gxplussize", C.c_int), ("wxplussize", C.c_int),
         ("pattern", C.c_int), ("XDIM", C.c_int), ("YDIM", C.c_int), ("ITER", C.c_long),
         ("forcing", C.c_int), ("force_const", C.c_double), ("precision", C.c_int), ("device", C.c_int),
-        ("xdu", C.c_int), ("ydu", C.c_int), ("zdu", C.c_int),
+        ("xdu", C.c_int), ("ydu", C.c_int), ("zdu", C.c_int), ("fltr", C.c_int),
     ]
 
 

@@ -56,7 +56,7 @@ struct Inst {
   float om_c, om_f, fac_if, fac_inj;
   // finalize constants (encalc2.c, wshearstr.c)
   double g3, norm, norm2, mu, ub, gconst, pgrad_scale, flow_scale, den_offset;
-  int cfr, pad;
+  int cfr, fltr;          // constant flow rate; filtered fine-to-coarse transfer (FLTR)
   float *fc[2], *ff[2];   // coarse / fine SoA deviations, ping-pong
   float *hist;            // 3 ring slots x [2 walls][23][ny][nx]
   float4 *corner;         // interface corner data [2 walls][23][ny][nx]

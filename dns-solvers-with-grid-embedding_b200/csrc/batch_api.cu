@@ -350,6 +350,7 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
   I.pgrad_scale = (g.nzs - 2.) / (2. * g.gr);
   I.flow_scale = (double)((long)g.nyf * (g.nzs - 2));
   I.cfr = q.forcing == DNS_FORCING_CFR ? 1 : 0;
+  I.fltr = q.fltr;
   I.den_offset = encalc2_weight_sum(d);
   const int slot = b->free_slots.back();
   I.slot = slot;

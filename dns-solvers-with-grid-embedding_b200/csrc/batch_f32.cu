@@ -418,7 +418,23 @@ __global__ void __launch_bounds__(kThreads) b_inject(const Mix *__restrict__ M, 
     const int ic = bx * kThreads + threadIdx.x;
     const int gr = I.gr, zdf = I.zdf, zds = I.zds, nx = I.nx, ny = I.ny, nzc = I.nzc;
     double acc[2] = {0., 0.};
-    if (ic < nx) {
+    if (I.fltr && ic < nx) {
+      float fo[19];
+      filtered_node_f32(I.ff[D.cf ^ (gr & 1)], I.nxf, I.nyf, zds, zdf, gr, wall, ic, jc, I.fac_inj, fo);
+      const int kc = wall == 0 ? 0 : nzc - 1;
+      const size_t cstride = (size_t)nzc * ny * nx;
+      float *cdst = I.fc[D.cc ^ 1];
+      float mom = 0.f, den = 0.f;
+#pragma unroll
+      for (int a = 0; a < 19; a++) {
+        cdst[(size_t)a * cstride + ((size_t)kc * ny + jc) * nx + ic] = fo[a];
+        den += fo[a];
+        if (ex_of(a) > 0) mom += fo[a];
+        if (ex_of(a) < 0) mom -= fo[a];
+      }
+      acc[0] = mom;
+      acc[1] = den;
+    } else if (ic < nx) {
       const int ps = wall == 0 ? (zdf - 1 - gr) - 1 : zds + gr;
       const size_t fstride = (size_t)2 * zds * I.nyf * I.nxf;
       float f[19];

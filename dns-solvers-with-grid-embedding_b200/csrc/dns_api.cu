@@ -153,6 +153,7 @@ extern "C" int dns_params_default(dns_params *p) {
   p->xdu = 512;
   p->ydu = 256;
   p->zdu = 221;
+  p->fltr = 0;
   return DNS_OK;
 }
 
@@ -196,6 +197,7 @@ extern "C" int dns_params_from_definitions(const char *path, dns_params *p) {
     else if (n == "RSLIP") p->pattern = DNS_PATTERN_RSLIP;
     else if (n == "PSLIP") p->pattern = DNS_PATTERN_PSLIP;
     else if (n == "SSLIP") p->pattern = DNS_PATTERN_SSLIP;
+    else if (n == "FLTR") p->fltr = 1;
   }
   std::fclose(fp);
   return DNS_OK;
@@ -212,6 +214,10 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   if (p->Rebs <= 0 || p->ub <= 0 || p->CFL <= 0) return fail(DNS_EINVAL, "Rebs, ub and CFL must be positive");
   if (p->precision != DNS_FP64 && p->precision != DNS_FP32) return fail(DNS_EINVAL, "precision must be DNS_FP64 or DNS_FP32");
   if (p->precision == DNS_FP32 && p->zds > 32) return fail(DNS_EINVAL, "the FP32 form supports zds <= 32");
+  if (p->fltr != 0 && p->fltr != 1) return fail(DNS_EINVAL, "fltr must be 0 or 1");
+  if (p->fltr && (p->gratio != 4 || p->zds < 7))
+    return fail(DNS_EINVAL,
+                "the filtered transfer (FLTR) needs gratio 4 (the reference's 5-plane stencil array) and zds >= 7");
   std::memset(g, 0, sizeof(*g));
   const int GR = p->gratio;
   g->gr = GR;
@@ -858,9 +864,10 @@ static void L_iface(dns_handle *h, int fbuf, int it, cudaStream_t st) {
 static void L_inject(dns_handle *h, int fbuf, int cbuf, cudaStream_t st) {
   if (is_f32(h))
     launch_inject_f32(F(h->ff[fbuf]), F(h->fc[cbuf]), h->d, h->shape, h->g.omega_c, h->g.omega_f, h->partials, h->pl,
-                      st);
+                      h->p.fltr != 0, st);
   else
-    launch_inject_f64(h->ff[fbuf], h->fc[cbuf], h->d, h->shape, h->g.omega_c, h->g.omega_f, h->partials, h->pl, st);
+    launch_inject_f64(h->ff[fbuf], h->fc[cbuf], h->d, h->shape, h->g.omega_c, h->g.omega_f, h->partials, h->pl,
+                      h->p.fltr != 0, st);
 }
 static void rotate_history(dns_handle *h) {
   // the new level n takes the slot of pp (xcomputations.c:548-556)

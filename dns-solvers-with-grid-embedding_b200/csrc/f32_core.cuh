@@ -117,6 +117,51 @@ __device__ __forceinline__ void load19f(const float *__restrict__ src, size_t id
   for (int a = 0; a < 19; a++) d[a] = __ldg(src + idx + (size_t)a * stride);
 }
 
+// ------------------------------------------------------------------ filtered transfer
+// One coarse vertex of the filtered fine-to-coarse transfer (FLTR,
+// ftcdtransfer_lesfltr.c:163-363, GR = 4) in deviation form: the trapezoid-
+// weighted (1/2, 1, 1, 1, 1/2 per axis) sum over the 5 x 5 x 5 fine nodes around
+// the vertex (planes kb-2..kb+2, x and y wrapped) of w f^neq / GR^3, added as
+// fac x sum to the deviation equilibrium of the vertex node's density and
+// momentum (the reference's equilibrium takes the momentum as the velocity).
+// Output: f - w of the coarse node.
+__device__ __forceinline__ void filtered_node_f32(const float *__restrict__ fs, int nxf, int nyf, int zds, int zdf,
+                                                  int gr, int wall, int ic, int jc, float fac, float (&out)[19]) {
+  const int kb = wall == 0 ? zdf - 1 - gr : gr;
+  const size_t fstride = (size_t)2 * zds * nyf * nxf;
+  const float inv_g3 = 1.f / (float)(gr * gr * gr);
+  const int i = ic * gr, j = jc * gr;
+  float t[19];
+#pragma unroll
+  for (int a = 0; a < 19; a++) t[a] = 0.f;
+  Mac32 c{};
+#pragma unroll 1
+  for (int ii = -2; ii < 3; ii++) {
+    const int x = wrapf(i + ii, nxf);
+#pragma unroll 1
+    for (int jj = -2; jj < 3; jj++) {
+      const int y = wrapf(j + jj, nyf);
+      const float wxy = ((ii == -2 || ii == 2) ? 0.5f : 1.f) * ((jj == -2 || jj == 2) ? 0.5f : 1.f) * inv_g3;
+#pragma unroll 1
+      for (int kk = -2; kk < 3; kk++) {
+        const int k = kb + kk;
+        const int p = wall == 0 ? k - 1 : zds + k;
+        float f[19];
+        load19f(fs, ((size_t)p * nyf + y) * nxf + x, fstride, f);
+        const Mac32 m = macro_f32(f);
+        if (ii == 0 && jj == 0 && kk == 0) c = m;
+        const float wq = wxy * ((kk == -2 || kk == 2) ? 0.5f : 1.f);
+#pragma unroll
+        for (int a = 0; a < 19; a++) t[a] += wq * (f[a] - deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq));
+      }
+    }
+  }
+  const float U0 = c.u0 * c.rho, U1 = c.u1 * c.rho, U2 = c.u2 * c.rho;
+  const float Usq = U0 * U0 + U1 * U1 + U2 * U2;
+#pragma unroll
+  for (int a = 0; a < 19; a++) out[a] = deq_f32(a, c.drho, c.rho, U0, U1, U2, Usq) + fac * t[a];
+}
+
 // ------------------------------------------------------------------ coarse
 template <bool STATS>
 __device__ __forceinline__ void coarse_node_f32(float (&f)[19], int i, int j, int k, const Dims &d, float om,

@@ -74,8 +74,10 @@ void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const 
 void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *mac, double *fdst,
                           const Dims &d, const LaunchShape &s, int substep, double omega_c, double omega_f,
                           cudaStream_t stream);
+// filtered: the FLTR transfer (ftcdtransfer_lesfltr.c) instead of ftcdtransfer.c
 void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
-                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
+                       double omega_f, double *partials, const PartialLayout &pl, bool filtered,
+                       cudaStream_t stream);
 // counter: one device unsigned int, zero between launches (the kernel resets it)
 void launch_finalize(DevState *st, DevLog *log_row, double *partials, unsigned int *counter,
                      const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
@@ -136,7 +138,8 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
 void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *corner, float *fdst,
                           const Dims &d, int substep, double omega_c, double omega_f, cudaStream_t stream);
 void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,
-                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream);
+                       double omega_f, double *partials, const PartialLayout &pl, bool filtered,
+                       cudaStream_t stream);
 void launch_flow_sums_f32(const float *fc, const float *ff, DevState *st, double *partials, const PartialLayout &pl,
                           const Dims &d, const LaunchShape &s, const StepParams &sp, cudaStream_t stream);
 void launch_seed_f32(float *fc, float *ff, float *hist3, const Dims &d, uint64_t seed, double uc, double amp,

@@ -153,12 +153,28 @@ __global__ void __launch_bounds__(kThreads) iface_eval_f32(IfParams32 P) {
 }
 
 // ------------------------------------------------------------------ injection
+template <bool FLT>
 __global__ void __launch_bounds__(kThreads) inject_f32(const float *__restrict__ fsrc, float *__restrict__ cdst, Dims d,
                                                       float fac, double *__restrict__ part) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc, gr = d.gr, zdf = d.zdf, zds = d.zds;
   const int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y, w = blockIdx.z;
   double acc[2] = {0., 0.};
-  if (ic < nx) {
+  if (FLT && ic < nx) {
+    float fo[19];
+    filtered_node_f32(fsrc, d.nxf, d.nyf, zds, zdf, gr, w, ic, jc, fac, fo);
+    const int kc = w == 0 ? 0 : nzc - 1;
+    const size_t cstride = (size_t)nzc * ny * nx;
+    float mom = 0.f, den = 0.f;
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      cdst[(size_t)a * cstride + ((size_t)kc * ny + jc) * nx + ic] = fo[a];
+      den += fo[a];
+      if (ex_of(a) > 0) mom += fo[a];
+      if (ex_of(a) < 0) mom -= fo[a];
+    }
+    acc[0] = mom;
+    acc[1] = den;
+  } else if (!FLT && ic < nx) {
     const int ps = w == 0 ? (zdf - 1 - gr) - 1 : zds + gr;
     const size_t fstride = (size_t)2 * zds * d.nyf * d.nxf;
     float f[19];
@@ -435,9 +451,14 @@ void launch_interface_f32(const float *hn, const float *hp, const float *hpp, fl
 }
 
 void launch_inject_f32(const float *fsrc, float *cdst, const Dims &d, const LaunchShape &s, double omega_c,
-                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream) {
+                       double omega_f, double *partials, const PartialLayout &pl, bool filtered,
+                       cudaStream_t stream) {
   dim3 grid(s.jgx, s.jgy, 2), block(s.bx);
-  inject_f32<<<grid, block, 0, stream>>>(fsrc, cdst, d, (float)(d.gr * (omega_f / omega_c)), partials + pl.inject);
+  const float fac = (float)(d.gr * (omega_f / omega_c));
+  if (filtered)
+    inject_f32<true><<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
+  else
+    inject_f32<false><<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
 }
 
 void launch_flow_sums_f32(const float *fc, const float *ff, DevState *st, double *partials, const PartialLayout &pl,

@@ -435,13 +435,92 @@ __global__ void __launch_bounds__(TPX *TPY) interface_pop_kernel(const double *_
 // vertex at lower k = zdf-1-GR / upper k = GR gives the coarse planes 0 and
 // zdc-1 as feq + GR omega_f/omega_c (f - feq).  Partials: what this writes into
 // the state weighs GR^3 / 2 in encalc2.
+//
+// Filtered form (FLTR, ftcdtransfer_lesfltr.c:163-363, GR = 4): f - feq of each
+// of the 5 x 5 x 5 fine nodes around the vertex (planes kb-2..kb+2, x and y
+// wrapped), summed as (w f^neq) / GR^3 with the trapezoid weights
+// (1/2, 1, 1, 1, 1/2) per axis, x outer, z inner; the equilibrium is that of
+// the vertex node's density and momentum sums (the reference keeps the
+// momentum where it reads the velocity back, :185-188, :222-225).
+__device__ __forceinline__ double trapezoid5(int q) { return (q == -2 || q == 2) ? 0.5 : 1.0; }
+
+__device__ __forceinline__ void filtered_node_f64(const double *__restrict__ fsrc, const Dims &d, int w, int ic,
+                                                  int jc, double fac, double (&out)[19]) {
+  const int gr = d.gr, zds = d.zds, nxf = d.nxf, nyf = d.nyf;
+  const int kb = w == 0 ? d.zdf - 1 - gr : gr;
+  const size_t fstride = (size_t)2 * zds * nyf * nxf;
+  const double g3 = (double)gr * gr * gr;
+  const int i = ic * gr, j = jc * gr;
+  double t[19];
+#pragma unroll
+  for (int a = 0; a < 19; a++) t[a] = 0.;
+  double cdens = 0., cmx = 0., cmy = 0., cmz = 0.;
+#pragma unroll 1
+  for (int ii = -2; ii < 3; ii++) {
+    int x = i + ii;
+    x = x < 0 ? x + nxf : (x >= nxf ? x - nxf : x);
+#pragma unroll 1
+    for (int jj = -2; jj < 3; jj++) {
+      int y = j + jj;
+      y = y < 0 ? y + nyf : (y >= nyf ? y - nyf : y);
+      const double wxy = trapezoid5(ii) * trapezoid5(jj);
+#pragma unroll 1
+      for (int kk = -2; kk < 3; kk++) {
+        const int k = kb + kk;
+        const int p = w == 0 ? k - 1 : zds + k;
+        double f[19];
+        load19(fsrc, ((size_t)p * nyf + y) * nxf + x, fstride, f);
+        double dens, mx, my, mz;
+        moments_f64(f, dens, mx, my, mz);
+        if (ii == 0 && jj == 0 && kk == 0) {
+          cdens = dens;
+          cmx = mx;
+          cmy = my;
+          cmz = mz;
+        }
+        const double u0 = mx / dens, u1 = my / dens, u2 = mz / dens;
+        const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+        const Weighted wr = weighted_rho(dens);
+        const double wgt = wxy * trapezoid5(kk);
+#pragma unroll
+        for (int a = 0; a < 19; a++) {
+          const int c = wclass_of(a);
+          const double feq = feq_f64(c == 0 ? wr.w0 : (c == 1 ? wr.w1 : wr.w2), proj_f64(a, u0, u1, u2), t15v);
+          t[a] += (wgt * (f[a] - feq)) / g3;
+        }
+      }
+    }
+  }
+  const double t15v = 1.5 * (cmx * cmx + cmy * cmy + cmz * cmz);
+  const Weighted wr = weighted_rho(cdens);
+#pragma unroll
+  for (int a = 0; a < 19; a++) {
+    const int c = wclass_of(a);
+    const double feq = feq_f64(c == 0 ? wr.w0 : (c == 1 ? wr.w1 : wr.w2), proj_f64(a, cmx, cmy, cmz), t15v);
+    out[a] = feq + fac * t[a];
+  }
+}
+
+template <bool FLT>
 __global__ void __launch_bounds__(kMaxThreads) inject_kernel(const double *__restrict__ fsrc,
                                                             double *__restrict__ cdst, Dims d, double fac,
                                                             double *__restrict__ part) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc, gr = d.gr, zdf = d.zdf, zds = d.zds;
   const int ic = blockIdx.x * blockDim.x + threadIdx.x, jc = blockIdx.y, w = blockIdx.z;
   double acc[2] = {0., 0.};
-  if (ic < nx) {
+  if (FLT && ic < nx) {
+    double fo[19];
+    filtered_node_f64(fsrc, d, w, ic, jc, fac, fo);
+    const int kc = w == 0 ? 0 : nzc - 1;
+    const size_t cstride = (size_t)nzc * ny * nx;
+#pragma unroll
+    for (int a = 0; a < 19; a++) {
+      cdst[(size_t)a * cstride + ((size_t)kc * ny + jc) * nx + ic] = fo[a];
+      acc[1] += fo[a];
+      if (ex_of(a) > 0) acc[0] += fo[a];
+      if (ex_of(a) < 0) acc[0] -= fo[a];
+    }
+  } else if (!FLT && ic < nx) {
     const int ps = w == 0 ? (zdf - 1 - gr) - 1 : zds + gr;  // lower k = zdf-1-GR, upper k = GR
     const size_t fstride = (size_t)2 * zds * d.nyf * d.nxf;
     double f[19];
@@ -923,10 +1002,14 @@ void launch_interface_f64(const double *hn, const double *hp, const double *hpp,
 }
 
 void launch_inject_f64(const double *fsrc, double *cdst, const Dims &d, const LaunchShape &s, double omega_c,
-                       double omega_f, double *partials, const PartialLayout &pl, cudaStream_t stream) {
+                       double omega_f, double *partials, const PartialLayout &pl, bool filtered,
+                       cudaStream_t stream) {
   const double fac = d.gr * (omega_f / omega_c);
   dim3 grid(s.jgx, s.jgy, 2), block(s.bx);
-  inject_kernel<<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
+  if (filtered)
+    inject_kernel<true><<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
+  else
+    inject_kernel<false><<<grid, block, 0, stream>>>(fsrc, cdst, d, fac, partials + pl.inject);
 }
 
 static FinArgs fin_args(const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp) {

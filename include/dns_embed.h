@@ -66,6 +66,11 @@ typedef struct dns_params {
   int device;           /* CUDA device ordinal */
   /* uniform grid of a mode -i start (definitions.h:103-109): xdu x ydu x (zdu + 2) */
   int xdu, ydu, zdu;
+  /* 1 when FLTR is defined (definitions.h:87-88): the filtered fine-to-coarse
+     transfer of ftcdtransfer_lesfltr.c instead of ftcdtransfer.c.  The
+     reference defines it for gratio 4 (its stencil array holds gratio + 1 = 5
+     planes) and it needs zds >= 7; other combinations are DNS_EINVAL. */
+  int fltr;
 } dns_params;
 
 /* Derived sizes; computed on the host, no GPU needed. */

@@ -48,6 +48,7 @@ from ref_configs import REF_CONFIGS  # noqa: E402
 VALUE_MACROS = ("Rebs", "ub", "zdv", "ydv", "xdv", "TSTR", "TEND", "CFL", "gratio", "zds",
                 "gyplussize", "wyplussize", "gxplussize", "wxplussize", "XDIM", "YDIM", "xdu", "ydu", "zdu")
 PATTERNS = ("PSLIP", "RSLIP", "SSLIP")
+# "fltr": True selects the filtered fine-to-coarse transfer (FLTR instead of NOFLTR)
 
 
 def render_definitions(cfg: dict) -> str:
@@ -64,6 +65,11 @@ def render_definitions(cfg: dict) -> str:
                 continue
             if name in PATTERNS:
                 out.append(f"#define {name}" if cfg.get("pattern") == name else f"//#define {name}")
+                seen.add(name)
+                continue
+            if name in ("NOFLTR", "FLTR"):
+                on = bool(cfg.get("fltr")) == (name == "FLTR")
+                out.append(f"#define {name}" if on else f"//#define {name}")
                 seen.add(name)
                 continue
             if name == "ITER":

@@ -513,6 +513,64 @@ static void inject(port_state *s) {
   }
 }
 
+/* filtered fine-to-coarse transfer (ftcdtransfer_lesfltr.c:163-363, FLTR),
+   for GR = 4: f^neq of every fine node of the five planes kb-2..kb+2 around the
+   transfer plane kb (:166-196), a sum over the 5 x 5 x 5 nodes around the coarse
+   vertex of weight x f^neq / GR^3 with the trapezoid weights (1/2, 1, 1, 1, 1/2)
+   per axis (:22-27, :232-246), in the order (x, y, z) outer, population inner,
+   and the equilibrium of the centre node's density and MOMENTUM: the reference
+   stores the momentum sums where it later reads the velocity (:185-188,
+   :222-225).  x and y wrap periodically, as the halo exchange does. */
+static void inject_filtered(port_state *s) {
+  static const double c5[5] = {0.5, 1., 1., 1., 0.5};
+  int gr = s->gr, nxf = s->nxf, nyf = s->nyf;
+  double fac = gr * (s->omf / s->omc);
+  double *fq = (double *)malloc(sizeof(double) * (size_t)nxf * nyf * 5 * 19);
+  double *mc = (double *)malloc(sizeof(double) * (size_t)nxf * nyf * 4);
+  for (int w = 0; w < 2; w++) {
+    const double *src = w == 0 ? s->fl[0] : s->fu[0];
+    int kb = w == 0 ? s->zdf - 1 - gr : gr;
+    int kc = w == 0 ? 0 : s->zdc - 1;
+    for (int i = 0; i < nxf; i++)
+      for (int j = 0; j < nyf; j++)
+        for (int kk = -2; kk < 3; kk++) {
+          const double *f = src + FIDX(s, i, j, kb + kk);
+          double dens, ux, uy, uz;
+          moments(f, &dens, &ux, &uy, &uz);
+          double u0 = ux / dens, u1 = uy / dens, u2 = uz / dens;
+          double v = u0 * u0 + u1 * u1 + u2 * u2;
+          double *o = fq + (((size_t)i * nyf + j) * 5 + (kk + 2)) * 19;
+          for (int a = 0; a < 19; a++) o[a] = f[a] - feq_of(a, dens, u0, u1, u2, v);
+          if (kk == 0) {
+            double *m = mc + ((size_t)i * nyf + j) * 4;
+            m[0] = dens;
+            m[1] = ux;
+            m[2] = uy;
+            m[3] = uz;
+          }
+        }
+    for (int ic = 0; ic < s->nx; ic++)
+      for (int jc = 0; jc < s->ny; jc++) {
+        int i = ic * gr, j = jc * gr;
+        const double *m = mc + ((size_t)i * nyf + j) * 4;
+        double dens = m[0], u0 = m[1], u1 = m[2], u2 = m[3];
+        double v = u0 * u0 + u1 * u1 + u2 * u2;
+        double t[19] = {0.};
+        for (int ii = -2; ii < 3; ii++)
+          for (int jj = -2; jj < 3; jj++)
+            for (int kk = -2; kk < 3; kk++) {
+              double wgt = c5[ii + 2] * c5[jj + 2] * c5[kk + 2];
+              const double *q = fq + (((size_t)wrap(i + ii, nxf) * nyf + wrap(j + jj, nyf)) * 5 + (kk + 2)) * 19;
+              for (int a = 0; a < 19; a++) t[a] += (wgt * q[a]) / ((double)gr * gr * gr);
+            }
+        double *o = s->fc[1] + CIDX(s, ic, jc, kc);
+        for (int a = 0; a < 19; a++) o[a] = feq_of(a, dens, u0, u1, u2, v) + fac * t[a];
+      }
+  }
+  free(fq);
+  free(mc);
+}
+
 static void swap2(double **p) {
   double *t = p[0];
   p[0] = p[1];
@@ -538,7 +596,8 @@ void port_step(port_state *s, long n, port_log *log) {
       swap2(s->fl);
       swap2(s->fu);
     }
-    inject(s);
+    if (s->c.fltr) inject_filtered(s);
+    else inject(s);
     swap2(s->fc);
     if (log) log[st] = lg;
   }

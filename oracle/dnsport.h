@@ -30,6 +30,7 @@ typedef struct port_cfg {
   double Reb, ub, CFL;
   int pattern;
   int gy, wy, gx, wx; /* gyplussize, wyplussize, gxplussize, wxplussize */
+  int fltr;           /* 1: filtered fine-to-coarse transfer (FLTR), GR = 4 */
 } port_cfg;
 
 /* one coarse step's log values (reference encalc2.c / wshearstr.c) */

@@ -22,13 +22,14 @@ PATTERNS = {None: 0, "RSLIP": 1, "PSLIP": 2, "SSLIP": 3}
 class PortCfg(C.Structure):
     _fields_ = [("xdv", C.c_int), ("ydv", C.c_int), ("zdc", C.c_int), ("zds", C.c_int), ("gr", C.c_int),
                 ("Reb", C.c_double), ("ub", C.c_double), ("CFL", C.c_double), ("pattern", C.c_int),
-                ("gy", C.c_int), ("wy", C.c_int), ("gx", C.c_int), ("wx", C.c_int)]
+                ("gy", C.c_int), ("wy", C.c_int), ("gx", C.c_int), ("wx", C.c_int), ("fltr", C.c_int)]
 
     @classmethod
     def from_macros(cls, m: dict) -> "PortCfg":
         return cls(int(m["xdv"]), int(m["ydv"]), int(m["zdv"]), int(m["zds"]), int(m["gratio"]),
                    float(m["Rebs"]), float(m["ub"]), float(m["CFL"]), PATTERNS[m.get("pattern")],
-                   int(m["gyplussize"]), int(m["wyplussize"]), int(m["gxplussize"]), int(m["wxplussize"]))
+                   int(m["gyplussize"]), int(m["wyplussize"]), int(m["gxplussize"]), int(m["wxplussize"]),
+                   1 if m.get("fltr") else 0)
 
 
 class PortLog(C.Structure):

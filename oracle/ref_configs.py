@@ -44,6 +44,10 @@ REF_CONFIGS = {
     "t_posts": _tiny(pattern="PSLIP"),
     "t_span": _tiny(pattern="SSLIP"),
     "t_gr4": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8),
+    # the filtered fine-to-coarse transfer (FLTR), defined by the reference for
+    # GR = 4 (its stencil array holds GR + 1 = 5 planes)
+    "t_gr4f": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8, fltr=True,
+                    main=True),
     "t_odd": _tiny(xdv=12, ydv=6, zdv=9, zds=6, pattern="RSLIP", gyplussize=6, wyplussize=6),
     "c1": dict(Rebs=repr(150.0 * UB * _h(27, 8, 2)), ub=UB, zdv=27, ydv=64, xdv=64, TSTR=0, TEND=1,
                CFL=0.1, gratio=2, zds=8, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4,

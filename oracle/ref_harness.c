@@ -10,7 +10,8 @@
  *   encalc2 -> wshearstr -> [statistics] -> xcomputations ->
  *   (GR-1) x {xfcomputations, tinterpolate_hrmt, derivative x2, ctfdtransfer_opt, fexchange} ->
  *   xfcomputations, tinterpolate_hrmt(GR), derivative x2, ctfdtransfer_opt(GR),
- *   ftcdtransfer, exchange, fexchange
+ *   ftcdtransfer (ftcdtransfer_lesfltr when FLTR is defined, as main does at
+ *   :1366-1372), exchange, fexchange
  *
  * The only departure from main is the forcing switch: in constant-force mode
  * force[0] is reset to the given value after encalc2 (which still runs, so the
@@ -290,7 +291,11 @@ cold_start:
     derivative(xdc, ydc, V.uint);
     derivative(xdc, ydc, V.lint);
     V = ctfdtransfer_opt(xdc, ydc, zdc, xdf, ydf, zdf, GR, tauc, tauf, GR, V, pd);
+#ifdef FLTR
+    V = ftcdtransfer_lesfltr(xdf, ydf, zdf, xdc, ydc, zdc, GR, tauc, tauf, GR, V, pd);
+#else
     V = ftcdtransfer(xdc, ydc, zdc, xdf, ydf, zdf, GR, tauc, tauf, GR, V, pd);
+#endif
     V = exchange(V);
     V = fexchange(V);
   }

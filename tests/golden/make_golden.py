@@ -30,7 +30,7 @@ from ref_configs import REF_CONFIGS  # noqa: E402
 
 CASES = [
     ("t_noslip", "const", 20), ("t_noslip", "cfr", 20), ("t_ridges", "cfr", 20), ("t_posts", "const", 20),
-    ("t_span", "cfr", 20), ("t_gr4", "cfr", 10), ("t_odd", "const", 20),
+    ("t_span", "cfr", 20), ("t_gr4", "cfr", 10), ("t_odd", "const", 20), ("t_gr4f", "cfr", 10),
 ]
 SEED, UC, AMP, GCONST = 42, 0.05, 0.005, 1.0e-5
 

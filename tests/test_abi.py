@@ -33,6 +33,7 @@ def test_library_exports_every_declared_symbol(pkg):
 def test_defaults_mirror_reference_definitions(pkg):
     p = pkg.default_params()
     assert (p.xdv, p.ydv, p.zdv, p.zds, p.gratio) == (512, 256, 220, 10, 4)
+    assert (p.xdu, p.ydu, p.zdu, p.fltr) == (512, 256, 221, 0)
     assert p.Rebs == 7200.0 and p.ub == 0.0866034 and p.CFL == 0.1
     assert p.pattern == pkg.PATTERN_RSLIP and p.ITER < 0
 
@@ -54,11 +55,20 @@ def test_params_from_definitions_file(pkg, tmp_path):
 //#define SSLIP
 #define XDIM 4
 #define YDIM 2
+#define NOFLTR
+//#define FLTR
 //#define ITER 1
+#define xdu 384
+#define ydu 192
+#define zdu 95
 """)
     p = pkg.params_from_definitions(src)
     assert (p.xdv, p.ydv, p.zdv, p.zds, p.gratio) == (256, 128, 83, 16, 2)
     assert p.pattern == pkg.PATTERN_RSLIP and p.ITER < 0 and p.Rebs == 5533.0
+    assert (p.xdu, p.ydu, p.zdu) == (384, 192, 95) and p.fltr == 0
+    src.write_text(src.read_text().replace("#define NOFLTR", "//#define NOFLTR").replace("//#define FLTR",
+                                                                                        "#define FLTR"))
+    assert pkg.params_from_definitions(src).fltr == 1
     with pytest.raises(pkg.DnsError) as e:
         pkg.params_from_definitions(tmp_path / "missing.h")
     assert e.value.code == pkg.DNS_EIO
@@ -83,7 +93,9 @@ def test_geometry_matches_reference_formulas(pkg, port, ref_configs):
 
 
 @pytest.mark.parametrize("bad", [dict(gratio=1), dict(zds=2), dict(zdv=3), dict(xdv=2), dict(Rebs=-1.0),
-                                 dict(pattern=9), dict(precision=7)])
+                                 dict(pattern=9), dict(precision=7), dict(fltr=2),
+                                 dict(fltr=1),                       # FLTR is defined for gratio 4
+                                 dict(fltr=1, gratio=4, zds=6)])     # and needs zds >= 7
 def test_invalid_parameters_are_rejected(pkg, bad):
     p = pkg.make_params(xdv=16, ydv=16, zdv=9, zds=6, gratio=2)
     for k, v in bad.items():

@@ -31,7 +31,7 @@ def states(b, i):
 
 
 @pytest.mark.parametrize("name,mode", [("t_noslip", "const"), ("t_ridges", "cfr"), ("t_posts", "cfr"),
-                                       ("t_span", "const"), ("t_gr4", "cfr"), ("t_odd", "cfr")])
+                                       ("t_span", "const"), ("t_gr4", "cfr"), ("t_gr4f", "cfr"), ("t_odd", "cfr")])
 def test_batch_instance_tracks_fp64_oracle(pkg, port, ref_configs, name, mode):
     m = ref_configs[name]
     with pkg.Batch() as b:

@@ -45,7 +45,7 @@ def test_fp32_seed_is_one_rounding_of_fp64(pkg, port, ref_configs, name):
 
 
 @pytest.mark.parametrize("name,mode", [("t_noslip", "const"), ("t_ridges", "cfr"), ("t_posts", "cfr"),
-                                       ("t_span", "const"), ("t_gr4", "cfr"), ("t_odd", "cfr")])
+                                       ("t_span", "const"), ("t_gr4", "cfr"), ("t_gr4f", "cfr"), ("t_odd", "cfr")])
 def test_fp32_steps_track_fp64(pkg, port, ref_configs, name, mode):
     ch, o = pair32(pkg, port, ref_configs[name], mode)
     la = ch.step(30)

@@ -24,7 +24,8 @@ def params_for(pkg, m, mode, g=GCONST):
         xdv=m["xdv"], ydv=m["ydv"], zdv=m["zdv"], zds=m["zds"], gratio=m["gratio"], Rebs=float(m["Rebs"]),
         ub=m["ub"], CFL=m["CFL"], TSTR=m["TSTR"], pattern=m.get("pattern"), gyplussize=m["gyplussize"],
         wyplussize=m["wyplussize"], gxplussize=m["gxplussize"], wxplussize=m["wxplussize"],
-        forcing=pkg.FORCING_CFR if mode == "cfr" else pkg.FORCING_CONST, force_const=g if mode == "const" else 0.0)
+        forcing=pkg.FORCING_CFR if mode == "cfr" else pkg.FORCING_CONST, force_const=g if mode == "const" else 0.0,
+        fltr=1 if m.get("fltr") else 0)
 
 
 def pair(pkg, port, m, mode, g=GCONST, seed=42, uc=0.05, amp=0.005):
@@ -53,8 +54,8 @@ def assert_state(ch, p, exact, rtol=RTOL_CFR):
 
 
 CASES = [("t_noslip", "const"), ("t_noslip", "cfr"), ("t_ridges", "cfr"), ("t_posts", "const"),
-         ("t_posts", "cfr"), ("t_span", "cfr"), ("t_gr4", "const"), ("t_gr4", "cfr"), ("t_odd", "const"),
-         ("t_odd", "cfr")]
+         ("t_posts", "cfr"), ("t_span", "cfr"), ("t_gr4", "const"), ("t_gr4", "cfr"), ("t_gr4f", "const"),
+         ("t_gr4f", "cfr"), ("t_odd", "const"), ("t_odd", "cfr")]
 
 
 @pytest.mark.parametrize("name", ["t_noslip", "t_gr4", "t_odd", "c1"])

@@ -105,7 +105,8 @@ def test_port_matches_golden(port, ref_configs, case):
 
 
 @pytest.mark.parametrize("name,mode,steps", [("t_noslip", "cfr", 12), ("t_posts", "cfr", 12),
-                                             ("t_gr4", "const", 6), ("t_odd", "cfr", 12)])
+                                             ("t_gr4", "const", 6), ("t_gr4f", "cfr", 12), ("t_gr4f", "const", 6),
+                                             ("t_odd", "cfr", 12)])
 def test_port_matches_compiled_reference(port, ref_configs, tmp_path, name, mode, steps):
     exe = ref_binary(name)
     if exe is None:
@@ -129,7 +130,7 @@ def test_port_matches_compiled_reference(port, ref_configs, tmp_path, name, mode
         np.testing.assert_array_equal(h[:, w].reshape(-1), np.fromfile(dout / f"{fn}.0004"))
 
 
-@pytest.mark.parametrize("name", ["t_noslip", "t_ridges"])
+@pytest.mark.parametrize("name", ["t_noslip", "t_ridges", "t_gr4f"])
 def test_port_matches_reference_main(port, ref_configs, tmp_path, name):
     """Pin against the unmodified reference main program (mode -p, ITER = 50,
     one unit time per step): its restart written at step 50, and its
