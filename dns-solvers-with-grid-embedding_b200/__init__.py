@@ -29,6 +29,14 @@ STAT_NAMES = ("z", "U", "V", "W", "rho", "uu", "vv", "ww", "uw", "rr", "uu_t", "
 NKERNEL = 7
 KERNEL_NAMES = ("coarse", "extract", "fine", "interface", "inject", "finalize", "stats")
 PLANE_STAT_NAMES = ("UAVG", "VAVG", "WAVG", "UTIN", "VTIN", "WTIN", "REYS", "DAVG", "DTIN")
+# profiles of dns_tke_budget, in the order of the reference's turb-fld-2d (19),
+# vort-fluc-2d (3) and KE-Budget-2d (30) files
+TKE_FILES = (("turb-fld-2d", 19), ("vort-fluc-2d", 3), ("KE-Budget-2d", 30))
+TKE_NAMES = ("UAVG", "VAVG", "WAVG", "UTIN", "VTIN", "WTIN", "uw", "DAVG", "DTIN", "SKEWu", "SKEWv", "SKEWw",
+             "SKEWuw", "SKEWp", "KURTu", "KURTv", "KURTw", "KURTuw", "KURTp", "wx", "wy", "wz", "Pii", "Puu", "Pvv",
+             "Pww", "Puw", "Tiir", "Tuur", "Tvvr", "Twwr", "Tuwr", "Tiipai", "Tuupai", "Tvvpai", "Twwpai", "Tuwpai",
+             "Paiuu", "Paivv", "Paiww", "Paiuw", "Tiis", "Tuus", "Tvvs", "Twws", "Tuws", "Epii", "Epuu", "Epvv",
+             "Epww", "Epuw", "KE")
 
 
 class DnsError(RuntimeError):
@@ -107,6 +115,9 @@ def lib() -> C.CDLL:
         "dns_write_restart": (I, [P, C.c_char_p, I]),
         "dns_load_uniform": (I, [P, C.c_char_p, I]),
         "dns_write_fields": (I, [P, C.c_char_p, I]),
+        "dns_tke_budget": (I, [P, P, P, P]),
+        "dns_tke_budget_files": (I, [C.POINTER(Params), C.c_char_p, I, P, P, P]),
+        "dns_write_tke_budget": (I, [C.POINTER(Params), C.c_char_p, I, P, P, P]),
         "dns_init_seeded": (I, [P, C.c_uint64, D, D]),
         "dns_export_state": (I, [P, I, P]),
         "dns_import_state": (I, [P, I, P]),
@@ -228,6 +239,13 @@ class Channel:
         """vel-{c,slf,suf} / den-{c,slf,suf} field files (the reference's vel_print)."""
         _check(lib().dns_write_fields(self.h, str(directory).encode(), cntr), "dns_write_fields")
 
+    def tke_budget(self, fluct_plane: bool = False):
+        """Turbulence statistics and kinetic-energy budget of the current state
+        (the reference's TKE-budget/computations on the fields vel_print would
+        write): (TKE_NAMES x NZ) profiles, plus the u / v fluctuations of the
+        lower fine plane k = 4 when fluct_plane."""
+        return _tke_call(self.params, lambda pr, u, v: lib().dns_tke_budget(self.h, pr, u, v), fluct_plane)
+
     def _level_shape(self, level: int):
         g = self.geom
         return (g.nx, g.ny, g.nzc, 19) if level == 0 else (g.nxf, g.nyf, g.zdf, 19)
@@ -293,6 +311,32 @@ class Channel:
         out = np.zeros((9, self.geom.nz_profile))
         _check(lib().dns_plane_stats(self.h, out.ctypes.data), "dns_plane_stats")
         return out
+
+
+def _tke_call(p: Params, fn, fluct_plane: bool):
+    g = geometry(p)
+    prof = np.zeros((len(TKE_NAMES), g.nz_profile))
+    ufl = vfl = None
+    if fluct_plane:
+        ufl = np.zeros((g.nxf, g.nyf))
+        vfl = np.zeros((g.nxf, g.nyf))
+    ptr = lambda a: None if a is None else a.ctypes.data
+    _check(fn(prof.ctypes.data, ptr(ufl), ptr(vfl)), "dns_tke_budget")
+    return (prof, ufl, vfl) if fluct_plane else prof
+
+
+def tke_budget_files(p: Params, directory, cntr: int, fluct_plane: bool = False):
+    """The budget from vel-* / den-* files of snapshot cntr in directory."""
+    d = str(directory).encode()
+    return _tke_call(p, lambda pr, u, v: lib().dns_tke_budget_files(C.byref(p), d, cntr, pr, u, v), fluct_plane)
+
+
+def write_tke_budget(p: Params, directory, cntr: int, prof, ufl=None, vfl=None):
+    """turb-fld-2d / vort-fluc-2d / KE-Budget-2d (.000.cntr) and ufl4 / vfl4 files."""
+    prof, ufl, vfl = (None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (prof, ufl, vfl))
+    ptr = lambda a: None if a is None else a.ctypes.data
+    _check(lib().dns_write_tke_budget(C.byref(p), str(directory).encode(), cntr, prof.ctypes.data, ptr(ufl), ptr(vfl)),
+           "dns_write_tke_budget")
 
 
 def batch_footprint(p: Params) -> int:

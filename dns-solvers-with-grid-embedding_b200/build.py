@@ -2,7 +2,7 @@
 
 ``kernels_f64.cu`` is compiled with ``-fmad=false``: the FP64 plain form must
 not fuse multiply-adds, so that its per-node arithmetic rounds exactly like the
-reference.  Everything else uses the default flags.  Run
+reference.  ``tke.cu`` (the statistics / budget analysis) likewise.  Everything else uses the default flags.  Run
 ``python build.py`` (or call ``build()``); nvcc cross-compiles without a GPU.
 """
 from __future__ import annotations
@@ -26,6 +26,7 @@ UNITS = {  # source -> extra flags
     "dns_api.cu": [],
     "batch_api.cu": [],
     "noalloc.cu": [],
+    "tke.cu": ["-fmad=false"],
 }
 
 

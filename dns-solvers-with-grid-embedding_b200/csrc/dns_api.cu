@@ -743,6 +743,34 @@ extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
 }
 
 // ---------------------------------------------------------------- field output
+// vel_print's moments of a wall plane held on the host (n nodes): vel[n][3], den[n]
+static void wall_plane_fields(const std::vector<double> &wall, size_t n, double *vel, double *den) {
+  static const double EX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0};
+  static const double EY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
+  static const double EZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+  for (size_t c = 0; c < n; c++) {
+    const double *f = wall.data() + c * 19;
+    double ux = 0., uy = 0., uz = 0., dens = 0.;
+    for (int a = 0; a < 19; a++) {
+      ux += EX[a] * f[a];
+      uy += EY[a] * f[a];
+      uz += EZ[a] * f[a];
+      dens += f[a];
+    }
+    if (dens > 0.) {
+      ux /= dens;
+      uy /= dens;
+      uz /= dens;
+    } else {
+      ux = uy = uz = dens = 0.;
+    }
+    vel[c * 3] = ux;
+    vel[c * 3 + 1] = uy;
+    vel[c * 3 + 2] = uz;
+    den[c] = dens;
+  }
+}
+
 // vel_print.c:15-275 (called by main at :1342): per level, u = (sum E f) / rho
 // and rho = sum f of the post-stream state, summed in population order, zero
 // where rho <= 0; vel-* (nx, ny, nz, 3) and den-* (nx, ny, nz), C order,
@@ -761,9 +789,6 @@ extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
     return fail(DNS_ENOMEM, "field staging");
   }
   std::vector<double> vel(nmax * 3), den(nmax);
-  static const double EX[19] = {0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, 1, -1, -1, 0, 0, 0, 0};
-  static const double EY[19] = {0, 0, 0, 1, -1, 0, 0, 1, 1, -1, -1, 0, 0, 0, 0, 1, 1, -1, -1};
-  static const double EZ[19] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, -1, -1, 1, 1, -1, -1, 1};
   const char *names[3] = {"c", "slf", "suf"};
   int rc = DNS_OK;
   for (int lv = 0; lv < 3 && rc == DNS_OK; lv++) {
@@ -785,29 +810,14 @@ extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
       break;
     }
     if (lv > 0) {
-      const std::vector<double> &wall = lv == 1 ? h->wall_lo : h->wall_hi;
+      const size_t npl = (size_t)nx * ny;
+      std::vector<double> wv(npl * 3), wd(npl);
+      wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
       const int kw = lv == 1 ? 0 : g.zdf - 1;
-      for (size_t c = 0; c < (size_t)nx * ny; c++) {
-        const double *f = wall.data() + c * 19;
-        double ux = 0., uy = 0., uz = 0., dens = 0.;
-        for (int a = 0; a < 19; a++) {
-          ux += EX[a] * f[a];
-          uy += EY[a] * f[a];
-          uz += EZ[a] * f[a];
-          dens += f[a];
-        }
-        if (dens > 0.) {
-          ux /= dens;
-          uy /= dens;
-          uz /= dens;
-        } else {
-          ux = uy = uz = dens = 0.;
-        }
+      for (size_t c = 0; c < npl; c++) {
         const size_t o = c * nz + kw;
-        vel[o * 3] = ux;
-        vel[o * 3 + 1] = uy;
-        vel[o * 3 + 2] = uz;
-        den[o] = dens;
+        std::memcpy(&vel[o * 3], &wv[c * 3], 3 * 8);
+        den[o] = wd[c];
       }
     }
     char base[16];
@@ -820,6 +830,142 @@ extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
   }
   cudaFree(dvel);
   cudaFree(dden);
+  return rc;
+}
+
+// ---------------------------------------------------------------- statistics / budget
+// The fields of the three levels as device arrays in the file layout (the
+// wall planes from the host copies); dvel[l] / dden[l] sized by the caller.
+static int fields_on_device(dns_handle *h, double *const dvel[3], double *const dden[3]) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  for (int lv = 0; lv < 3; lv++) {
+    const int nx = lv == 0 ? g.nx : g.nxf, ny = lv == 0 ? g.ny : g.nyf, nz = lv == 0 ? g.nzc : g.zdf;
+    const int P = lv == 0 ? g.nzc : 2 * zds, p0 = lv == 2 ? zds : 0, np = lv == 0 ? g.nzc : zds;
+    const int k0 = lv == 1 ? 1 : 0;
+    if (is_f32(h))
+      launch_fields_f32(F(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f]), dvel[lv], dden[lv], nx, ny, P, p0, np, nz,
+                        k0, h->stream);
+    else
+      launch_fields_f64(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f], dvel[lv], dden[lv], nx, ny, P, p0, np, nz, k0,
+                        h->stream);
+    CUDA_TRY(cudaGetLastError());
+    if (lv > 0) {
+      const size_t npl = (size_t)nx * ny;
+      std::vector<double> wv(npl * 3), wd(npl);
+      wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
+      const int kw = lv == 1 ? 0 : g.zdf - 1;
+      CUDA_TRY(cudaMemcpy2DAsync(dvel[lv] + (size_t)kw * 3, (size_t)nz * 3 * 8, wv.data(), 3 * 8, 3 * 8, npl,
+                                 cudaMemcpyHostToDevice, h->stream));
+      CUDA_TRY(cudaMemcpy2DAsync(dden[lv] + kw, (size_t)nz * 8, wd.data(), 8, 8, npl, cudaMemcpyHostToDevice,
+                                 h->stream));
+      CUDA_TRY(cudaStreamSynchronize(h->stream));  // wv / wd go out of scope
+    }
+  }
+  return DNS_OK;
+}
+
+static size_t level_nodes(const dns_geometry &g, int lv) {
+  return lv == 0 ? (size_t)g.nx * g.ny * g.nzc : (size_t)g.nxf * g.nyf * g.zdf;
+}
+
+extern "C" int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *vfl) {
+  if (!h || !prof) return fail(DNS_EINVAL, "bad argument");
+  int rc = tke_validate(h->p);
+  if (rc) return rc;
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  const dns_geometry &g = h->g;
+  size_t tot = 0;
+  for (int l = 0; l < 3; l++) tot += level_nodes(g, l) * 4;
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, tot * 8) != cudaSuccess) return fail(DNS_ENOMEM, "field buffers for the budget");
+  double *vel[3], *den[3], *o = buf;
+  for (int l = 0; l < 3; l++) {
+    vel[l] = o;
+    den[l] = o + level_nodes(g, l) * 3;
+    o += level_nodes(g, l) * 4;
+  }
+  rc = fields_on_device(h, vel, den);
+  if (rc == DNS_OK) {
+    const double *cv[3] = {vel[0], vel[1], vel[2]}, *cd[3] = {den[0], den[1], den[2]};
+    rc = tke_budget_device(h->p, g, cv, cd, prof, ufl, vfl, h->stream);
+  }
+  cudaFree(buf);
+  return rc;
+}
+
+// reading.c:14-226: vel-* / den-* of the three levels (the first xdv (or
+// GR xdv) x-planes; the reference reads its x-halo planes from the same files)
+extern "C" int dns_tke_budget_files(const dns_params *p, const char *dir, int cntr, double *prof, double *ufl,
+                                    double *vfl) {
+  if (!p || !dir || !prof) return fail(DNS_EINVAL, "bad argument");
+  dns_geometry g;
+  int rc = dns_geometry_of(p, &g);
+  if (rc) return rc;
+  if ((rc = tke_validate(*p))) return rc;
+  CUDA_TRY(cudaSetDevice(p->device));
+  size_t tot = 0;
+  for (int l = 0; l < 3; l++) tot += level_nodes(g, l) * 4;
+  std::vector<double> host(tot);
+  const char *names[3] = {"c", "slf", "suf"};
+  double *hv[3], *hd[3], *o = host.data();
+  for (int l = 0; l < 3 && rc == DNS_OK; l++) {
+    hv[l] = o;
+    hd[l] = o + level_nodes(g, l) * 3;
+    o += level_nodes(g, l) * 4;
+    char base[16];
+    std::snprintf(base, sizeof base, "vel-%s", names[l]);
+    rc = read_file(cname(dir, base, cntr), hv[l], level_nodes(g, l) * 3);
+    if (rc == DNS_OK) {
+      std::snprintf(base, sizeof base, "den-%s", names[l]);
+      rc = read_file(cname(dir, base, cntr), hd[l], level_nodes(g, l));
+    }
+  }
+  if (rc) return rc;
+  cudaStream_t st;
+  CUDA_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, tot * 8) != cudaSuccess) {
+    cudaStreamDestroy(st);
+    return fail(DNS_ENOMEM, "field buffers for the budget");
+  }
+  cudaError_t e = cudaMemcpyAsync(buf, host.data(), tot * 8, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) {
+    const double *cv[3], *cd[3];
+    for (int l = 0; l < 3; l++) {
+      cv[l] = buf + (hv[l] - host.data());
+      cd[l] = buf + (hd[l] - host.data());
+    }
+    rc = tke_budget_device(*p, g, cv, cd, prof, ufl, vfl, st);
+  } else {
+    rc = fail(DNS_ECUDA, cudaGetErrorString(e));
+  }
+  cudaStreamSynchronize(st);
+  cudaFree(buf);
+  cudaStreamDestroy(st);
+  return rc;
+}
+
+extern "C" int dns_write_tke_budget(const dns_params *p, const char *dir, int cntr, const double *prof,
+                                    const double *ufl, const double *vfl) {
+  if (!p || !dir || !prof) return fail(DNS_EINVAL, "bad argument");
+  dns_geometry g;
+  int rc = dns_geometry_of(p, &g);
+  if (rc) return rc;
+  const size_t NZ = g.nz_profile;
+  // budget2D.c:1553 / :1583 / :1590: name.RANK.TTTT, rank 000
+  const char *names[3] = {"turb-fld-2d", "vort-fluc-2d", "KE-Budget-2d"};
+  const int rows[3] = {19, 3, 30};
+  const double *src = prof;
+  for (int f = 0; f < 3 && rc == DNS_OK; f++) {
+    char base[32];
+    std::snprintf(base, sizeof base, "%s.000", names[f]);
+    rc = write_file(cname(dir, base, cntr), src, rows[f] * NZ, 1);
+    src += rows[f] * NZ;
+  }
+  const size_t npl = (size_t)g.nxf * g.nyf;
+  if (rc == DNS_OK && ufl) rc = write_file(cname(dir, "ufl4", cntr), ufl, npl, 1);
+  if (rc == DNS_OK && vfl) rc = write_file(cname(dir, "vfl4", cntr), vfl, npl, 1);
   return rc;
 }
 

@@ -7,6 +7,8 @@
 
 #include <cuda_runtime.h>
 
+#include "../../include/dns_embed.h"
+
 namespace dns {
 
 // Device-side scalar state carried between steps (one instance per handle).
@@ -120,6 +122,13 @@ struct UniformMap {
   double fac;                // (dxr / dx_level) (omega / omega_level), the f^neq rescaling
 };
 void launch_uniform_interp_f64(const double *uni, const UniformMap &m, double *out, int *bad, cudaStream_t stream);
+// Turbulence statistics / kinetic-energy budget of one snapshot (tke.cu) from
+// the device field arrays of the three levels in the reference file layout
+// (0 coarse vel[i][j][k][3] / den[i][j][k], 1 lower fine, 2 upper fine);
+// prof on the host, [DNS_TKE_NPROF][nz_profile]; ufl / vfl optional.
+int tke_validate(const dns_params &p);
+int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *const vel[3],
+                      const double *const den[3], double *prof, double *ufl, double *vfl, cudaStream_t st);
 // layout transposes between the device SoA state and the reference AoS order
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);

@@ -142,6 +142,30 @@ int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double amp);
    uniform grid too short for the channel); DNS_EIO when the file is missing or
    shorter than one lattice. */
 int dns_load_uniform(dns_handle *h, const char *dir, int cntr);
+/* ---- turbulence statistics and kinetic-energy budget ----------------------
+   The reference's offline program TKE-budget/computations (budget-no-slip-mgrd.c
+   loop body :95-105: budget2D.c:13-1736, uv_fluc.c:15-49) on the device, for one
+   snapshot.  prof receives DNS_TKE_NPROF profiles of NZ = 2 zdf + zdc - 4 points
+   (dns_geometry.nz_profile), in the order of the three files the reference
+   writes: turb-fld-2d (UAVG VAVG WAVG UTIN VTIN WTIN uw DAVG DTIN SKEWu SKEWv
+   SKEWw SKEWuw SKEWp KURTu KURTv KURTw KURTuw KURTp), vort-fluc-2d (wx wy wz),
+   KE-Budget-2d (Pii Puu Pvv Pww Puw Tiir Tuur Tvvr Twwr Tuwr Tiipai Tuupai
+   Tvvpai Twwpai Tuwpai Paiuu Paivv Paiww Paiuw Tiis Tuus Tvvs Twws Tuws Epii
+   Epuu Epvv Epww Epuw KE).  ufl / vfl (may be NULL) receive the u / v
+   fluctuations of the lower fine plane k = 4, [GR xdv][GR ydv] (uv_fluc's
+   ufl4 / vfl4).  Needs zds >= 5, zdv >= 7, xdv and ydv >= 4 (DNS_EINVAL). */
+#define DNS_TKE_NPROF 52
+/* from the handle's current state (the fields vel_print would write) */
+int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *vfl);
+/* from vel-c/slf/suf.cntr and den-c/slf/suf.cntr in dir (reading.c:14-226);
+   runs on GPU p->device */
+int dns_tke_budget_files(const dns_params *p, const char *dir, int cntr, double *prof, double *ufl, double *vfl);
+/* turb-fld-2d.000.cntr, vort-fluc-2d.000.cntr, KE-Budget-2d.000.cntr and, when
+   ufl / vfl are given, ufl4.cntr / vfl4.cntr (budget2D.c:1553-1641,
+   uv_fluc.c:35-46), native doubles */
+int dns_write_tke_budget(const dns_params *p, const char *dir, int cntr, const double *prof, const double *ufl,
+                         const double *vfl);
+
 /* Post-stream state S in reference AoS order f[i][j][k][a] of the global domain:
    level 0 coarse (xdv, ydv, zdc, 19), 1 lower fine, 2 upper fine
    ((GR xdv), (GR ydv), zdf, 19).  out must hold that many doubles. */

@@ -7,7 +7,13 @@ reference tree, into ``oracle/_ref/<config>/``:
   main program, plus ``oracle/ref_harness.c`` (drives the routines in the main
   loop's order) and the single-rank MPI shim;
 * ``ref_main`` (configurations that ask for it) — the unmodified main program
-  ``dns-q-mgrd-all-patterns-xyc.c`` with the same routines and the shim.
+  ``dns-q-mgrd-all-patterns-xyc.c`` with the same routines and the shim;
+* ``tke_budget`` (configurations with ``tke``) — the unmodified turbulence
+  statistics / kinetic-energy budget program of ``TKE-budget/computations/``
+  (``budget-no-slip-mgrd.c`` with ``reading.c``, ``budget2D.c``, ``uv_fluc.c``
+  ...), configured through its own ``definitions.h`` with the same grid and
+  ``TSTR = TEND`` = the configuration's ``TSTR``; it reads ``../vel-*.TTTT`` /
+  ``../den-*.TTTT`` relative to its working directory.
 
 The reference has no build system beyond a two-line Makefile (``mpicc -O3``).
 It configures itself only through compile-time macros in ``src/definitions.h``
@@ -37,6 +43,9 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 REF_SRC = Path("/root/reference/DNS-solver-with-grid-embedding/src")
+TKE_SRC = Path("/root/reference/TKE-budget/computations")
+# macros of TKE-budget/computations/definitions.h:21-47 taken from the configuration
+TKE_MACROS = ("zdv", "ydv", "xdv", "CFL", "Rebs", "ub", "gratio", "zds", "TSTR", "TEND", "DT")
 OUT = HERE / "_ref"
 SHIM = HERE / "mpi_shim"
 MAIN_FILE = "dns-q-mgrd-all-patterns-xyc.c"
@@ -83,6 +92,24 @@ def render_definitions(cfg: dict) -> str:
     return "\n".join(out) + "\n"
 
 
+def render_tke_definitions(cfg: dict) -> str:
+    vals = {k: cfg[k] for k in TKE_MACROS if k in cfg}
+    vals["TEND"] = vals["TSTR"] = cfg["TSTR"]
+    vals["DT"] = 1
+    out, seen = [], set()
+    for line in (TKE_SRC / "definitions.h").read_text().splitlines():
+        m = re.match(r"^\s*#define\s+(\w+)\b(.*)$", line)
+        if m and m.group(1) in vals:
+            out.append(f"#define {m.group(1)} {vals[m.group(1)]}")
+            seen.add(m.group(1))
+            continue
+        out.append(line)
+    missing = [k for k in vals if k not in seen]
+    if missing:
+        raise RuntimeError(f"macros not found in the TKE-budget definitions.h: {missing}")
+    return "\n".join(out) + "\n"
+
+
 def _cc(args, cwd):
     r = subprocess.run(args, cwd=cwd, capture_output=True, text=True)
     if r.returncode != 0:
@@ -118,7 +145,28 @@ def build_config(name: str) -> Path:
     for p in d.iterdir():
         if p.name not in ("ref_harness", "ref_main"):
             p.unlink()
+    if cfg.get("tke"):
+        build_tke(cfg, d)
     return d
+
+
+def build_tke(cfg: dict, d: Path) -> Path:
+    """TKE-budget/computations compiled unmodified into d/tke_budget."""
+    t = d / "tke_src"
+    t.mkdir()
+    (t / "definitions.h").write_text(render_tke_definitions(cfg))
+    sources = sorted(p.name for p in TKE_SRC.glob("*.c"))
+    for s in sources + ["fun_defs.h"]:
+        os.symlink(TKE_SRC / s, t / s)
+    cflags = ["gcc", "-O3", "-ffp-contract=off", "-w", f"-I{t}", f"-I{SHIM}"]
+    objs = []
+    for s in sources + [str(SHIM / "mpi_shim.c")]:
+        o = t / (Path(s).name[:-2] + ".o")
+        _cc(cflags + ["-c", str(t / s) if "/" not in s else s, "-o", str(o)], t)
+        objs.append(str(o))
+    _cc(["gcc", "-o", str(d / "tke_budget")] + objs + ["-lm"], t)
+    shutil.rmtree(t)
+    return d / "tke_budget"
 
 
 def main(names):

@@ -107,6 +107,7 @@ int MPI_Request_free(MPI_Request *req);
 int MPI_Sendrecv(const void *sbuf, int scount, MPI_Datatype stype, int dest, int stag,
                  void *rbuf, int rcount, MPI_Datatype rtype, int source, int rtag,
                  MPI_Comm comm, MPI_Status *st);
+int MPI_Reduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op, int root, MPI_Comm comm);
 int MPI_Allreduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op,
                   MPI_Comm comm);
 int MPI_Bcast(void *buf, int count, MPI_Datatype t, int root, MPI_Comm comm);
@@ -120,6 +121,8 @@ int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI
 int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype etype,
                       MPI_Datatype filetype, const char *rep, MPI_Info info);
 int MPI_File_read_all(MPI_File fh, void *buf, int count, MPI_Datatype t, MPI_Status *st);
+int MPI_File_read(MPI_File fh, void *buf, int count, MPI_Datatype t, MPI_Status *st);
+int MPI_File_read_at_all(MPI_File fh, MPI_Offset offset, void *buf, int count, MPI_Datatype t, MPI_Status *st);
 int MPI_File_write_all(MPI_File fh, const void *buf, int count, MPI_Datatype t,
                        MPI_Status *st);
 int MPI_File_close(MPI_File *fh);

@@ -320,6 +320,11 @@ int MPI_Sendrecv(const void *sbuf, int scount, MPI_Datatype stype, int dest, int
   return MPI_SUCCESS;
 }
 
+int MPI_Reduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op, int root, MPI_Comm comm) {
+  (void)op; (void)root; (void)comm;
+  memmove(rbuf, sbuf, (size_t)count * t->size);
+  return MPI_SUCCESS;
+}
 int MPI_Allreduce(const void *sbuf, void *rbuf, int count, MPI_Datatype t, MPI_Op op, MPI_Comm comm) {
   (void)op; (void)comm;
   memmove(rbuf, sbuf, (size_t)count * t->size);
@@ -342,7 +347,8 @@ int MPI_Info_free(MPI_Info *info) { *info = 0; return MPI_SUCCESS; }
 struct shim_file {
   FILE *fp;
   MPI_Offset disp;
-  MPI_Datatype filetype;
+  MPI_Datatype etype, filetype;
+  size_t pos; /* individual file pointer: bytes of the view's data stream consumed */
 };
 
 int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI_File *fh) {
@@ -361,27 +367,39 @@ int MPI_File_open(MPI_Comm comm, const char *name, int amode, MPI_Info info, MPI
   struct shim_file *f = (struct shim_file *)calloc(1, sizeof(*f));
   f->fp = fp;
   f->disp = 0;
+  f->etype = MPI_CHAR;
   f->filetype = MPI_CHAR;
+  f->pos = 0;
   *fh = f;
   return MPI_SUCCESS;
 }
 int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype etype, MPI_Datatype filetype,
                       const char *rep, MPI_Info info) {
-  (void)etype; (void)rep; (void)info;
+  (void)rep; (void)info;
   fh->disp = disp;
+  fh->etype = etype;
   fh->filetype = filetype;
+  fh->pos = 0;
   return MPI_SUCCESS;
 }
 
-/* walk the data stream through the tiled filetype, calling io() per segment */
-static int file_stream(MPI_File fh, char *data, size_t bytes, int writing) {
+/* walk the data stream through the tiled filetype from stream byte `start`,
+   reading or writing `bytes` */
+static int file_stream_at(MPI_File fh, char *data, size_t bytes, int writing, size_t start) {
   seglist s = type_segments(fh->filetype);
-  size_t done = 0;
+  size_t done = 0, skip = start;
   for (size_t tile = 0; done < bytes; tile++) {
     for (size_t i = 0; i < s.n && done < bytes; i++) {
-      size_t len = s.v[i].len;
+      size_t seg_off = s.v[i].off, len = s.v[i].len;
+      if (skip >= len) {
+        skip -= len;
+        continue;
+      }
+      seg_off += skip;
+      len -= skip;
+      skip = 0;
       if (len > bytes - done) len = bytes - done;
-      long long off = fh->disp + (long long)(tile * fh->filetype->extent + s.v[i].off);
+      long long off = fh->disp + (long long)(tile * fh->filetype->extent + seg_off);
       if (fseeko(fh->fp, (off_t)off, SEEK_SET) != 0) { free(s.v); return -1; }
       size_t got = writing ? fwrite(data + done, 1, len, fh->fp) : fread(data + done, 1, len, fh->fp);
       if (got != len) { free(s.v); return -1; }
@@ -391,6 +409,32 @@ static int file_stream(MPI_File fh, char *data, size_t bytes, int writing) {
   }
   free(s.v);
   return 0;
+}
+static int file_stream(MPI_File fh, char *data, size_t bytes, int writing) {
+  return file_stream_at(fh, data, bytes, writing, 0);
+}
+
+/* independent read at the individual file pointer, which it advances */
+int MPI_File_read(MPI_File fh, void *buf, int count, MPI_Datatype t, MPI_Status *st) {
+  size_t bytes = (size_t)count * t->size;
+  char *tmp = (char *)malloc(bytes ? bytes : 1);
+  if (file_stream_at(fh, tmp, bytes, 0, fh->pos) != 0) shim_die("short read in MPI_File_read");
+  fh->pos += bytes;
+  unpack(tmp, buf, count, t);
+  free(tmp);
+  if (st) st->count_bytes = (long long)bytes;
+  return MPI_SUCCESS;
+}
+/* collective read at an explicit offset in etype units of the view */
+int MPI_File_read_at_all(MPI_File fh, MPI_Offset offset, void *buf, int count, MPI_Datatype t, MPI_Status *st) {
+  size_t bytes = (size_t)count * t->size;
+  char *tmp = (char *)malloc(bytes ? bytes : 1);
+  if (file_stream_at(fh, tmp, bytes, 0, (size_t)offset * fh->etype->size) != 0)
+    shim_die("short read in MPI_File_read_at_all");
+  unpack(tmp, buf, count, t);
+  free(tmp);
+  if (st) st->count_bytes = (long long)bytes;
+  return MPI_SUCCESS;
 }
 
 int MPI_File_read_all(MPI_File fh, void *buf, int count, MPI_Datatype t, MPI_Status *st) {

@@ -15,6 +15,9 @@ Names:
        zds = 16, with streamwise ridges (pitch 48, gas fraction 0.5) or square
        posts (pitch 32, gas fraction 0.75).
 
+``tke``: also build the reference's turbulence-statistics / kinetic-energy
+budget program (TKE-budget/computations) for that grid.
+
 Reynolds numbers: for c1 the bulk Reynolds number is chosen so that the fine
 relaxation time is 0.52 (Reb = 150 ub H, H = NZs - 2 fine cells); c2/c3 use
 Dean's correlation Re_tau = 0.0955 Re_b^(7/8) (Re_b on the full height) for
@@ -43,15 +46,15 @@ REF_CONFIGS = {
     "t_ridges": _tiny(pattern="RSLIP", main=True, xdu=12, ydu=12, zdu=11),
     "t_posts": _tiny(pattern="PSLIP"),
     "t_span": _tiny(pattern="SSLIP"),
-    "t_gr4": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8),
+    "t_gr4": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8, tke=True),
     # the filtered fine-to-coarse transfer (FLTR), defined by the reference for
     # GR = 4 (its stencil array holds GR + 1 = 5 planes)
     "t_gr4f": _tiny(xdv=8, ydv=4, zdv=7, zds=8, gratio=4, pattern="PSLIP", gxplussize=8, wxplussize=8, fltr=True,
                     main=True),
-    "t_odd": _tiny(xdv=12, ydv=6, zdv=9, zds=6, pattern="RSLIP", gyplussize=6, wyplussize=6),
+    "t_odd": _tiny(xdv=12, ydv=6, zdv=9, zds=6, pattern="RSLIP", gyplussize=6, wyplussize=6, tke=True),
     "c1": dict(Rebs=repr(150.0 * UB * _h(27, 8, 2)), ub=UB, zdv=27, ydv=64, xdv=64, TSTR=0, TEND=1,
                CFL=0.1, gratio=2, zds=8, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4,
-               XDIM=1, YDIM=1),
+               XDIM=1, YDIM=1, tke=True),
     "c2": dict(Rebs=5533.0, ub=UB, zdv=83, ydv=128, xdv=256, TSTR=0, TEND=1, CFL=0.1, gratio=2,
                zds=16, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4, XDIM=1, YDIM=1),
     "c3r": dict(Rebs=13585.0, ub=UB, zdv=115, ydv=192, xdv=384, TSTR=0, TEND=1, CFL=0.1, gratio=2,

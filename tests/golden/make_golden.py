@@ -7,7 +7,9 @@ SHA-256 digests of the post-stream lattices and interface histories it writes,
 plus a few sampled values and the logged flow rate.  The tests check the CPU
 restatement against these digests on machines where the reference tree is not
 mounted.  A second file, ``uniform_golden.json``, holds the same digests for
-mode -i starts of the unmodified reference main from a uniform-grid file.
+mode -i starts of the unmodified reference main from a uniform-grid file, and
+``tke_golden.json`` the output profiles of the reference's offline budget
+program (TKE-budget/computations) on the fields of a seeded state.
 
 Run from the repository root: ``python tests/golden/make_golden.py``.
 """
@@ -102,6 +104,35 @@ def run_uniform_case(name, seed_first, seed_second):
     return out
 
 
+# the reference's offline budget program (oracle/_ref/<config>/tke_budget) on
+# the fields of a seeded state after a few constant-force coarse steps, written
+# by the reference's own vel_print through the harness
+TKE_CASES = [("t_odd", 6), ("t_gr4", 4)]
+
+
+def run_tke_case(name, steps):
+    m = REF_CONFIGS[name]
+    cntr = int(m["TSTR"])
+    p = port.Port(m)
+    p.init_seeded(42, UC, AMP, GCONST)
+    p.set_forcing(False, GCONST)
+    with tempfile.TemporaryDirectory() as d:
+        din, dout = Path(d, "in"), Path(d, "out")
+        din.mkdir()
+        (dout / "tke").mkdir(parents=True)
+        p.save(din, cntr - 1)
+        exe = ROOT / "oracle" / "_ref" / name / "ref_harness"
+        subprocess.run([str(exe), str(din), str(cntr - 1), str(dout), str(cntr), str(steps), "const",
+                        GCONST.hex(), "0", "1"], check=True, capture_output=True)
+        subprocess.run([str(ROOT / "oracle" / "_ref" / name / "tke_budget")], cwd=dout / "tke", check=True,
+                       capture_output=True)
+        nz = 2 * (int(m["zds"]) + 1) + int(m["zdv"]) - 4
+        prof = []
+        for fn in ("turb-fld-2d", "vort-fluc-2d", "KE-Budget-2d"):
+            prof.extend(np.fromfile(dout / "tke" / f"{fn}.000.{cntr:04d}").reshape(-1, nz).tolist())
+    return {"config": name, "seed": SEED, "uc": UC, "amp": AMP, "g": GCONST, "steps": steps, "profiles": prof}
+
+
 def main():
     cases = [run_case(*c) for c in CASES]
     (Path(__file__).parent / "oracle_golden.json").write_text(json.dumps(cases, indent=1))
@@ -109,6 +140,9 @@ def main():
     uni = [run_uniform_case(*c) for c in UNIFORM_CASES]
     (Path(__file__).parent / "uniform_golden.json").write_text(json.dumps(uni, indent=1))
     print(f"wrote {len(uni)} uniform-start cases")
+    tke = [run_tke_case(*c) for c in TKE_CASES]
+    (Path(__file__).parent / "tke_golden.json").write_text(json.dumps(tke))
+    print(f"wrote {len(tke)} budget cases")
 
 
 if __name__ == "__main__":

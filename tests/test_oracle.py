@@ -317,3 +317,22 @@ def test_port_uniform_start_rejects_short_grid(port, ref_configs):
     with pytest.raises(ValueError):
         p.init_uniform(port.uniform_state(12, 4, 11, 1))
     p.init_uniform(port.uniform_state(12, 12, 5, 1))   # a coarser wall-normal grid is fine
+
+
+# ------------------------------------------------------------ budget program
+TKE_GOLDEN = json.loads((ROOT / "tests" / "golden" / "tke_golden.json").read_text())
+
+
+@pytest.mark.parametrize("case", TKE_GOLDEN, ids=lambda c: c["config"])
+def test_reference_budget_program_reproduces_golden(case):
+    """The compiled reference budget program (TKE-budget/computations under the
+    single-rank shim) reproduces its stored output bit for bit."""
+    if ref_binary(case["config"], "tke_budget") is None or ref_binary(case["config"]) is None:
+        pytest.skip("compiled reference not available")
+    import sys
+
+    sys.path.insert(0, str(ROOT / "tests" / "golden"))
+    import make_golden
+
+    again = make_golden.run_tke_case(case["config"], case["steps"])
+    assert np.array_equal(np.array(again["profiles"]), np.array(case["profiles"]))
