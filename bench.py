@@ -22,6 +22,11 @@ second with step budgets of 1000-10000, admitted against a 150 GB budget:
 p50/p99 latency and aggregate MLUPS, against the same requests served one at a
 time by the FP64 form).
 
+A ``budget`` object times the turbulence statistics / kinetic-energy budget of
+the final state (the reference's offline TKE-budget program) on the device,
+from the live state and from field files, beside the reference program itself
+on one host core reading the same files.
+
 N > 1 runs under torchrun: every rank advances its own independent channel
 (replicas, weak scaling); the reported value is the whole job's updates over
 the slowest rank's device time.  ``--impl reference`` times the reference's own
@@ -340,6 +345,51 @@ def bench_served(pkg, torch, args, peak, fp64_cache):
 PKG = "dns-solvers-with-grid-embedding_b200"
 
 
+def bench_budget(pkg, ch, p, config: str):
+    """The turbulence statistics / kinetic-energy budget of one snapshot of the
+    channel's current state: on the device from the live state and from the
+    field files, and the reference's own offline program (TKE-budget/
+    computations, compiled under the single-rank shim) on the same files on
+    one host core.  Wall-clock seconds of whole calls (file reads included
+    where files are read); the largest profile deviation from the reference's
+    output, relative to each profile's magnitude."""
+    import numpy as np
+
+    cntr = int(CONFIGS[config][0].get("TSTR", 0))
+    g = pkg.geometry(p)
+    out = {"workload": f"{config} fields ({g.nx}x{g.ny}x{g.nzc} coarse, 2 x {g.nxf}x{g.nyf}x{g.zdf} fine)",
+           "profiles": len(pkg.TKE_NAMES), "nz": g.nz_profile}
+    ch.tke_budget()
+    t0 = time.perf_counter()
+    reps = 3
+    for _ in range(reps):
+        prof = ch.tke_budget()
+    out["gpu_ms_live"] = 1e3 * (time.perf_counter() - t0) / reps
+    with tempfile.TemporaryDirectory() as d:
+        d = Path(d)
+        ch.write_fields(d, cntr)
+        pkg.tke_budget_files(p, d, cntr)
+        t0 = time.perf_counter()
+        files = pkg.tke_budget_files(p, d, cntr)
+        out["gpu_ms_files"] = 1e3 * (time.perf_counter() - t0)
+        exe = ROOT / "oracle" / "_ref" / config / "tke_budget"
+        if exe.exists():
+            (d / "tke").mkdir()
+            t0 = time.perf_counter()
+            subprocess.run([str(exe)], cwd=d / "tke", check=True, capture_output=True)
+            secs = time.perf_counter() - t0
+            ref = np.concatenate([np.fromfile(d / "tke" / f"{n}.000.{cntr:04d}").reshape(k, -1)
+                                  for n, k in pkg.TKE_FILES])
+            scale = np.maximum(np.max(np.abs(ref), axis=1, keepdims=True), 1e-300)
+            out["cpu_baseline"] = {"value": 1e3 * secs, "unit": "ms", "cores": 1, "kind": "reference",
+                                   "sample": "one snapshot, reading the same files"}
+            out["speedup_files_vs_cpu"] = 1e3 * secs / out["gpu_ms_files"]
+            dev = np.maximum(np.max(np.abs(prof - ref) / scale, axis=1), np.max(np.abs(files - ref) / scale, axis=1))
+            out["max_rel_dev_vs_reference"] = float(np.max(dev))
+            out["worst_profile"] = pkg.TKE_NAMES[int(np.argmax(dev))]
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import numpy as np
     import torch
@@ -463,6 +513,8 @@ def run_ours(args, rank, world, local_rank):
         "clocks": clk.summary(),
         "log_tail": {"force": float(log[-1, 1]), "flowrate": float(log[-1, 4]), "stress": float(log[-1, 7])},
     }
+    if world == 1 and not args.no_budget:
+        line["budget"] = bench_budget(pkg, ch, p, args.config)
     # ---- the FP32 deviation-storage form on the same workload (same GPU), run
     # by the batched engine as a batch of one
     fp64_cache = {}
@@ -517,6 +569,7 @@ def main():
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
+    ap.add_argument("--no-budget", action="store_true")
     ap.add_argument("--c4-instances", type=int, default=96)
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--c5-requests", type=int, default=16)

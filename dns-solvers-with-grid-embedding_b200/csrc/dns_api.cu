@@ -70,6 +70,8 @@ struct dns_handle {
   DevLog *hlog = nullptr;              // pinned mirror
   double *stats_acc = nullptr;         // [nz_profile][16]
   double *iface_mac = nullptr;         // FP64: interface rho, u [2][4][nyf][nxf]; FP32: corner data
+  void *tke_ws = nullptr;              // statistics / budget work space (allocated on first use)
+  size_t tke_ws_bytes = 0;
   unsigned int *fin_counter = nullptr; // finalize's block counter
   cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
   cudaStream_t hip = nullptr;          // interface transfers (highest priority)
@@ -290,6 +292,7 @@ extern "C" void dns_destroy(dns_handle *h) {
   cudaFree(h->dlog);
   cudaFree(h->stats_acc);
   cudaFree(h->iface_mac);
+  cudaFree(h->tke_ws);
   cudaFree(h->fin_counter);
   if (h->hlog) cudaFreeHost(h->hlog);
   for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
@@ -834,9 +837,14 @@ extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
 }
 
 // ---------------------------------------------------------------- statistics / budget
-// The fields of the three levels as device arrays in the file layout (the
-// wall planes from the host copies); dvel[l] / dden[l] sized by the caller.
-static int fields_on_device(dns_handle *h, double *const dvel[3], double *const dden[3]) {
+static size_t level_nodes(const dns_geometry &g, int lv) {
+  return lv == 0 ? (size_t)g.nx * g.ny * g.nzc : (size_t)g.nxf * g.nyf * g.zdf;
+}
+
+// The fields of the current state as planar device arrays q[l] = [4][nz][ny][nx]
+// (u, v, w, den / 3; the moments vel_print writes), the wall planes from the
+// host copies.
+static int fields_planar(dns_handle *h, double *const q[3]) {
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
   for (int lv = 0; lv < 3; lv++) {
@@ -844,29 +852,34 @@ static int fields_on_device(dns_handle *h, double *const dvel[3], double *const 
     const int P = lv == 0 ? g.nzc : 2 * zds, p0 = lv == 2 ? zds : 0, np = lv == 0 ? g.nzc : zds;
     const int k0 = lv == 1 ? 1 : 0;
     if (is_f32(h))
-      launch_fields_f32(F(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f]), dvel[lv], dden[lv], nx, ny, P, p0, np, nz,
-                        k0, h->stream);
+      launch_fields_planar_f32(F(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f]), q[lv], nx, ny, P, p0, np, nz, k0,
+                               h->stream);
     else
-      launch_fields_f64(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f], dvel[lv], dden[lv], nx, ny, P, p0, np, nz, k0,
-                        h->stream);
+      launch_fields_planar_f64(lv == 0 ? h->fc[h->cur_c] : h->ff[h->cur_f], q[lv], nx, ny, P, p0, np, nz, k0,
+                               h->stream);
     CUDA_TRY(cudaGetLastError());
-    if (lv > 0) {
-      const size_t npl = (size_t)nx * ny;
-      std::vector<double> wv(npl * 3), wd(npl);
-      wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
-      const int kw = lv == 1 ? 0 : g.zdf - 1;
-      CUDA_TRY(cudaMemcpy2DAsync(dvel[lv] + (size_t)kw * 3, (size_t)nz * 3 * 8, wv.data(), 3 * 8, 3 * 8, npl,
-                                 cudaMemcpyHostToDevice, h->stream));
-      CUDA_TRY(cudaMemcpy2DAsync(dden[lv] + kw, (size_t)nz * 8, wd.data(), 8, 8, npl, cudaMemcpyHostToDevice,
-                                 h->stream));
-      CUDA_TRY(cudaStreamSynchronize(h->stream));  // wv / wd go out of scope
-    }
   }
+  // wall planes: lower k = 0, upper k = zdf - 1, [c][j][i] per plane
+  const size_t npl = (size_t)g.nxf * g.nyf, lvl = level_nodes(g, 1);
+  std::vector<double> wv(npl * 3), wd(npl), planes(2 * 4 * npl);
+  for (int lv = 1; lv < 3; lv++) {
+    wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
+    double *o = planes.data() + (size_t)(lv - 1) * 4 * npl;
+    for (int i = 0; i < g.nxf; i++)
+      for (int j = 0; j < g.nyf; j++) {
+        const size_t c = (size_t)i * g.nyf + j, t = (size_t)j * g.nxf + i;
+        o[t] = wv[c * 3];
+        o[npl + t] = wv[c * 3 + 1];
+        o[2 * npl + t] = wv[c * 3 + 2];
+        o[3 * npl + t] = (1. / 3.) * wd[c];
+      }
+    const int kw = lv == 1 ? 0 : g.zdf - 1;
+    for (int c = 0; c < 4; c++)
+      CUDA_TRY(cudaMemcpyAsync(q[lv] + c * lvl + (size_t)kw * npl, o + c * npl, npl * 8, cudaMemcpyHostToDevice,
+                               h->stream));
+  }
+  CUDA_TRY(cudaStreamSynchronize(h->stream));  // planes goes out of scope
   return DNS_OK;
-}
-
-static size_t level_nodes(const dns_geometry &g, int lv) {
-  return lv == 0 ? (size_t)g.nx * g.ny * g.nzc : (size_t)g.nxf * g.nyf * g.zdf;
 }
 
 extern "C" int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *vfl) {
@@ -877,20 +890,25 @@ extern "C" int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *
   const dns_geometry &g = h->g;
   size_t tot = 0;
   for (int l = 0; l < 3; l++) tot += level_nodes(g, l) * 4;
-  double *buf = nullptr;
-  if (cudaMalloc(&buf, tot * 8) != cudaSuccess) return fail(DNS_ENOMEM, "field buffers for the budget");
-  double *vel[3], *den[3], *o = buf;
+  // planar fields and the budget's work space stay allocated for later calls
+  const size_t need = tot * 8 + tke_workspace_bytes(g);
+  if (h->tke_ws_bytes < need) {
+    cudaFree(h->tke_ws);
+    h->tke_ws = nullptr;
+    h->tke_ws_bytes = 0;
+    if (cudaMalloc(&h->tke_ws, need) != cudaSuccess) return fail(DNS_ENOMEM, "field buffers for the budget");
+    h->tke_ws_bytes = need;
+  }
+  double *q[3], *o = static_cast<double *>(h->tke_ws);
   for (int l = 0; l < 3; l++) {
-    vel[l] = o;
-    den[l] = o + level_nodes(g, l) * 3;
+    q[l] = o;
     o += level_nodes(g, l) * 4;
   }
-  rc = fields_on_device(h, vel, den);
+  rc = fields_planar(h, q);
   if (rc == DNS_OK) {
-    const double *cv[3] = {vel[0], vel[1], vel[2]}, *cd[3] = {den[0], den[1], den[2]};
-    rc = tke_budget_device(h->p, g, cv, cd, prof, ufl, vfl, h->stream);
+    const double *cq[3] = {q[0], q[1], q[2]};
+    rc = tke_budget_planar(h->p, g, cq, prof, ufl, vfl, h->stream, o);
   }
-  cudaFree(buf);
   return rc;
 }
 

@@ -108,6 +108,12 @@ void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int 
                        int k0_aos, cudaStream_t stream);
 void launch_fields_f32(const float *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);
+// the same moments as planar fields q[c][k][j][i] (c = u, v, w, den / 3) of a
+// level with nz planes, device plane p0 + s at k = k0 + s
+void launch_fields_planar_f64(const double *soa, double *q, int nx, int ny, int P, int p0, int np, int nz,
+                              int k0, cudaStream_t stream);
+void launch_fields_planar_f32(const float *soa, double *q, int nx, int ny, int P, int p0, int np, int nz, int k0,
+                              cudaStream_t stream);
 // Mode -i start: one level of the embedded grid interpolated from a uniform-grid
 // state.  uni is the uniform state in reference AoS order [xu][yu][zd][19]; out
 // receives the level in reference AoS order [nxl][nyl][nzl][19] (wall plane of a
@@ -129,6 +135,12 @@ void launch_uniform_interp_f64(const double *uni, const UniformMap &m, double *o
 int tke_validate(const dns_params &p);
 int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *const vel[3],
                       const double *const den[3], double *prof, double *ufl, double *vfl, cudaStream_t st);
+// the same from planar fields q[l] = [4][nz][ny][nx] (u, v, w, den / 3) per level
+// work: device space of tke_workspace_bytes(g) (8-byte aligned), or null to
+// allocate per call
+size_t tke_workspace_bytes(const dns_geometry &g);
+int tke_budget_planar(const dns_params &p, const dns_geometry &g, const double *const q[3], double *prof,
+                      double *ufl, double *vfl, cudaStream_t st, void *work = nullptr);
 // layout transposes between the device SoA state and the reference AoS order
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);

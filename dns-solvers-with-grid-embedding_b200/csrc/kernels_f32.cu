@@ -355,6 +355,7 @@ __global__ void aos_to_dev_kernel(const double *__restrict__ aos, float *__restr
 
 // ------------------------------------------------------------------ field output
 // f = w + d in FP64, then the moments in population order as the FP64 form
+template <bool PLANAR>
 __global__ void fields_f32_kernel(const float *__restrict__ soa, double *__restrict__ vel, double *__restrict__ den,
                                   int nx, int ny, int P, int p0, int nz_aos, int k0_aos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
@@ -376,6 +377,14 @@ __global__ void fields_f32_kernel(const float *__restrict__ soa, double *__restr
     uz = mz / dens;
   } else {
     dens = 0.;
+  }
+  if (PLANAR) {  // vel[c][k][j][i], c = u, v, w, den / 3
+    const size_t plane = (size_t)nz_aos * ny * nx, o = ((size_t)(k0_aos + q) * ny + j) * nx + i;
+    vel[o] = ux;
+    vel[plane + o] = uy;
+    vel[2 * plane + o] = uz;
+    vel[3 * plane + o] = (1. / 3.) * dens;
+    return;
   }
   const size_t o = ((size_t)i * ny + j) * nz_aos + k0_aos + q;
   vel[o * 3 + 0] = ux;
@@ -491,7 +500,13 @@ void launch_aos_to_dev_f32(const double *aos, float *soa, int nx, int ny, int P,
 void launch_fields_f32(const float *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream) {
   dim3 grid((nx + 127) / 128, ny, np), block(128);
-  fields_f32_kernel<<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
+  fields_f32_kernel<false><<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_fields_planar_f32(const float *soa, double *q, int nx, int ny, int P, int p0, int np, int nz, int k0,
+                              cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  fields_f32_kernel<true><<<grid, block, 0, stream>>>(soa, q, nullptr, nx, ny, P, p0, nz, k0);
 }
 
 }  // namespace dns

@@ -885,6 +885,7 @@ __global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__rest
 // ------------------------------------------------------------------ field output
 // vel_print.c:86-125: per node u = (sum E f) / rho, rho = sum f, both summed in
 // population order (moments_f64 is that order); zero where rho <= 0
+template <bool PLANAR>
 __global__ void fields_kernel(const double *__restrict__ soa, double *__restrict__ vel, double *__restrict__ den,
                               int nx, int ny, int P, int p0, int nz_aos, int k0_aos) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
@@ -901,6 +902,14 @@ __global__ void fields_kernel(const double *__restrict__ soa, double *__restrict
     uz = mz / dens;
   } else {
     dens = 0.;
+  }
+  if (PLANAR) {  // vel[c][k][j][i], c = u, v, w, den / 3
+    const size_t plane = (size_t)nz_aos * ny * nx, o = ((size_t)(k0_aos + q) * ny + j) * nx + i;
+    vel[o] = ux;
+    vel[plane + o] = uy;
+    vel[2 * plane + o] = uz;
+    vel[3 * plane + o] = (1. / 3.) * dens;
+    return;
   }
   const size_t o = ((size_t)i * ny + j) * nz_aos + k0_aos + q;
   vel[o * 3 + 0] = ux;
@@ -1139,7 +1148,13 @@ void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, in
 void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream) {
   dim3 grid((nx + 127) / 128, ny, np), block(128);
-  fields_kernel<<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
+  fields_kernel<false><<<grid, block, 0, stream>>>(soa, vel, den, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_fields_planar_f64(const double *soa, double *q, int nx, int ny, int P, int p0, int np, int nz,
+                              int k0, cudaStream_t stream) {
+  dim3 grid((nx + 127) / 128, ny, np), block(128);
+  fields_kernel<true><<<grid, block, 0, stream>>>(soa, q, nullptr, nx, ny, P, p0, nz, k0);
 }
 
 // ------------------------------------------------------------------ mode -i start

@@ -7,7 +7,8 @@
 //   1. planar copy of each level's fields, q[c][k][j][i] with c = u, v, w and
 //      den / 3 (the reference's pressure, budget2D.c:184);
 //   2. plane means of the composite profile (budget2D.c:178-241): lower fine
-//      planes 0..zdf-1, coarse planes 2..zdc-3, upper fine planes 0..zdf-1;
+//      planes 0..zdf-1, coarse planes 2..zdc-3, upper fine planes 0..zdf-1,
+//      each summed in the reference's order, so they are bit-identical;
 //   3. per-plane sums of the 44 products of fluctuations and their gradients
 //      (budget2D.c:448-1002): 4th-order central differences in x and y,
 //      the reference's plane-dependent rules in z (one-sided at the walls,
@@ -15,8 +16,9 @@
 //   4. on the host, the O(NZ) finalisation of budget2D.c:1004-1550: plane
 //      averages, rms, skewness, flatness, vorticity rms, production,
 //      turbulent / pressure / viscous transport, pressure strain, dissipation.
-// Block partials are summed in a fixed order, so results are deterministic;
-// they differ from the reference's sequential plane sums by rounding only.
+// Block partials of the 44 products are summed in a fixed order, so results are
+// deterministic; they differ from the reference's sequential plane sums by
+// rounding only.
 // This unit is built without fused multiply-add, like the reference.
 #include <cmath>
 #include <cstdio>
@@ -96,18 +98,24 @@ __device__ __forceinline__ int profile_of(const TkeArgs &A, int l, int k) {
   return l == 1 ? k : (l == 0 ? A.zdf - 2 + k : A.zdf + A.zdc - 4 + k);
 }
 
-// row sums of the four fields of the profile planes k0.. of level L
-// (budget2D.c:178-241); grid (ny, planes)
+// plane means of the four fields of the profile planes k0.. of level L, each
+// summed by one thread in the reference's order (j outer, i inner) and divided
+// by the plane's node count (budget2D.c:178-241): the means, and with them
+// every fluctuation, are the reference's to the last bit.  grid (planes),
+// threads 0..3 = u, v, w, den / 3.
 template <int L>
-__global__ void __launch_bounds__(kT) tke_mean_rows(TkeArgs A, int k0) {
-  const int j = blockIdx.x, k = k0 + blockIdx.y;
+__global__ void tke_mean_seq(TkeArgs A, int k0, double *__restrict__ mean) {
+  const int c = threadIdx.x, k = k0 + blockIdx.x;
+  if (c >= 4) return;
   const int nx = A.nx[L], ny = A.ny[L], nz = A.nz[L];
-  const size_t plane = (size_t)nz * ny * nx, row = ((size_t)k * ny + j) * nx;
-  double s[4] = {0., 0., 0., 0.};
-  for (int i = threadIdx.x; i < nx; i += blockDim.x)
-#pragma unroll
-    for (int c = 0; c < 4; c++) s[c] += A.q[L][c * plane + row + i];
-  block_sum<4>(s, A.part + ((size_t)profile_of(A, L, k) * A.nymax + j) * 4);
+  const double *q = A.q[L] + (size_t)c * nz * ny * nx + (size_t)k * ny * nx;
+  double s = 0.;
+  for (int j = 0; j < ny; j++) {
+    const double *row = q + (size_t)j * nx;
+#pragma unroll 8
+    for (int i = 0; i < nx; i++) s += row[i];
+  }
+  mean[(size_t)profile_of(A, L, k) * 4 + c] = s / (double)(nx * ny);
 }
 
 // plane totals of W row partials in row order
@@ -486,8 +494,13 @@ int tke_validate(const dns_params &p) {
   return DNS_OK;
 }
 
-int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *const vel[3],
-                      const double *const den[3], double *prof, double *ufl, double *vfl, cudaStream_t st) {
+size_t tke_workspace_bytes(const dns_geometry &g) {
+  const size_t NZ = g.nz_profile;
+  return (NZ * g.nyf * kNS + NZ * 4 + NZ * kNS) * 8 + NZ * sizeof(int);
+}
+
+int tke_budget_planar(const dns_params &p, const dns_geometry &g, const double *const q[3], double *prof,
+                      double *ufl, double *vfl, cudaStream_t st, void *work) {
   int rc = tke_validate(p);
   if (rc) return rc;
   TkeArgs A{};
@@ -499,6 +512,7 @@ int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *
     A.ny[l] = g.nyf;
     A.nz[l] = g.zdf;
   }
+  for (int l = 0; l < 3; l++) A.q[l] = q[l];
   A.gr = g.gr;
   A.zdf = g.zdf;
   A.zdc = g.nzc;
@@ -509,76 +523,54 @@ int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *
   // budget2D.c:57-60, tauf the fine relaxation time
   const double tauf = (3. / p.Rebs) * p.ub * (g.nzs - 2.) + 0.5;
   const double nu = (1. / 6.) * (2. * tauf - 1.);
-  size_t nq = 0;
-  for (int l = 0; l < 3; l++) nq += 4ull * A.nx[l] * A.ny[l] * A.nz[l];
   const size_t npart = (size_t)NZ * A.nymax * kNS;
-  double *buf = nullptr;
-  int *rows = nullptr;
-  const size_t nbuf = nq + npart + (size_t)NZ * 4 + (size_t)NZ * kNS;
-  if (cudaMalloc(&buf, nbuf * 8) != cudaSuccess) return fail_with(DNS_ENOMEM, "budget work space");
-  if (cudaMalloc(&rows, NZ * sizeof(int)) != cudaSuccess) {
-    cudaFree(buf);
-    return fail_with(DNS_ENOMEM, "budget work space");
+  const size_t nbuf = npart + (size_t)NZ * 4 + (size_t)NZ * kNS;
+  void *owned = nullptr;
+  if (!work) {
+    if (cudaMalloc(&owned, tke_workspace_bytes(g)) != cudaSuccess) return fail_with(DNS_ENOMEM, "budget work space");
+    work = owned;
   }
-  double *q = buf, *part = buf + nq, *mean = part + npart, *sums = mean + (size_t)NZ * 4;
-  std::vector<int> hrows(NZ);
-  for (int K = 0; K < NZ; K++) hrows[K] = (K >= g.zdf && K < g.zdf + g.nzc - 4) ? g.ny : g.nyf;
-  cudaError_t e = cudaMemcpyAsync(rows, hrows.data(), NZ * sizeof(int), cudaMemcpyHostToDevice, st);
-  double *ql = q;
-  for (int l = 0; l < 3 && e == cudaSuccess; l++) {
-    A.q[l] = ql;
-    dim3 grid((A.nx[l] + kT - 1) / kT, A.ny[l], A.nz[l]);
-    tke_planar_kernel<<<grid, kT, 0, st>>>(vel[l], den[l], A.nx[l], A.ny[l], A.nz[l], ql);
-    ql += 4ull * A.nx[l] * A.ny[l] * A.nz[l];
-    e = cudaGetLastError();
-  }
+  double *buf = static_cast<double *>(work);
+  int *dims = reinterpret_cast<int *>(buf + nbuf);
+  double *part = buf, *mean = part + npart, *sums = mean + (size_t)NZ * 4;
+  std::vector<int> hdims(NZ);
+  for (int K = 0; K < NZ; K++) hdims[K] = (K >= g.zdf && K < g.zdf + g.nzc - 4) ? g.ny : g.nyf;
   A.part = part;
   A.mean = mean;
+  const int nyc = g.ny, nyf = g.nyf;
+  cudaError_t e = cudaMemcpyAsync(dims, hdims.data(), NZ * sizeof(int), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
-    tke_mean_rows<1><<<dim3(g.nyf, g.zdf), kT, 0, st>>>(A, 0);
-    tke_mean_rows<0><<<dim3(g.ny, g.nzc - 4), kT, 0, st>>>(A, 2);
-    tke_mean_rows<2><<<dim3(g.nyf, g.zdf), kT, 0, st>>>(A, 0);
-    tke_sum_rows<<<NZ, 32, 0, st>>>(part, A.nymax, 4, rows, mean);
-    // plane sums -> means (one division per plane, as the reference)
+    tke_mean_seq<1><<<g.zdf, 32, 0, st>>>(A, 0, mean);
+    tke_mean_seq<0><<<g.nzc - 4, 32, 0, st>>>(A, 2, mean);
+    tke_mean_seq<2><<<g.zdf, 32, 0, st>>>(A, 0, mean);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, npart * 8, st);  // profile planes 0, NZ-1: no products
+  if (e == cudaSuccess) {
+    tke_budget_rows<1><<<dim3(nyf, g.zdf - 1), kT, 0, st>>>(A, 1);
+    tke_budget_rows<0><<<dim3(nyc, g.nzc - 4), kT, 0, st>>>(A, 2);
+    tke_budget_rows<2><<<dim3(nyf, g.zdf - 1), kT, 0, st>>>(A, 0);
+    tke_sum_rows<<<NZ, 64, 0, st>>>(part, A.nymax, kNS, dims, sums);
     e = cudaGetLastError();
   }
   std::vector<double> hmean((size_t)NZ * 4), hsums((size_t)NZ * kNS);
   if (e == cudaSuccess) e = cudaMemcpyAsync(hmean.data(), mean, hmean.size() * 8, cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e == cudaSuccess) {
-    for (int K = 0; K < NZ; K++) {
-      const int l = K < g.zdf ? 1 : (K < g.zdf + g.nzc - 4 ? 0 : 2);
-      const double num = (double)((long)A.nx[l] * A.ny[l]);
-      for (int c = 0; c < 4; c++) hmean[(size_t)K * 4 + c] /= num;
-    }
-    e = cudaMemcpyAsync(mean, hmean.data(), hmean.size() * 8, cudaMemcpyHostToDevice, st);
-  }
-  if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, npart * 8, st);  // profile planes 0, NZ-1: no products
-  if (e == cudaSuccess) {
-    tke_budget_rows<1><<<dim3(g.nyf, g.zdf - 1), kT, 0, st>>>(A, 1);
-    tke_budget_rows<0><<<dim3(g.ny, g.nzc - 4), kT, 0, st>>>(A, 2);
-    tke_budget_rows<2><<<dim3(g.nyf, g.zdf - 1), kT, 0, st>>>(A, 0);
-    tke_sum_rows<<<NZ, 64, 0, st>>>(part, A.nymax, kNS, rows, sums);
-    e = cudaGetLastError();
-  }
   if (e == cudaSuccess) e = cudaMemcpyAsync(hsums.data(), sums, hsums.size() * 8, cudaMemcpyDeviceToHost, st);
   // uv_fluc.c:24-33: fluctuations of the lower fine plane k = 4
+  const size_t pl = (size_t)g.nyf * g.nxf;
   std::vector<double> plane;
   if (e == cudaSuccess && (ufl || vfl)) {
-    const size_t pl = (size_t)g.nyf * g.nxf;
     plane.resize(2 * pl);
-    const size_t stride = (size_t)g.zdf * pl;
-    e = cudaMemcpyAsync(plane.data(), A.q[1] + 4 * pl, pl * 8, cudaMemcpyDeviceToHost, st);
+    e = cudaMemcpyAsync(plane.data(), q[1] + 4 * pl, pl * 8, cudaMemcpyDeviceToHost, st);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(plane.data() + pl, A.q[1] + stride + 4 * pl, pl * 8, cudaMemcpyDeviceToHost, st);
+      e = cudaMemcpyAsync(plane.data() + pl, q[1] + (size_t)g.zdf * pl + 4 * pl, pl * 8, cudaMemcpyDeviceToHost,
+                          st);
   }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(buf);
-  cudaFree(rows);
+  if (owned) cudaFree(owned);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, cudaGetErrorString(e));
   finalize(A, nu, hmean.data(), hsums.data(), prof);
   if (ufl || vfl) {
-    const size_t pl = (size_t)g.nyf * g.nxf;
     for (int i = 0; i < g.nxf; i++)
       for (int j = 0; j < g.nyf; j++) {
         if (ufl) ufl[(size_t)i * g.nyf + j] = plane[(size_t)j * g.nxf + i] - hmean[4 * 4 + 0];
@@ -586,6 +578,31 @@ int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *
       }
   }
   return DNS_OK;
+}
+
+int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *const vel[3],
+                      const double *const den[3], double *prof, double *ufl, double *vfl, cudaStream_t st) {
+  int rc = tke_validate(p);
+  if (rc) return rc;
+  const int nx[3] = {g.nx, g.nxf, g.nxf}, ny[3] = {g.ny, g.nyf, g.nyf}, nz[3] = {g.nzc, g.zdf, g.zdf};
+  size_t nq = 0;
+  for (int l = 0; l < 3; l++) nq += 4ull * nx[l] * ny[l] * nz[l];
+  double *buf = nullptr;
+  if (cudaMalloc(&buf, nq * 8) != cudaSuccess) return fail_with(DNS_ENOMEM, "budget planar fields");
+  const double *q[3];
+  double *ql = buf;
+  cudaError_t e = cudaSuccess;
+  for (int l = 0; l < 3 && e == cudaSuccess; l++) {
+    q[l] = ql;
+    dim3 grid((nx[l] + kT - 1) / kT, ny[l], nz[l]);
+    tke_planar_kernel<<<grid, kT, 0, st>>>(vel[l], den[l], nx[l], ny[l], nz[l], ql);
+    ql += 4ull * nx[l] * ny[l] * nz[l];
+    e = cudaGetLastError();
+  }
+  rc = e == cudaSuccess ? tke_budget_planar(p, g, q, prof, ufl, vfl, st) : fail_with(DNS_ECUDA, cudaGetErrorString(e));
+  cudaStreamSynchronize(st);
+  cudaFree(buf);
+  return rc;
 }
 
 }  // namespace dns

@@ -56,7 +56,7 @@ REF_CONFIGS = {
                CFL=0.1, gratio=2, zds=8, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4,
                XDIM=1, YDIM=1, tke=True),
     "c2": dict(Rebs=5533.0, ub=UB, zdv=83, ydv=128, xdv=256, TSTR=0, TEND=1, CFL=0.1, gratio=2,
-               zds=16, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4, XDIM=1, YDIM=1),
+               zds=16, gyplussize=4, wyplussize=4, gxplussize=4, wxplussize=4, XDIM=1, YDIM=1, tke=True),
     "c3r": dict(Rebs=13585.0, ub=UB, zdv=115, ydv=192, xdv=384, TSTR=0, TEND=1, CFL=0.1, gratio=2,
                 zds=16, gyplussize=24, wyplussize=24, gxplussize=16, wxplussize=16, XDIM=1, YDIM=1,
                 pattern="RSLIP"),
