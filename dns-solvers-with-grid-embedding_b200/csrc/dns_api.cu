@@ -72,6 +72,8 @@ struct dns_handle {
   double *iface_mac = nullptr;         // FP64: interface rho, u [2][4][nyf][nxf]; FP32: corner data
   void *tke_ws = nullptr;              // statistics / budget work space (allocated on first use)
   size_t tke_ws_bytes = 0;
+  double *tke_wall = nullptr;          // planar fields of the two wall planes [2][4][nyf][nxf]
+  long tke_wall_gen = -1;              // wall_gen they were made from
   unsigned int *fin_counter = nullptr; // finalize's block counter
   cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
   cudaStream_t hip = nullptr;          // interface transfers (highest priority)
@@ -81,6 +83,7 @@ struct dns_handle {
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
   long sample_every = 0;
   std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
+  long wall_gen = 0;                     // bumped whenever wall_lo / wall_hi change
   Profiler prof;
 };
 
@@ -293,6 +296,7 @@ extern "C" void dns_destroy(dns_handle *h) {
   cudaFree(h->stats_acc);
   cudaFree(h->iface_mac);
   cudaFree(h->tke_ws);
+  cudaFree(h->tke_wall);
   cudaFree(h->fin_counter);
   if (h->hlog) cudaFreeHost(h->hlog);
   for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
@@ -461,6 +465,7 @@ static int import_level_f32(dns_handle *h, int level, const double *in) {
   if (e != cudaSuccess) return fail(DNS_ECUDA, cudaGetErrorString(e));
   if (level > 0) {
     std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+    h->wall_gen++;
     const int kw = level == 1 ? 0 : g.zdf - 1;
     for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
       std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
@@ -519,6 +524,7 @@ static int import_level(dns_handle *h, int level, const double *in) {
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
+  h->wall_gen++;
   const int kw = level == 1 ? 0 : g.zdf - 1;
   for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
     std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
@@ -640,6 +646,7 @@ extern "C" int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double a
   CUDA_TRY(cudaGetLastError());
   std::fill(h->wall_lo.begin(), h->wall_lo.end(), 0.0);
   std::fill(h->wall_hi.begin(), h->wall_hi.end(), 0.0);
+  h->wall_gen++;
   h->ss = 0;
   h->tm = h->p.TSTR;
   return refresh_flow(h, h->p.forcing == DNS_FORCING_CFR ? 0.0 : h->p.force_const);
@@ -859,26 +866,35 @@ static int fields_planar(dns_handle *h, double *const q[3]) {
                                h->stream);
     CUDA_TRY(cudaGetLastError());
   }
-  // wall planes: lower k = 0, upper k = zdf - 1, [c][j][i] per plane
+  // wall planes: lower k = 0, upper k = zdf - 1, [c][j][i] per plane; made on
+  // the host from the wall populations when those change, kept on the device
   const size_t npl = (size_t)g.nxf * g.nyf, lvl = level_nodes(g, 1);
-  std::vector<double> wv(npl * 3), wd(npl), planes(2 * 4 * npl);
+  if (h->tke_wall_gen != h->wall_gen) {
+    if (!h->tke_wall && cudaMalloc(&h->tke_wall, 2 * 4 * npl * 8) != cudaSuccess)
+      return fail(DNS_ENOMEM, "wall-plane fields for the budget");
+    std::vector<double> wv(npl * 3), wd(npl), planes(2 * 4 * npl);
+    for (int lv = 1; lv < 3; lv++) {
+      wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
+      double *o = planes.data() + (size_t)(lv - 1) * 4 * npl;
+      for (int i = 0; i < g.nxf; i++)
+        for (int j = 0; j < g.nyf; j++) {
+          const size_t c = (size_t)i * g.nyf + j, t = (size_t)j * g.nxf + i;
+          o[t] = wv[c * 3];
+          o[npl + t] = wv[c * 3 + 1];
+          o[2 * npl + t] = wv[c * 3 + 2];
+          o[3 * npl + t] = (1. / 3.) * wd[c];
+        }
+    }
+    CUDA_TRY(cudaMemcpyAsync(h->tke_wall, planes.data(), planes.size() * 8, cudaMemcpyHostToDevice, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));  // planes goes out of scope
+    h->tke_wall_gen = h->wall_gen;
+  }
   for (int lv = 1; lv < 3; lv++) {
-    wall_plane_fields(lv == 1 ? h->wall_lo : h->wall_hi, npl, wv.data(), wd.data());
-    double *o = planes.data() + (size_t)(lv - 1) * 4 * npl;
-    for (int i = 0; i < g.nxf; i++)
-      for (int j = 0; j < g.nyf; j++) {
-        const size_t c = (size_t)i * g.nyf + j, t = (size_t)j * g.nxf + i;
-        o[t] = wv[c * 3];
-        o[npl + t] = wv[c * 3 + 1];
-        o[2 * npl + t] = wv[c * 3 + 2];
-        o[3 * npl + t] = (1. / 3.) * wd[c];
-      }
     const int kw = lv == 1 ? 0 : g.zdf - 1;
     for (int c = 0; c < 4; c++)
-      CUDA_TRY(cudaMemcpyAsync(q[lv] + c * lvl + (size_t)kw * npl, o + c * npl, npl * 8, cudaMemcpyHostToDevice,
-                               h->stream));
+      CUDA_TRY(cudaMemcpyAsync(q[lv] + c * lvl + (size_t)kw * npl, h->tke_wall + ((size_t)(lv - 1) * 4 + c) * npl,
+                               npl * 8, cudaMemcpyDeviceToDevice, h->stream));
   }
-  CUDA_TRY(cudaStreamSynchronize(h->stream));  // planes goes out of scope
   return DNS_OK;
 }
 

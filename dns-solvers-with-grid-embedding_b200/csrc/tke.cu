@@ -99,23 +99,40 @@ __device__ __forceinline__ int profile_of(const TkeArgs &A, int l, int k) {
 }
 
 // plane means of the four fields of the profile planes k0.. of level L, each
-// summed by one thread in the reference's order (j outer, i inner) and divided
-// by the plane's node count (budget2D.c:178-241): the means, and with them
-// every fluctuation, are the reference's to the last bit.  grid (planes),
-// threads 0..3 = u, v, w, den / 3.
+// summed in the reference's order (j outer, i inner: the plane's memory order)
+// and divided by the plane's node count (budget2D.c:178-241): the means, and
+// with them every fluctuation, are the reference's to the last bit.  The block
+// stages the plane through shared memory in coalesced chunks; threads 0..3
+// (u, v, w, den / 3) add each chunk in order.
+constexpr int kMeanChunk = 1024;
+
 template <int L>
-__global__ void tke_mean_seq(TkeArgs A, int k0, double *__restrict__ mean) {
-  const int c = threadIdx.x, k = k0 + blockIdx.x;
-  if (c >= 4) return;
+__device__ __forceinline__ void mean_plane(const TkeArgs &A, int k, double (*buf)[kMeanChunk],
+                                           double *__restrict__ mean) {
   const int nx = A.nx[L], ny = A.ny[L], nz = A.nz[L];
-  const double *q = A.q[L] + (size_t)c * nz * ny * nx + (size_t)k * ny * nx;
+  const size_t n = (size_t)nx * ny, field = (size_t)nz * n;
+  const double *q = A.q[L] + (size_t)k * n;
   double s = 0.;
-  for (int j = 0; j < ny; j++) {
-    const double *row = q + (size_t)j * nx;
-#pragma unroll 8
-    for (int i = 0; i < nx; i++) s += row[i];
+  for (size_t base = 0; base < n; base += kMeanChunk) {
+    const int len = (int)(n - base < (size_t)kMeanChunk ? n - base : (size_t)kMeanChunk);
+#pragma unroll
+    for (int c = 0; c < 4; c++)
+      for (int t = threadIdx.x; t < len; t += blockDim.x) buf[c][t] = q[c * field + base + t];
+    __syncthreads();
+    if (threadIdx.x < 4)
+      for (int t = 0; t < len; t++) s += buf[threadIdx.x][t];
+    __syncthreads();
   }
-  mean[(size_t)profile_of(A, L, k) * 4 + c] = s / (double)(nx * ny);
+  if (threadIdx.x < 4) mean[(size_t)profile_of(A, L, k) * 4 + threadIdx.x] = s / (double)(nx * ny);
+}
+
+// one block per profile plane K
+__global__ void __launch_bounds__(kT) tke_mean_seq(TkeArgs A, double *__restrict__ mean) {
+  __shared__ double buf[4][kMeanChunk];
+  const int K = blockIdx.x;
+  if (K < A.zdf) mean_plane<1>(A, K, buf, mean);
+  else if (K < A.zdf + A.zdc - 4) mean_plane<0>(A, K - A.zdf + 2, buf, mean);
+  else mean_plane<2>(A, K - (A.zdf + A.zdc - 4), buf, mean);
 }
 
 // plane totals of W row partials in row order
@@ -540,9 +557,7 @@ int tke_budget_planar(const dns_params &p, const dns_geometry &g, const double *
   const int nyc = g.ny, nyf = g.nyf;
   cudaError_t e = cudaMemcpyAsync(dims, hdims.data(), NZ * sizeof(int), cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) {
-    tke_mean_seq<1><<<g.zdf, 32, 0, st>>>(A, 0, mean);
-    tke_mean_seq<0><<<g.nzc - 4, 32, 0, st>>>(A, 2, mean);
-    tke_mean_seq<2><<<g.zdf, 32, 0, st>>>(A, 0, mean);
+    tke_mean_seq<<<NZ, kT, 0, st>>>(A, mean);
     e = cudaGetLastError();
   }
   if (e == cudaSuccess) e = cudaMemsetAsync(part, 0, npart * 8, st);  // profile planes 0, NZ-1: no products
