@@ -42,7 +42,11 @@ def _stale(obj: Path, deps) -> bool:
 
 
 def build(verbose: bool = False) -> Path:
+    """Compile stale units and link.  Extra nvcc flags (e.g. a tuning macro
+    such as -DDNS_ITY=16) can be given in DNS_NVCC_FLAGS; touch the sources to
+    rebuild with them."""
     nvcc = _nvcc()
+    extra_env = os.environ.get("DNS_NVCC_FLAGS", "").split()
     gen = CSRC / "bicubic_gen.cuh"
     if _stale(gen, [CSRC / "gen_bicubic.py"]):
         subprocess.run([sys.executable, str(CSRC / "gen_bicubic.py")], check=True)
@@ -53,7 +57,7 @@ def build(verbose: bool = False) -> Path:
     for src, extra in UNITS.items():
         obj = build_dir / (Path(src).stem + ".o")
         if _stale(obj, [CSRC / src] + headers):
-            cmd = [nvcc] + ARCH + COMMON + extra + ["-c", str(CSRC / src), "-o", str(obj)]
+            cmd = [nvcc] + ARCH + COMMON + extra + extra_env + ["-c", str(CSRC / src), "-o", str(obj)]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

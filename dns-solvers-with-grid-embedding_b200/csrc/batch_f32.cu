@@ -524,12 +524,20 @@ __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, D
     __syncthreads();
     if (last) {
       __threadfence();
-      if (threadIdx.x < kFinComp) {
+      // the chunk rows are loaded by the whole block at once (into the free
+      // reduction buffer), then summed in chunk order by one thread each
+      static_assert(kFinChunks * kFinComp <= kFinComp * kThreads, "staging fits");
+      double *flat = &sh[0][0];
+      {
         const volatile double *L = l2;
-        double a = 0.;
-        for (int q = 0; q < kFinChunks; q++) a += L[q * kFinComp + threadIdx.x];
-        sh[threadIdx.x][0] = a;
+        for (int q = threadIdx.x; q < kFinChunks * kFinComp; q += kThreads) flat[q] = L[q];
       }
+      __syncthreads();
+      double a = 0.;
+      if (threadIdx.x < kFinComp)
+        for (int q = 0; q < kFinChunks; q++) a += flat[q * kFinComp + threadIdx.x];
+      __syncthreads();
+      if (threadIdx.x < kFinComp) sh[threadIdx.x][0] = a;
       __syncthreads();
       if (threadIdx.x == 0) {
         double S[kFinComp];

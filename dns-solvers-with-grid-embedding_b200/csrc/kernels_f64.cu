@@ -267,9 +267,18 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
 // d2/dxdy, bicubic coefficients per coarse cell, Horner evaluation at the
 // GR x GR fine nodes and f = feq + omega_c/(GR omega_f) fneq.  A tile of
 // ITX x ITY coarse cells stages the (ITX+5) x (ITY+5) periodic patch of one
-// field at a time in shared memory; one thread owns one coarse cell.
-constexpr int ITX = 32, ITY = 16;          // coarse cells per tile
-constexpr int TPX = 16, TPY = 8;           // threads per tile (each owns 2 x 2 cells)
+// field at a time in shared memory; each thread owns CPT coarse cells.  The
+// tile is 32 x 8 cells (2 per thread): twice the blocks of 32 x 16 tiles, so
+// the last of the ~5 waves of population blocks is a smaller share of the
+// launch (a 2 x 19 x 64-tile grid at 7 blocks per SM leaves the third of 2.35
+// waves a third full).
+#ifndef DNS_ITY
+#define DNS_ITY 8
+#endif
+constexpr int ITX = 32, ITY = DNS_ITY;     // coarse cells per tile
+constexpr int TPX = 16, TPY = 8;           // threads per tile
+constexpr int CPT = (ITX / TPX) * (ITY / TPY);  // cells per thread
+static_assert(ITX % TPX == 0 && ITY % TPY == 0, "tile / thread layout");
 constexpr int PX = ITX + 5, PY = ITY + 5;  // staged periodic patch
 
 struct IfaceArgs {
@@ -371,8 +380,8 @@ __global__ void __launch_bounds__(TPX *TPY) interface_macro_kernel(const double 
   iface_stage(S, hn, hp, hpp, ((size_t)w * 23 + b) * plane, i0, j0, nx, ny, ia);
   double *o = mac + ((size_t)w * 4 + b) * fplane;
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int cx = tx + TPX * (q & 1), cy = ty + TPY * (q >> 1);
+  for (int q = 0; q < CPT; q++) {
+    const int cx = tx + TPX * (q % (ITX / TPX)), cy = ty + TPY * (q / (ITX / TPX));
     const int ic = i0 + cx, jc = j0 + cy;
     if (ic < nx && jc < ny) {
       double cf[16];
@@ -409,8 +418,8 @@ __global__ void __launch_bounds__(TPX *TPY) interface_pop_kernel(const double *_
   const double *m = mac + (size_t)w * 4 * fplane;
   double *out = fdst + (size_t)a * fstride + (size_t)pf * fplane;
 #pragma unroll
-  for (int q = 0; q < 4; q++) {
-    const int cx = tx + TPX * (q & 1), cy = ty + TPY * (q >> 1);
+  for (int q = 0; q < CPT; q++) {
+    const int cx = tx + TPX * (q % (ITX / TPX)), cy = ty + TPY * (q / (ITX / TPX));
     const int ic = i0 + cx, jc = j0 + cy;
     if (ic < nx && jc < ny) {
       double cf[16];
@@ -695,10 +704,17 @@ __global__ void __launch_bounds__(kFin2Threads) finalize2_kernel(DevState *st, D
   if (!last) return;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x < kFin2Comp) {
+  // the level-2 rows are loaded by the whole block at once, then summed in
+  // block order by one thread per component
+  __shared__ double rows[kFin2Blocks * kFin2Comp];
+  {
     const volatile double *l2 = level2;
+    for (int q = threadIdx.x; q < nb * kFin2Comp; q += blockDim.x) rows[q] = l2[q];
+  }
+  __syncthreads();
+  if (threadIdx.x < kFin2Comp) {
     double s = 0.;
-    for (int q = 0; q < nb; q++) s += l2[q * kFin2Comp + threadIdx.x];
+    for (int q = 0; q < nb; q++) s += rows[q * kFin2Comp + threadIdx.x];
     sh[threadIdx.x] = s;
   }
   __syncthreads();
