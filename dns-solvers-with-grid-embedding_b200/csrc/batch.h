@@ -96,8 +96,9 @@ struct Grids {
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)
+// stats: launch the statistics phases (some resident instance samples)
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
-                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev);  // ev: 10 events (fork/join of the two streams)
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats);  // ev: 10 events (fork/join of the two streams)
 void tile_counts(const Inst &I, int counts[PH_NPHASE]);
 
 }  // namespace batch

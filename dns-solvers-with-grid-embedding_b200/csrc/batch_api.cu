@@ -164,7 +164,9 @@ struct dns_batch {
   Dyn *hdyn[2] = {nullptr, nullptr};      // pinned snapshots
   DevLog *hlog[2] = {nullptr, nullptr};
   Grids grids{};
-  cudaGraphExec_t gexec[2] = {nullptr, nullptr};  // kGroup steps, 1 step
+  // [with statistics phases][kGroup steps, 1 step]; the statistics launches
+  // are left out while no resident instance samples
+  cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
   std::vector<Record> recs;  // by id
   std::vector<int> free_slots;
   std::map<ShapeKey, dns_tile> tuned;
@@ -178,8 +180,9 @@ static void release(dns_batch *b) {
   for (Record &r : b->recs)
     if (r.chunk) cudaFreeAsync(r.chunk, b->s);
   if (b->s) cudaStreamSynchronize(b->s);
-  for (cudaGraphExec_t &g : b->gexec)
-    if (g) cudaGraphExecDestroy(g);
+  for (auto &row : b->gexec)
+    for (cudaGraphExec_t &g : row)
+      if (g) cudaGraphExecDestroy(g);
   cudaFree(b->dmix);
   cudaFree(b->ddyn);
   cudaFree(b->dstate);
@@ -432,11 +435,11 @@ static int upload_mix(dns_batch *b) {
   return DNS_OK;
 }
 
-static int capture(dns_batch *b, int steps, cudaGraphExec_t *out) {
+static int capture(dns_batch *b, int steps, bool stats, cudaGraphExec_t *out) {
   cudaGraph_t graph = nullptr;
   BTRY(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
   for (int q = 0; q < steps; q++)
-    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->dcount, b->gr, b->grids, b->s, b->aux, b->ev);
+    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->dcount, b->gr, b->grids, b->s, b->aux, b->ev, stats);
   cudaError_t e = cudaStreamEndCapture(b->s, &graph);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
   e = cudaGraphInstantiate(out, graph, 0);
@@ -476,24 +479,27 @@ extern "C" int dns_batch_run(dns_batch *b, long long nsteps, int *active) {
   BTRY(cudaSetDevice(b->device));
   int rc;
   int live = 0, maxslot = -1;
+  bool sampling = false;
   for (const Record &r : b->recs)
     if (r.live) {
       live++;
       maxslot = std::max(maxslot, r.inst.slot);
+      sampling = sampling || r.inst.sample_every > 0;
     }
   if (live > 0 && nsteps > 0) {
     if (b->dirty && (rc = upload_mix(b))) return rc;
-    if (!b->gexec[0] && (rc = capture(b, kGroup, &b->gexec[0]))) return rc;
-    if (!b->gexec[1] && (rc = capture(b, 1, &b->gexec[1]))) return rc;
+    cudaGraphExec_t *gx = b->gexec[sampling ? 1 : 0];
+    if (!gx[0] && (rc = capture(b, kGroup, sampling, &gx[0]))) return rc;
+    if (!gx[1] && (rc = capture(b, 1, sampling, &gx[1]))) return rc;
     const size_t logbytes = sizeof(DevLog) * kLogRows * (size_t)(maxslot + 1);
     long long left = nsteps;
     int k = 0;
     while (left > 0) {
       const int n = left >= kGroup ? kGroup : (int)left;
       if (n == kGroup) {
-        BTRY(cudaGraphLaunch(b->gexec[0], b->s));
+        BTRY(cudaGraphLaunch(gx[0], b->s));
       } else {
-        for (int q = 0; q < n; q++) BTRY(cudaGraphLaunch(b->gexec[1], b->s));
+        for (int q = 0; q < n; q++) BTRY(cudaGraphLaunch(gx[1], b->s));
       }
       BTRY(cudaMemcpyAsync(b->hdyn[k & 1], b->ddyn, sizeof(Dyn) * (size_t)(maxslot + 1), cudaMemcpyDeviceToHost, b->s));
       BTRY(cudaMemcpyAsync(b->hlog[k & 1], b->dlog, logbytes, cudaMemcpyDeviceToHost, b->s));

@@ -665,11 +665,13 @@ static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g
 // The statistics read the state fine(2) and iface(2) overwrite; both follow
 // iface(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject.
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
-                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev) {
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats) {
   cudaEventRecord(ev[0], s);
   cudaStreamWaitEvent(aux, ev[0], 0);
-  b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
-  b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
+  if (stats) {
+    b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
+    b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
+  }
   b_coarse<true><<<g.cbulk, kThreads, 0, s>>>(m, dyn, state);
   b_coarse<false><<<g.cedge, kThreads, 0, s>>>(m, dyn, state);
   b_extract<<<g.extract, kThreads, 0, s>>>(m, dyn);
