@@ -521,13 +521,16 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_fp32:
         ch.close()  # (idempotent)
         b1 = pkg.Batch(local_rank)
-        b1.add(pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank), steps=10 ** 9, seed=42 + rank)
+        p32 = pkg.make_params(**m, forcing=pkg.FORCING_CFR, device=local_rank)
+        tile32 = b1.autotune(p32, steps=5)[0] if args.autotune else None
+        b1.add(p32, steps=10 ** 9, seed=42 + rank)
         b1.run(args.warmup)
         ms32 = timed_batch_run(torch, b1, args.steps)
         b1.close()
         v32 = U * args.steps * world / (ms32 * 1e-3) / 1e6
         line["fp32"] = {"value": v32, "unit": "MLUPS", "ms_per_step": ms32 / args.steps,
                         "dtype": "f32 (deviation storage, FP64 reductions)", "engine": "batched, one instance",
+                        "tile": tile32 if tile32 else "default",
                         "over_fp64": v32 / value,
                         "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak}
     if world == 1 and not args.no_batched:
@@ -570,6 +573,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-budget", action="store_true")
+    ap.add_argument("--autotune", action=argparse.BooleanOptionalAction, default=False,
+                    help="autotune the FP32 leg's tile (the engine's own tuner) before timing it")
     ap.add_argument("--c4-instances", type=int, default=96)
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--c5-requests", type=int, default=16)
