@@ -119,8 +119,11 @@ __device__ __forceinline__ void mean_plane(const TkeArgs &A, int k, double (*buf
     for (int c = 0; c < 4; c++)
       for (int t = threadIdx.x; t < len; t += blockDim.x) buf[c][t] = q[c * field + base + t];
     __syncthreads();
-    if (threadIdx.x < 4)
+    if (threadIdx.x < 4) {
+      // unrolled so the shared-memory loads run ahead of the (ordered) adds
+#pragma unroll 16
       for (int t = 0; t < len; t++) s += buf[threadIdx.x][t];
+    }
     __syncthreads();
   }
   if (threadIdx.x < 4) mean[(size_t)profile_of(A, L, k) * 4 + threadIdx.x] = s / (double)(nx * ny);
