@@ -423,8 +423,11 @@ inline IfParams32 iface_params32(const float *hn, const float *hp, const float *
 
 // pass 1 tile: CTX x CTY interface nodes; a work item covers a group of fields
 constexpr int CTX = 32, CTY = 8;
-constexpr int kCornerFieldGroups = 3;  // fields [0, 8), [8, 16), [16, 23)
-__host__ __device__ constexpr int corner_field(int g) { return g * 8 < 23 ? g * 8 : 23; }
+#ifndef DNS_CORNER_FIELD_GROUPS
+#define DNS_CORNER_FIELD_GROUPS 3
+#endif
+constexpr int kCornerFieldGroups = DNS_CORNER_FIELD_GROUPS;  // work items per (tile, wall): field groups
+__host__ __device__ constexpr int corner_field(int g) { return 23 * g / kCornerFieldGroups; }
 struct IfCornerSmem {
   float V[CTY + 4][CTX + 4];
   float DY[CTY][CTX + 4];
@@ -528,7 +531,10 @@ struct IfTile<4> {
   static constexpr int TX = 16, TY = 4;
 };
 constexpr int kEvalStages = 4;     // corner tiles in flight
-constexpr int kEvalPopGroups = 2;  // population groups per (tile, wall)
+#ifndef DNS_EVAL_POP_GROUPS
+#define DNS_EVAL_POP_GROUPS 2
+#endif
+constexpr int kEvalPopGroups = DNS_EVAL_POP_GROUPS;  // population groups per (tile, wall)
 
 template <int GR>
 struct IfEvalSmem {
