@@ -206,6 +206,12 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   const bool wall_sum_plane =
       upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
   const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
+  // Planes whose pushes all land on planes of encalc2 weight 1 (no wall, no
+  // dropped push into the interface plane): a node's flow-rate partials are
+  // its post-collision moments, mass dens and momentum dens u0 + dens Gf (the
+  // collision keeps both; the forcing adds rho G to sum e_x f, since
+  // sum_a e_x^2 BI_a = 1).  Other planes sum the pushes with their weights.
+  const bool unit_plane = upper ? (k >= gr + 2 && k <= zdf - 3) : (k >= 2 && k <= zdf - gr - 2);
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
   double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
@@ -223,6 +229,10 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
     if (MODE & 4) {
       sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += dens;
       sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += dens * dens;
+    }
+    if ((MODE & 1) && unit_plane) {
+      acc[0] += dens * u0 + dens * Gf;
+      acc[1] += dens;
     }
     const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
     const int8_t own = wf[(size_t)j * nx + i];
@@ -246,7 +256,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
         pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
       }
       dst[(size_t)ad * pstride + ((size_t)pd * ny + jd) * nx + id] = f[a];
-      if (MODE & 1) {
+      if ((MODE & 1) && !unit_plane) {
         const double wgt = weight(kd);
         acc[1] += wgt * f[a];
         if (exd > 0) acc[0] += wgt * f[a];
