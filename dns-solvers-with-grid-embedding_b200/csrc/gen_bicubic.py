@@ -9,7 +9,10 @@ reference forms c = W x with a dense 16-term loop per coefficient
 (``bcucof_opt.c:55-61``, ``xx += wt[i][k]*x[k]`` for k = 0..15).  Adding a zero
 product leaves a non-zero partial sum unchanged, so the emitted code keeps only
 the non-zero terms, in ascending k, left-associated — the same rounding
-sequence without the 60% of multiply-adds that are zero.
+sequence without the 60% of multiply-adds that are zero.  Weights of +-1 become
+an addition or subtraction (1 x and -1 x are exact), and power-of-two weights
+(+-2, +-4) a fused multiply-add: their product is exact, so rounding once after
+the add is what rounding the product and then the sum gives.
 
 Run: ``python gen_bicubic.py`` (writes next to this file).
 """
@@ -72,16 +75,26 @@ def emit(path: Path):
         "// from x[type*4+corner] (type: value, d/dt, d/du, d2/dtdu; corners",
         "// counter-clockwise from (0,0)).  Non-zero terms only, ascending k,",
         "// left-associated (the rounding sequence of a dense k = 0..15 loop).",
+        "// A weight of +-1 is an exact sign; a weight that is a power of two",
+        "// makes the product exact, so fma(w, x, s) rounds as s + w x does.",
         "#pragma once",
         "#define DNS_BICUBIC_COEFFS(c, x) \\",
     ]
     def body(suffix):
         out = []
         for r, row in enumerate(W):
-            terms = [f"({float(w)!r}{suffix} * (x)[{k}])" for k, w in enumerate(row) if w != 0]
-            expr = terms[0]
-            for t in terms[1:]:
-                expr = f"({expr} + {t})"
+            nz = [(k, w) for k, w in enumerate(row) if w != 0]
+            k0, w0 = nz[0]
+            expr = f"(x)[{k0}]" if w0 == 1 else (f"(-(x)[{k0}])" if w0 == -1 else f"({float(w0)!r}{suffix} * (x)[{k0}])")
+            for k, w in nz[1:]:
+                if w == 1:
+                    expr = f"({expr} + (x)[{k}])"
+                elif w == -1:
+                    expr = f"({expr} - (x)[{k}])"
+                elif abs(w) & (abs(w) - 1) == 0:   # +-2, +-4, ...: the product is exact
+                    expr = f"fma({float(w)!r}{suffix}, (x)[{k}], {expr})"
+                else:
+                    expr = f"({expr} + ({float(w)!r}{suffix} * (x)[{k}]))"
             out.append(f"  (c)[{r}] = {expr};")
         return out
     lines.append(" \\\n".join(body("")))

@@ -355,11 +355,26 @@ __device__ __forceinline__ void iface_coeffs(const IfaceSmem &S, int cx, int cy,
 // at u = 0 each inner polynomial is its constant term.  Adding an exact zero
 // leaves a non-zero value unchanged, so the shortcuts give the same value
 // (a zero result can only differ in the sign of the zero).
+// For GR = 2 the only non-zero t and u are 1/2: every product is exact, so a
+// product and the sum it feeds become one fused multiply-add with the same
+// result.  The outer step is (t val + p u) + c0 in that association: the
+// reference adds the row's constant term last.
 template <int GR>
 __device__ __forceinline__ double iface_eval(const double (&cf)[16], int ii, int jj) {
   const double tt = ((double)ii) / ((double)GR);
   const double uu = ((double)jj) / ((double)GR);
   if (ii == 0 && jj == 0) return cf[0];
+  if (GR == 2) {
+    if (ii == 0) return fma(fma(fma(cf[3], uu, cf[2]), uu, cf[1]), uu, cf[0]);
+    if (jj == 0) return fma(tt, fma(tt, fma(tt, cf[12], cf[8]), cf[4]), cf[0]);
+    double val = fma(fma(fma(cf[15], uu, cf[14]), uu, cf[13]), uu, cf[12]);
+#pragma unroll
+    for (int nn = 2; nn > -1; nn--) {
+      const double p = fma(fma(cf[nn * 4 + 3], uu, cf[nn * 4 + 2]), uu, cf[nn * 4 + 1]);
+      val = fma(p, uu, tt * val) + cf[nn * 4];
+    }
+    return val;
+  }
   if (ii == 0) return ((cf[3] * uu + cf[2]) * uu + cf[1]) * uu + cf[0];
   if (jj == 0) {
     double val = cf[12];
