@@ -140,7 +140,8 @@ class ClockSampler:
 def reference_cpu(config: str, steps: int, processes: int, timeout: float = 900.0):
     """Time the reference's own routines (oracle/_ref/<config>/ref_harness, one
     rank per process, from rest, constant-force mode with zero force) on the host.
-    Returns (aggregate MLUPS, seconds per step per process, processes)."""
+    Returns each process's step-loop seconds (its own clock), or None when the
+    binary is missing or a process gave no time."""
     exe = ROOT / "oracle" / "_ref" / config / "ref_harness"
     if not exe.exists():
         return None
