@@ -143,6 +143,7 @@ def lib() -> C.CDLL:
         "dns_batch_info_of": (I, [P, I, C.POINTER(BatchInfo)]),
         "dns_batch_stats": (I, [P, I, P, C.POINTER(C.c_long)]),
         "dns_batch_export_state": (I, [P, I, I, P]),
+        "dns_batch_import_state": (I, [P, I, I, P]),
         "dns_batch_log": (I, [P, I, C.c_longlong, C.c_longlong, P]),
         "dns_batch_stream": (I, [P, C.POINTER(P)]),
         "dns_error_string": (C.c_char_p, [I]),
@@ -435,6 +436,14 @@ class Batch:
         out = np.empty(shape, dtype=np.float64)
         _check(lib().dns_batch_export_state(self.h, i, level, out.ctypes.data), "dns_batch_export_state")
         return out
+
+    def import_state(self, i: int, level: int, arr: np.ndarray):
+        g = self.geoms[i]
+        shape = (g.nx, g.ny, g.nzc, 19) if level == 0 else (g.nxf, g.nyf, g.zdf, 19)
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != shape:
+            raise DnsError(DNS_EINVAL, f"state shape {a.shape} != {shape}")
+        _check(lib().dns_batch_import_state(self.h, i, level, a.ctypes.data), "dns_batch_import_state")
 
     def log(self, i: int, first: int = 0, n: int | None = None) -> np.ndarray:
         if n is None:

@@ -286,6 +286,24 @@ extern "C" int dns_batch_set_tile(dns_batch *b, const dns_params *shape, const d
   return DNS_OK;
 }
 
+// encalc2 of the state in buffers (cc, cf) -> the instance's force for its
+// next step, as the single-channel refresh after a seed or an import
+static int refresh_flow(dns_batch *b, const Inst &I, const dns_params &q, const dns_geometry &g, int slot, int cc,
+                        int cf) {
+  const Dims d{g.nx, g.ny, g.nzc, g.nxf, g.nyf, g.zdf, q.zds, g.gr, g.nzs};
+  const DevState st0{I.cfr ? 0.0 : q.force_const, 0., 0., 0.};
+  BTRY(cudaMemcpyAsync(b->dstate + slot, &st0, sizeof st0, cudaMemcpyHostToDevice, b->s));
+  const LaunchShape shp = make_shape(d);
+  double *scratch = nullptr;
+  if (cudaMallocAsync(&scratch, (size_t)flow_sums_pairs(d, shp) * 2 * 8, b->s) != cudaSuccess)
+    return fail_with(DNS_ENOMEM, "flow-sum scratch");
+  PartialLayout pl{};
+  const StepParams sp{g.omega_c, g.omega_f, q.ub, q.force_const, I.cfr, I.den_offset};
+  launch_flow_sums_f32(I.fc[cc], I.ff[cf], b->dstate + slot, scratch, pl, d, shp, sp, b->s);
+  BTRY(cudaFreeAsync(scratch, b->s));
+  return DNS_OK;
+}
+
 extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *tile, uint64_t seed, double uc,
                              double amp, long long steps, long long sample_every, int *id) {
   if (!b || !p || !id || steps < 0 || sample_every < 0) return fail_with(DNS_EINVAL, "bad argument");
@@ -363,21 +381,12 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
   BTRY(cudaMemsetAsync(I.stats, 0, (size_t)I.nzp * 16 * 8, b->s));
   launch_seed_f32(I.fc[0], I.ff[0], I.hist, d, seed, uc, amp, b->s);
   // encalc2 of the seeded state -> force of the first step (as dns_init_seeded)
-  const DevState st0{I.cfr ? 0.0 : q.force_const, 0., 0., 0.};
-  BTRY(cudaMemcpyAsync(b->dstate + slot, &st0, sizeof st0, cudaMemcpyHostToDevice, b->s));
-  const LaunchShape shp = make_shape(d);
-  double *scratch = nullptr;
-  e = cudaMallocAsync(&scratch, (size_t)flow_sums_pairs(d, shp) * 2 * 8, b->s);
-  if (e != cudaSuccess) {
+  if ((rc = refresh_flow(b, I, q, g, slot, 0, 0))) {
     cudaFreeAsync(r.chunk, b->s);
-    return fail_with(DNS_ENOMEM, "flow-sum scratch");
+    return rc;
   }
-  PartialLayout pl{};
-  const StepParams sp{g.omega_c, g.omega_f, q.ub, q.force_const, I.cfr, I.den_offset};
-  launch_flow_sums_f32(I.fc[0], I.ff[0], b->dstate + slot, scratch, pl, d, shp, sp, b->s);
   const Dyn dy0{0, 0, 0, 1, 2, 0, 0, steps};
   BTRY(cudaMemcpyAsync(b->ddyn + slot, &dy0, sizeof dy0, cudaMemcpyHostToDevice, b->s));
-  cudaFreeAsync(scratch, b->s);
   e = cudaStreamSynchronize(b->s);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -581,6 +590,37 @@ extern "C" int dns_batch_export_state(dns_batch *b, int id, int level, double *a
   cudaFreeAsync(stage, b->s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->s);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, cudaGetErrorString(e));
+  return DNS_OK;
+}
+
+extern "C" int dns_batch_import_state(dns_batch *b, int id, int level, const double *aos_in) {
+  Record *r = record_of(b, id);
+  if (!r || !aos_in || level < 0 || level > 2) return fail_with(DNS_EINVAL, "bad argument");
+  BTRY(cudaSetDevice(b->device));
+  Dyn D;
+  BTRY(cudaMemcpyAsync(&D, b->ddyn + r->inst.slot, sizeof D, cudaMemcpyDeviceToHost, b->s));
+  BTRY(cudaStreamSynchronize(b->s));
+  const dns_geometry &g = r->g;
+  const Inst &I = r->inst;
+  const size_t n = level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
+  double *stage = nullptr;
+  BTRY(cudaMallocAsync(&stage, n * 8, b->s));
+  cudaError_t e = cudaMemcpyAsync(stage, aos_in, n * 8, cudaMemcpyHostToDevice, b->s);
+  if (e == cudaSuccess) {
+    if (level == 0)
+      launch_aos_to_dev_f32(stage, I.fc[D.cc], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, b->s);
+    else if (level == 1)
+      launch_aos_to_dev_f32(stage, I.ff[D.cf], g.nxf, g.nyf, 2 * I.zds, 0, I.zds, g.zdf, 1, b->s);
+    else
+      launch_aos_to_dev_f32(stage, I.ff[D.cf], g.nxf, g.nyf, 2 * I.zds, I.zds, I.zds, g.zdf, 0, b->s);
+  }
+  cudaFreeAsync(stage, b->s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->s);
+  if (e != cudaSuccess) return fail_with(DNS_ECUDA, cudaGetErrorString(e));
+  int rc = refresh_flow(b, I, r->p, g, I.slot, D.cc, D.cf);
+  if (rc) return rc;
+  BTRY(cudaStreamSynchronize(b->s));
+  BTRY(cudaGetLastError());
   return DNS_OK;
 }
 

@@ -672,12 +672,41 @@ static std::string cname(const char *dir, const char *base, int cntr) {
   return std::string(dir) + "/" + buf;
 }
 
+// A restart file shorter than its format for this grid is truncated (or was
+// written for a smaller grid).  The reference's MPI-IO reads (main
+// :1003-1163) would return short counts unchecked and run on from stale
+// memory; this load refuses.  A longer file is read like the reference reads
+// it, from the front (its writer opens without truncating, so a file that
+// replaced a larger one keeps the old tail).
+static int check_size(const std::string &fn, size_t n_doubles) {
+  FILE *fp = std::fopen(fn.c_str(), "rb");
+  if (!fp) return fail(DNS_EIO, "cannot open " + fn);
+  long sz = -1;
+  if (std::fseek(fp, 0, SEEK_END) == 0) sz = std::ftell(fp);
+  std::fclose(fp);
+  if (sz < 0) return fail(DNS_EIO, "cannot size " + fn);
+  if ((size_t)sz < n_doubles * 8)
+    return fail(DNS_EIO, fn + " is truncated: " + std::to_string(sz) + " bytes, this grid's file has " +
+                             std::to_string(n_doubles * 8));
+  return DNS_OK;
+}
+
 extern "C" int dns_load_restart(dns_handle *h, const char *dir, int cntr) {
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const dns_geometry &g = h->g;
-  std::vector<double> buf(19ull * std::max((size_t)g.nzc * g.ny * g.nx, (size_t)g.zdf * g.nyf * g.nxf));
   int rc;
+  // every file is sized before anything is imported, so a failed load leaves
+  // the state as it was
+  {
+    const size_t nc = 19ull * g.nzc * g.ny * g.nx, nf = 19ull * g.zdf * g.nyf * g.nxf;
+    const size_t nh = 3ull * g.nx * g.ny * 23;
+    const struct { const char *base; size_t n; } files[6] = {
+        {"lbf-c", 2 * nc}, {"lbf-slf", 2 * nf}, {"lbf-suf", 2 * nf}, {"force", 1}, {"lbf-lin", nh}, {"lbf-uin", nh}};
+    for (const auto &f : files)
+      if ((rc = check_size(cname(dir, f.base, cntr), f.n))) return rc;
+  }
+  std::vector<double> buf(19ull * std::max((size_t)g.nzc * g.ny * g.nx, (size_t)g.zdf * g.nyf * g.nxf));
   // lbf-c: [ftemp | f]; the post-stream state is the first half (:1006-1016)
   if ((rc = read_file(cname(dir, "lbf-c", cntr), buf.data(), 19ull * g.nzc * g.ny * g.nx))) return rc;
   if ((rc = import_level(h, 0, buf.data()))) return rc;

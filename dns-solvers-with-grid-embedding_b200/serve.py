@@ -60,10 +60,10 @@ class Server:
     def footprint(self, inst) -> int:
         return self.pkg.batch_footprint(inst.params(self.pkg))
 
-    def _retire(self, rec: Record, now: float):
+    def _retire(self, rec: Record, now: float, status: int | None = None):
         b = self.batch
         info = b.info(rec.id)
-        rec.status = int(info.status)
+        rec.status = int(info.status) if status is None or info.status != 0 else status
         stats, _ = b.stats(rec.id)
         log = b.log(rec.id)
         if rec.status == 0 and len(log):
@@ -74,10 +74,15 @@ class Server:
         self.used -= rec.bytes
         rec.finished = now
 
-    def run(self, requests, clock=time.perf_counter, sleep=time.sleep):
+    def run(self, requests, clock=time.perf_counter, sleep=time.sleep, deadline: float | None = None):
         """Serve requests (arrival times in seconds from the start); returns
         the records in arrival order.  A request larger than the whole budget
-        is rejected with status DNS_ENOMEM."""
+        is rejected with status DNS_ENOMEM.  An instance whose wall shear
+        stress turns non-finite is retired at once with DNS_ENAN; the others
+        run on unaffected.  With a deadline (seconds from the start), the loop
+        ends at the first step-group boundary past it: resident requests are
+        retired with DNS_ETIMEOUT (the steps they took are reported), queued
+        and later ones get DNS_ETIMEOUT without running."""
         pending = sorted(requests, key=lambda r: r.arrival)
         recs = [Record(inst=r, arrival=r.arrival) for r in pending]
         queue: deque[Record] = deque()
@@ -86,6 +91,13 @@ class Server:
         t0 = clock()
         while nxt < len(recs) or queue or active:
             now = clock() - t0
+            if deadline is not None and now >= deadline:
+                for i in list(active):
+                    self._retire(active.pop(i), now, status=self.pkg.DNS_ETIMEOUT)
+                for rec in list(queue) + recs[nxt:]:
+                    rec.status = self.pkg.DNS_ETIMEOUT
+                    rec.finished = now
+                break
             while nxt < len(recs) and recs[nxt].arrival <= now:
                 queue.append(recs[nxt])
                 nxt += 1
@@ -109,12 +121,14 @@ class Server:
                 active[rec.id] = rec
             if not active:
                 if nxt < len(recs):
-                    sleep(max(0.0, recs[nxt].arrival - (clock() - t0)))
+                    wake = recs[nxt].arrival if deadline is None else min(recs[nxt].arrival, deadline)
+                    sleep(max(0.0, wake - (clock() - t0)))
                 continue
             self.batch.run(self.group)
             now = clock() - t0
             for i in list(active):
-                if self.batch.info(i).remaining == 0:
+                info = self.batch.info(i)
+                if info.remaining == 0 or info.status != 0:
                     self._retire(active.pop(i), now)
         return recs
 

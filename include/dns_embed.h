@@ -298,6 +298,9 @@ int dns_batch_info_of(dns_batch *b, int id, dns_batch_info *out);
 int dns_batch_stats(dns_batch *b, int id, double *out, long *nsamples);
 /* The instance's post-stream state, as dns_export_state. */
 int dns_batch_export_state(dns_batch *b, int id, int level, double *aos_out);
+/* Replace one level of the instance's post-stream state, as dns_import_state
+   (the interface history is kept; the next step's force is recomputed). */
+int dns_batch_import_state(dns_batch *b, int id, int level, const double *aos_in);
 /* Log rows [first, first + n) of the instance (rows of steps taken). */
 int dns_batch_log(dns_batch *b, int id, long long first, long long n, dns_step_log *rows);
 /* The batch's CUDA stream (cudaStream_t as void*): run() is ordered on it, so

@@ -69,17 +69,18 @@ class FakeBatch:
     """Stand-in with the Batch interface: each run(n) advances every instance
     with budget left by up to n steps and moves the virtual clock by n ms."""
 
-    def __init__(self, clock):
+    def __init__(self, clock, fail_at=None):
         self.clock = clock
         self.inst = {}
         self.geoms = {}
         self.nid = 0
         self.resident_max = 0
+        self.fail_at = fail_at or {}  # seed -> step whose wall stress turns non-finite
 
     def add(self, p, steps, seed, uc, amp, sample_every):
         i = self.nid
         self.nid += 1
-        self.inst[i] = dict(steps=steps, done=0, U=p.xdv * p.ydv)
+        self.inst[i] = dict(steps=steps, done=0, U=p.xdv * p.ydv, status=0, fail=self.fail_at.get(seed))
         self.geoms[i] = type("G", (), {"zdf": p.zds + 1})
         self.resident_max = max(self.resident_max, len(self.inst))
         return i
@@ -87,13 +88,18 @@ class FakeBatch:
     def run(self, n):
         self.clock.t += 1e-3 * n
         for v in self.inst.values():
+            if v["status"] != 0:
+                continue
             v["done"] = min(v["steps"], v["done"] + n)
-        return sum(1 for v in self.inst.values() if v["done"] < v["steps"])
+            if v["fail"] is not None and v["done"] >= v["fail"]:
+                # the engine stops the instance after the failing step
+                v["done"], v["status"] = v["fail"], -4
+        return sum(1 for v in self.inst.values() if v["done"] < v["steps"] and v["status"] == 0)
 
     def info(self, i):
         v = self.inst[i]
-        return type("I", (), {"remaining": v["steps"] - v["done"], "steps_done": v["done"], "status": 0,
-                              "updates_per_step": v["U"]})
+        return type("I", (), {"remaining": 0 if v["status"] else v["steps"] - v["done"], "steps_done": v["done"],
+                              "status": v["status"], "updates_per_step": v["U"]})
 
     def stats(self, i):
         s = np.zeros((14, 20))
@@ -119,9 +125,9 @@ class Clock:
         self.t += dt
 
 
-def _server(pkg, budget, fp):
+def _server(pkg, budget, fp, fail_at=None):
     clk = Clock()
-    fb = FakeBatch(clk)
+    fb = FakeBatch(clk, fail_at)
     srv = S.Server(pkg, batch=fb, hbm_budget=budget, group=32)
     srv.footprint = lambda inst: fp[inst.seed]
     return srv, fb, clk
@@ -157,3 +163,43 @@ def test_server_rejects_oversize_and_waits_for_arrivals(pkg):
 def test_fifo_model():
     lat = S.fifo_latencies([0.0, 0.5, 0.6], [1.0, 1.0, 1.0])
     np.testing.assert_allclose(lat, [1.0, 1.5, 2.4])
+
+
+def test_server_retires_a_failed_instance_and_runs_the_rest(pkg):
+    """Fault injected on the host: one request's instance reports a
+    non-finite wall shear stress mid-run; it is retired with DNS_ENAN and its
+    memory released while the co-resident requests finish their budgets."""
+    assert pkg.DNS_ENAN == -4
+    reqs = W.request_stream(rate=100.0, n=6, seed=5, budget=(300, 300))
+    fp = {r.seed: 10 for r in reqs}
+    srv, fb, clk = _server(pkg, budget=100, fp=fp, fail_at={reqs[2].seed: 70})
+    recs = srv.run(reqs, clock=clk, sleep=clk.sleep)
+    bad = recs[2]
+    assert bad.status == pkg.DNS_ENAN and bad.result["steps"] == 70 and "cf" not in bad.result
+    assert bad.finished < max(r.finished for r in recs)  # retired at once, not at the end
+    for r in recs:
+        if r is not bad:
+            assert r.status == 0 and r.result["steps"] == 300
+    assert srv.used == 0 and not fb.inst
+    lat = S.latency_summary(recs)
+    assert lat["completed"] == 5 and lat["failed"] == 1
+
+
+def test_server_deadline_times_out_resident_and_queued(pkg):
+    """A CPU-side timeout of the request loop: past the deadline the resident
+    requests are retired with DNS_ETIMEOUT (their steps so far reported), the
+    queued and later ones are not run, and every byte is released."""
+    reqs = W.request_stream(rate=50.0, n=10, seed=6, budget=(400, 400))
+    fp = {r.seed: 10 for r in reqs}
+    srv, fb, clk = _server(pkg, budget=25, fp=fp)  # two resident at a time
+    recs = srv.run(reqs, clock=clk, sleep=clk.sleep, deadline=0.9)
+    st = [r.status for r in recs]
+    # 400 steps at 1 ms a step take ~0.42 s: two pairs finish before 0.9 s
+    assert st[:4] == [0, 0, 0, 0]
+    assert set(st[4:]) == {pkg.DNS_ETIMEOUT}
+    cut = [r for r in recs if r.status == pkg.DNS_ETIMEOUT and r.result]
+    assert len(cut) == 2 and all(0 < r.result["steps"] < 400 for r in cut)
+    never = [r for r in recs if r.status == pkg.DNS_ETIMEOUT and not r.result]
+    assert len(never) == 4 and all(r.admitted != r.admitted for r in never)  # NaN: not admitted
+    assert all(r.finished >= 0.9 for r in recs[4:])
+    assert srv.used == 0 and not fb.inst
