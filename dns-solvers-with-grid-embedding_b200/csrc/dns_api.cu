@@ -223,6 +223,14 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   if (p->fltr && (p->gratio != 4 || p->zds < 7))
     return fail(DNS_EINVAL,
                 "the filtered transfer (FLTR) needs gratio 4 (the reference's 5-plane stencil array) and zds >= 7");
+  // the kernels index one population array with 32-bit offsets: every
+  // population array (coarse nzc x ny x nx, fine 2 zds x nyf x nxf) must hold
+  // fewer than 2^31 nodes (a bound HBM reaches first: 2^31 nodes are 326 GB of
+  // FP64 populations per lattice)
+  if ((long long)p->gratio * p->xdv > (1LL << 20) || (long long)p->gratio * p->ydv > (1LL << 20) ||
+      (long long)p->zdv * p->ydv * p->xdv >= (1LL << 31) ||
+      2LL * p->zds * p->gratio * p->ydv * p->gratio * p->xdv >= (1LL << 31))
+    return fail(DNS_EINVAL, "grid too large: a population array must hold fewer than 2^31 nodes");
   std::memset(g, 0, sizeof(*g));
   const int GR = p->gratio;
   g->gr = GR;

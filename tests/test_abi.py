@@ -95,7 +95,10 @@ def test_geometry_matches_reference_formulas(pkg, port, ref_configs):
 @pytest.mark.parametrize("bad", [dict(gratio=1), dict(zds=2), dict(zdv=3), dict(xdv=2), dict(Rebs=-1.0),
                                  dict(pattern=9), dict(precision=7), dict(fltr=2),
                                  dict(fltr=1),                       # FLTR is defined for gratio 4
-                                 dict(fltr=1, gratio=4, zds=6)])     # and needs zds >= 7
+                                 dict(fltr=1, gratio=4, zds=6),      # and needs zds >= 7
+                                 dict(xdv=1 << 20),                  # 32-bit population offsets
+                                 dict(xdv=1 << 14, ydv=1 << 14, zdv=16),
+                                 dict(xdv=1 << 14, ydv=1 << 12, zds=16)])
 def test_invalid_parameters_are_rejected(pkg, bad):
     p = pkg.make_params(xdv=16, ydv=16, zdv=9, zds=6, gratio=2)
     for k, v in bad.items():
