@@ -499,8 +499,10 @@ def run_ours(args, rank, world, local_rank):
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded laminar profile + noise)",
         "config": {"workload": args.config, "description": desc, "updates_per_step": U,
-                   "l2": "state 2.1 GB >> 126 MB L2 (no flush needed)" if args.config != "c1"
-                   else "state smaller than needed to defeat L2", "parallelism": f"replicas x{world}"},
+                   "l2": (f"state {geom.device_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)"
+                          if geom.device_bytes > 8 * 126e6 else
+                          f"state {geom.device_bytes / 1e9:.2f} GB: not enough to defeat L2"),
+                   "parallelism": f"replicas x{world}"},
         "roofline": {"bound": "hbm", "kernel": "fine_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
