@@ -1473,7 +1473,7 @@ extern "C" const char *dns_error_string(int code) {
     case DNS_ENOMEM: return "out of memory";
     case DNS_EIO: return "i/o error";
     case DNS_ENAN: return "non-finite wall shear stress";
-    case DNS_ETIMEOUT: return "device wait timed out";
+    case DNS_ETIMEOUT: return "wait timed out";
     case DNS_ECUDA: return "CUDA error";
     default: return "unknown error";
   }

@@ -34,7 +34,7 @@ extern "C" {
 #define DNS_ENOMEM (-2)   /* device or host allocation failed / over budget */
 #define DNS_EIO (-3)      /* restart or output file missing, short or unwritable */
 #define DNS_ENAN (-4)     /* non-finite wall shear stress (reference aborts) */
-#define DNS_ETIMEOUT (-5) /* a bounded device wait gave up */
+#define DNS_ETIMEOUT (-5) /* a bounded wait gave up (the request loop's deadline) */
 #define DNS_ECUDA (-6)    /* CUDA runtime error */
 
 enum dns_pattern { DNS_PATTERN_NONE = 0, DNS_PATTERN_RSLIP = 1, DNS_PATTERN_PSLIP = 2, DNS_PATTERN_SSLIP = 3 };

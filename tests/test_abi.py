@@ -112,3 +112,29 @@ def test_error_strings(pkg):
     lib = pkg.lib()
     for code in (0, -1, -2, -3, -4, -5, -6):
         assert lib.dns_error_string(code)
+
+
+def test_python_structs_match_the_header_layout(pkg, tmp_path):
+    """The ctypes mirrors have the C structs' sizes and field offsets (a
+    program built with gcc against include/dns_embed.h prints them)."""
+    pairs = [("dns_params", pkg.Params), ("dns_geometry", pkg.Geometry), ("dns_step_log", pkg.StepLog),
+             ("dns_tile", pkg.Tile), ("dns_batch_info", pkg.BatchInfo)]
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "dns_embed.h"', "int main(void) {"]
+    for cname, py in pairs:
+        lines.append(f'  printf("{cname} sizeof %zu\\n", sizeof({cname}));')
+        for fname, _ in py._fields_:
+            lines.append(f'  printf("{cname} {fname} %zu\\n", offsetof({cname}, {fname}));')
+    lines += ["  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-I", str(HEADER.parent), str(src), "-o", str(exe)],
+                   check=True)
+    got = {}
+    for ln in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines():
+        cname, key, val = ln.split()
+        got[(cname, key)] = int(val)
+    for cname, py in pairs:
+        assert got[(cname, "sizeof")] == C.sizeof(py), cname
+        for fname, _ in py._fields_:
+            assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
