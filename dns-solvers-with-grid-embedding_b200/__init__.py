@@ -122,6 +122,7 @@ def lib() -> C.CDLL:
         "dns_export_state": (I, [P, I, P]),
         "dns_import_state": (I, [P, I, P]),
         "dns_export_history": (I, [P, P]),
+        "dns_import_history": (I, [P, P]),
         "dns_get_force": (I, [P, C.POINTER(D)]),
         "dns_step": (I, [P, C.c_long, P]),
         "dns_set_sampling": (I, [P, C.c_long]),
@@ -267,6 +268,13 @@ class Channel:
         out = np.empty((3, 2, g.nx, g.ny, 23), dtype=np.float64)
         _check(lib().dns_export_history(self.h, out.ctypes.data), "dns_export_history")
         return out
+
+    def import_history(self, arr: np.ndarray):
+        g = self.geom
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != (3, 2, g.nx, g.ny, 23):
+            raise DnsError(DNS_EINVAL, f"history shape {a.shape} != {(3, 2, g.nx, g.ny, 23)}")
+        _check(lib().dns_import_history(self.h, a.ctypes.data), "dns_import_history")
 
     def force(self) -> float:
         f = C.c_double()

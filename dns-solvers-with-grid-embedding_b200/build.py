@@ -1,4 +1,5 @@
-"""Build the CUDA library ``libdnsembed.so`` in-tree for sm_100a.
+"""Build the CUDA library ``libdnsembed.so`` in-tree for sm_100a, and the host
+driver ``dns_run`` (plain C over the library's C ABI).
 
 ``kernels_f64.cu`` is compiled with ``-fmad=false``: the FP64 plain form must
 not fuse multiply-adds, so that its per-node arithmetic rounds exactly like the
@@ -15,6 +16,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libdnsembed.so"
+DRIVER = HERE / "dns_run"
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -64,6 +66,13 @@ def build(verbose: bool = False) -> Path:
         objs.append(obj)
     if _stale(OUT, objs):
         cmd = [nvcc] + ARCH + ["-shared", "-o", str(OUT)] + [str(o) for o in objs] + ["-lcudart"]
+        if verbose:
+            print(" ".join(cmd))
+        subprocess.run(cmd, check=True)
+    # the host driver (C, against the C ABI only), found next to the library
+    if _stale(DRIVER, [CSRC / "dns_run.c", INCLUDE / "dns_embed.h", OUT]):
+        cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-Werror", "-I", str(INCLUDE), str(CSRC / "dns_run.c"),
+               "-o", str(DRIVER), "-L", str(HERE), "-ldnsembed", "-Wl,-rpath,$ORIGIN", "-lm"]
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)

@@ -629,6 +629,12 @@ extern "C" int dns_export_history(dns_handle *h, double *out) {
   return export_history(h, out);
 }
 
+extern "C" int dns_import_history(dns_handle *h, const double *in) {
+  if (!h || !in) return fail(DNS_EINVAL, "bad argument");
+  CUDA_TRY(cudaSetDevice(h->p.device));
+  return import_history(h, in);
+}
+
 extern "C" int dns_get_force(dns_handle *h, double *force) {
   if (!h || !force) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));

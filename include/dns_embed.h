@@ -171,8 +171,12 @@ int dns_write_tke_budget(const dns_params *p, const char *dir, int cntr, const d
    ((GR xdv), (GR ydv), zdf, 19).  out must hold that many doubles. */
 int dns_export_state(dns_handle *h, int level, double *aos_out);
 int dns_import_state(dns_handle *h, int level, const double *aos_in);
-/* Interface history [3 levels n,p,pp][2 walls lower,upper][xdv][ydv][23]. */
+/* Interface history [3 levels n,p,pp][2 walls lower,upper][xdv][ydv][23] of
+   fields [rho, u_x, u_y, u_z, fneq_0..18], as lbf-lin / lbf-uin hold it
+   (main :1078-1135).  Importing all zeros leaves the history as main's mode s
+   does (it never sets it). */
 int dns_export_history(dns_handle *h, double *out);
+int dns_import_history(dns_handle *h, const double *in);
 /* Field output as the reference's vel_print.c:15-275 (main :1342): vel-c,
    vel-slf, vel-suf (nx, ny, nz, 3) and den-c, den-slf, den-suf (nx, ny, nz),
    counter cntr, of the post-stream state; the FP64 form writes the

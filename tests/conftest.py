@@ -73,3 +73,21 @@ def gpu_available() -> bool:
         return torch.cuda.is_available()
     except Exception:
         return False
+
+
+def write_definitions(m: dict, path: Path, **over) -> Path:
+    """A reference-style definitions.h (#define NAME value lines) with the
+    macros of an oracle configuration, as the host driver reads it."""
+    m = dict(m, **over)
+    lines = []
+    for k in ("Rebs", "ub", "zdv", "ydv", "xdv", "TSTR", "TEND", "CFL", "gratio", "zds", "gyplussize",
+              "wyplussize", "gxplussize", "wxplussize", "XDIM", "YDIM", "xdu", "ydu", "zdu"):
+        if k in m:
+            lines.append(f"#define {k} {m[k]}")
+    if m.get("ITER") is not None:
+        lines.append(f"#define ITER {int(m['ITER'])}")
+    if m.get("pattern"):
+        lines.append(f"#define {m['pattern']}")
+    lines.append("#define FLTR" if m.get("fltr") else "#define NOFLTR")
+    path.write_text("\n".join(lines) + "\n")
+    return path

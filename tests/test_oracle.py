@@ -130,6 +130,36 @@ def test_port_matches_compiled_reference(port, ref_configs, tmp_path, name, mode
         np.testing.assert_array_equal(h[:, w].reshape(-1), np.fromfile(dout / f"{fn}.0004"))
 
 
+@pytest.mark.parametrize("name", ["t_noslip", "t_ridges", "t_gr4"])
+def test_port_log_rows_match_reference_text_logs(port, ref_configs, tmp_path, name):
+    """The per-step log values (force-derived p-grad included) against the text
+    logs the reference's own encalc2 / wshearstr append (flowrate.txt,
+    density.txt: encalc2.c:135-144; str-up, str-do, w-str, p-grad:
+    wshearstr.c:145-166), which print 12 decimals."""
+    exe = ref_binary(name)
+    if exe is None:
+        pytest.skip("compiled reference not available (reference tree not mounted)")
+    p = port.Port(ref_configs[name])
+    p.init_seeded(42, 0.05, 0.005, 0.0)
+    p.set_forcing(True)
+    din, dout = tmp_path / "in", tmp_path / "out"
+    din.mkdir()
+    dout.mkdir()
+    p.save(din, 100)
+    subprocess.run([str(exe), str(din), "100", str(dout), "-1", "10", "cfr"], check=True, capture_output=True)
+    rows = p.step(10)  # force momentum denst flowrate stup stdown stress pgrad
+    for fn, col in (("flowrate.txt", 3), ("density.txt", 2), ("str-up.txt", 4), ("str-do.txt", 5),
+                    ("w-str.txt", 6), ("p-grad.txt", 7)):
+        t = np.loadtxt(dout / fn)
+        assert t.shape == (10, 2), fn
+        np.testing.assert_allclose(t[:, 1], rows[:, col], rtol=0, atol=5.01e-13, err_msg=fn)
+    # the time stamps TM + dt ss with dt = GR / (0.5 (NZs - 2) / CFL)
+    _, _, nzs = p.params()
+    m = ref_configs[name]
+    dt = m["gratio"] * 1.0 / (0.5 * (nzs - 2.0) / m["CFL"])
+    np.testing.assert_allclose(t[:, 0], 100 + dt * np.arange(10), rtol=0, atol=5.01e-7)
+
+
 @pytest.mark.parametrize("name", ["t_noslip", "t_ridges", "t_gr4f"])
 def test_port_matches_reference_main(port, ref_configs, tmp_path, name):
     """Pin against the unmodified reference main program (mode -p, ITER = 50,
