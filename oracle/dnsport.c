@@ -945,6 +945,15 @@ long port_export_history(const port_state *s, double *out) {
   return (long)(3 * per);
 }
 
+/* the inverse of port_export_history; all zeros leaves the history as main's
+   mode s does (dns-q-mgrd-all-patterns-xyc.c:961-977 never sets it) */
+void port_import_history(port_state *s, const double *in) {
+  size_t per = (size_t)2 * s->nx * s->ny * 23;
+  memcpy(s->hist[s->hn], in, per * sizeof(double));
+  memcpy(s->hist[s->hp], in + per, per * sizeof(double));
+  memcpy(s->hist[s->hpp], in + 2 * per, per * sizeof(double));
+}
+
 /* ------------------------------------------------------------ statistics */
 /* statistics.c:48-300: per-plane means, then rms of the deviation from the
    plane mean, over the composite profile of NZ = 2 zdf + zdc - 4 planes */

@@ -62,6 +62,7 @@ void port_step(port_state *s, long n, port_log *log);
 /* S (post-stream state) in reference AoS order; level 0 coarse, 1 lower, 2 upper */
 long port_export(const port_state *s, int level, double *out);
 long port_export_history(const port_state *s, double *out); /* [3][2][xdv][ydv][23] */
+void port_import_history(port_state *s, const double *in);
 double port_force(const port_state *s);
 /* instantaneous plane statistics exactly as reference statistics.c:
    out[9][NZ] = UAVG VAVG WAVG UTIN VTIN WTIN REYS DAVG DTIN, NZ = 2 zdf + zdc - 4 */

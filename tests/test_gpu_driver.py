@@ -8,7 +8,11 @@ write restart files at counters 100 and 150, field and statistics files at
 every counter and the six per-step text logs.  Every such file of the
 reference has a counterpart from dns_run with the same name and layout; the
 values agree to the constant-flow-rate tolerance (the force is summed in
-another order on the device, 1e-12 relative on the populations).
+another order on the device, 1e-12 relative on the populations).  In mode -i
+only the start is compared: the reference's inter_init slips (not
+reproduced) make the two runs part after it.  tests/test_driver.py makes the
+same comparisons on the host, bit for bit, with the channel held by the
+oracle.
 """
 from __future__ import annotations
 
@@ -46,14 +50,18 @@ def _close(x, y, rtol, atol, what):
     np.testing.assert_allclose(x, y, rtol=rtol, atol=atol, err_msg=what)
 
 
-def _compare_dirs(a, b):
+def _compare_dirs(a, b, first_only=False):
     """Every restart, field and statistics file of the reference run (a) has
-    a counterpart in b that agrees; the per-step logs agree line by line."""
+    a counterpart in b that agrees; the per-step logs agree line by line.
+    first_only: contents of what iteration 0 writes (files of counter 100, the
+    first log line) only."""
     names = sorted(p.name for p in a.iterdir()
                    if p.name.startswith(("lbf-", "force.", "vel-", "den-", "turb-fld.")))
     assert any(n.startswith("lbf-c.") for n in names) and any(n.startswith("vel-") for n in names)
     for n in names:
         assert (b / n).exists(), n
+        if first_only and (not n.endswith((".0100", ".100")) or n.startswith(("lbf-lin.", "lbf-uin."))):
+            continue
         x, y = np.fromfile(b / n), np.fromfile(a / n)
         if n.startswith(("lbf-c.", "lbf-slf.", "lbf-suf.")):
             # [ftemp | f]: the first half is the state; the reference's second
@@ -69,13 +77,15 @@ def _compare_dirs(a, b):
         la = (a / n).read_text().splitlines()
         lb = (b / n).read_text().splitlines()
         assert len(la) == len(lb) == 51, n
+        if first_only:
+            la, lb = la[:1], lb[:1]
         ta = [ln.split()[0] for ln in la]
         tb = [ln.split()[0] for ln in lb]
         assert ta == tb, n
         va = np.array([float(ln.split()[1]) for ln in la])
         vb = np.array([float(ln.split()[1]) for ln in lb])
         _close(vb, va, 1e-10, 2e-12, n)
-    for n in ("uavg-temp.dat", "uavg-exact-lam.dat"):
+    for n in ("uavg-temp.dat", "uavg-exact-lam.dat")[first_only:]:
         _close(np.loadtxt(b / n), np.loadtxt(a / n), 1e-9, 2e-12, n)
 
 
@@ -117,7 +127,10 @@ def test_mode_i_matches_reference_main(port, ref_configs, tmp_path):
     for d in (a, b):
         port.write_uniform_file(d / f"lbf.{tstr:04d}", first, second)
     _run_both(exe, m, "i", a, b)
-    _compare_dirs(a, b)
+    # the reference's inter_init fills the interface history with two slips
+    # that are not reproduced (test_oracle.py pins them), so the runs part
+    # after the start: the start itself and the file set are compared
+    _compare_dirs(a, b, first_only=True)
 
 
 def test_fp32_driver_run_tracks_fp64(pkg, ref_configs, tmp_path):
