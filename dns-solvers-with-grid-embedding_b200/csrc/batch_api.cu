@@ -484,6 +484,7 @@ static int absorb(dns_batch *b, int q) {
 }
 
 extern "C" int dns_batch_run(dns_batch *b, long long nsteps, int *active) {
+  Range range("dns_batch_run");
   if (!b || nsteps < 0) return fail_with(DNS_EINVAL, "bad argument");
   BTRY(cudaSetDevice(b->device));
   int rc;

@@ -646,6 +646,7 @@ extern "C" int dns_get_force(dns_handle *h, double *force) {
 }
 
 extern "C" int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double amp) {
+  Range range("dns_init_seeded");
   if (!h) return fail(DNS_EINVAL, "null handle");
   CUDA_TRY(cudaSetDevice(h->p.device));
   h->cur_c = 0;
@@ -706,6 +707,7 @@ static int check_size(const std::string &fn, size_t n_doubles) {
 }
 
 extern "C" int dns_load_restart(dns_handle *h, const char *dir, int cntr) {
+  Range range("dns_load_restart");
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const dns_geometry &g = h->g;
@@ -768,6 +770,7 @@ static int write_file(const std::string &fn, const double *a, size_t n, int copi
 }
 
 extern "C" int dns_write_restart(dns_handle *h, const char *dir, int cntr) {
+  Range range("dns_write_restart");
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const dns_geometry &g = h->g;
@@ -830,6 +833,7 @@ static void wall_plane_fields(const std::vector<double> &wall, size_t n, double 
 // native doubles.  The moments are formed on the device (4 of the 19 values per
 // node cross to the host); the wall planes, kept on the host, are done here.
 extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
+  Range range("dns_write_fields");
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const dns_geometry &g = h->g;
@@ -942,6 +946,7 @@ static int fields_planar(dns_handle *h, double *const q[3]) {
 }
 
 extern "C" int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *vfl) {
+  Range range("dns_tke_budget");
   if (!h || !prof) return fail(DNS_EINVAL, "bad argument");
   int rc = tke_validate(h->p);
   if (rc) return rc;
@@ -975,6 +980,7 @@ extern "C" int dns_tke_budget(dns_handle *h, double *prof, double *ufl, double *
 // GR xdv) x-planes; the reference reads its x-halo planes from the same files)
 extern "C" int dns_tke_budget_files(const dns_params *p, const char *dir, int cntr, double *prof, double *ufl,
                                     double *vfl) {
+  Range range("dns_tke_budget_files");
   if (!p || !dir || !prof) return fail(DNS_EINVAL, "bad argument");
   dns_geometry g;
   int rc = dns_geometry_of(p, &g);
@@ -1113,6 +1119,7 @@ static void rotate_history(dns_handle *h) {
 // writes the upper plane's density and velocity into the lower history
 // (inter_init.c:202-205); neither slip is reproduced.
 extern "C" int dns_load_uniform(dns_handle *h, const char *dir, int cntr) {
+  Range range("dns_load_uniform");
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   const dns_params &p = h->p;
   if (p.xdu < 1 || p.ydu < 1 || p.zdu < 1) return fail(DNS_EINVAL, "xdu, ydu and zdu must be positive");
@@ -1271,6 +1278,7 @@ static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
 }
 
 extern "C" int dns_step(dns_handle *h, long ncoarse, dns_step_log *log) {
+  Range range("dns_step");
   if (!h || ncoarse < 0) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const double dt = h->g.gr * 1. / ((double)(0.5 * (h->g.nzs - 2.) / h->p.CFL));
@@ -1378,6 +1386,7 @@ extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
 // instantaneous plane statistics exactly as statistics.c:48-300 (two passes over
 // the exported state, same summation order)
 extern "C" int dns_plane_stats(dns_handle *h, double *out) {
+  Range range("dns_plane_stats");
   if (!h || !out) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
   const dns_geometry &g = h->g;

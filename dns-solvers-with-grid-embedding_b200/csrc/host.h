@@ -6,9 +6,21 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/dns_embed.h"
 
 namespace dns {
+
+// NVTX range around one ABI call, so that a profiler's timeline (nsys, ncu
+// --nvtx) groups the kernels of a step, a batch run or a file operation; a
+// no-op when no tool is attached
+struct Range {
+  explicit Range(const char *name) { nvtxRangePushA(name); }
+  ~Range() { nvtxRangePop(); }
+  Range(const Range &) = delete;
+  Range &operator=(const Range &) = delete;
+};
 
 // wall-plane flags [nyf][nxf] of the pattern in p (-1 solid, -2 slip)
 std::vector<int8_t> wall_flags(const dns_params &p, const dns_geometry &g);
