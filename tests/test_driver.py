@@ -8,6 +8,7 @@ from __future__ import annotations
 
 import subprocess
 
+import numpy as np
 import pytest
 
 from conftest import PKG_NAME, ROOT, gpu_available, write_definitions
@@ -157,3 +158,34 @@ def test_driver_files_equal_reference_main(fake_lib, port, ref_configs, tmp_path
     names = same_files(a, b, first_only=(mode == "i"))
     assert {"flowrate.txt", "w-str.txt", "p-grad.txt", "uavg-temp.dat", "lbf-c.0150", "force.0150"} <= set(names)
     assert "Total computational time is:" in (b / "report.code").read_text()
+
+
+def test_non_finite_stress_ends_the_run_as_the_reference_does(fake_lib, port, ref_configs, tmp_path):
+    """A NaN population next to the lower wall: both programs stop at the
+    first step with exit status 1, after the flow-rate and density logs of
+    that step and before its wall-stress logs (wshearstr.c:139-143)."""
+    from conftest import ref_binary
+
+    exe = ref_binary("t_noslip", "ref_main")
+    if exe is None:
+        pytest.skip("compiled reference main not available")
+    m = ref_configs["t_noslip"]
+    a, b = tmp_path / "reference", tmp_path / "driver"
+    a.mkdir()
+    b.mkdir()
+    p = port.Port(m)
+    p.init_seeded(42, 0.05, 0.005, 0.0)
+    p.set_forcing(True)
+    for d in (a, b):
+        p.save(d, 100)
+        f = np.fromfile(d / "lbf-slf.0100")
+        f[((3 * p.nyf + 3) * p.zdf + 2) * 19 + 5] = np.nan
+        f.tofile(d / "lbf-slf.0100")
+    ra = subprocess.run([str(exe), "-p"], cwd=a, capture_output=True, text=True)
+    write_definitions(m, b / "definitions.h")
+    rb = run_on_fake(fake_lib, ["-p"], b)
+    assert ra.returncode != 0 and rb.returncode == 1 and "NAN in wall shear stress" in rb.stderr
+    for n in ("flowrate.txt", "density.txt"):
+        assert (b / n).read_text() == (a / n).read_text() and len((b / n).read_text().splitlines()) == 1
+    for n in ("str-up.txt", "str-do.txt", "w-str.txt", "p-grad.txt"):
+        assert not (a / n).exists() and not (b / n).exists()
