@@ -1,5 +1,6 @@
 """Build the CUDA library ``libdnsembed.so`` in-tree for sm_100a, and the host
-driver ``dns_run`` (plain C over the library's C ABI).
+programs ``dns_run`` (the solver) and ``dns_budget`` (the budget analysis),
+plain C over the library's C ABI.
 
 ``kernels_f64.cu`` is compiled with ``-fmad=false``: the FP64 plain form must
 not fuse multiply-adds, so that its per-node arithmetic rounds exactly like the
@@ -16,7 +17,7 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / "csrc"
 OUT = HERE / "libdnsembed.so"
-DRIVER = HERE / "dns_run"
+PROGRAMS = (HERE / "dns_run", HERE / "dns_budget")
 INCLUDE = HERE.parent / "include"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -69,13 +70,15 @@ def build(verbose: bool = False) -> Path:
         if verbose:
             print(" ".join(cmd))
         subprocess.run(cmd, check=True)
-    # the host driver (C, against the C ABI only), found next to the library
-    if _stale(DRIVER, [CSRC / "dns_run.c", INCLUDE / "dns_embed.h", OUT]):
-        cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-Werror", "-I", str(INCLUDE), str(CSRC / "dns_run.c"),
-               "-o", str(DRIVER), "-L", str(HERE), "-ldnsembed", "-Wl,-rpath,$ORIGIN", "-lm"]
-        if verbose:
-            print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
+    # the host programs (C, against the C ABI only), found next to the library
+    for exe in PROGRAMS:
+        src = CSRC / (exe.name + ".c")
+        if _stale(exe, [src, INCLUDE / "dns_embed.h", OUT]):
+            cmd = ["gcc", "-O2", "-std=c11", "-Wall", "-Werror", "-I", str(INCLUDE), str(src), "-o", str(exe),
+                   "-L", str(HERE), "-ldnsembed", "-Wl,-rpath,$ORIGIN", "-lm"]
+            if verbose:
+                print(" ".join(cmd))
+            subprocess.run(cmd, check=True)
     return OUT
 
 

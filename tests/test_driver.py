@@ -189,3 +189,32 @@ def test_non_finite_stress_ends_the_run_as_the_reference_does(fake_lib, port, re
         assert (b / n).read_text() == (a / n).read_text() and len((b / n).read_text().splitlines()) == 1
     for n in ("str-up.txt", "str-do.txt", "w-str.txt", "p-grad.txt"):
         assert not (a / n).exists() and not (b / n).exists()
+
+
+# ---- dns_budget, the budget program (host-only parts)
+BUDGET = ROOT / PKG_NAME / "dns_budget"
+
+
+def test_budget_program_arguments_and_plan(ref_configs, tmp_path):
+    if not BUDGET.exists():
+        pytest.skip("dns_budget is not built")
+    r = subprocess.run([str(BUDGET), "-x"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 2 and "usage: dns_budget" in r.stderr
+    m = dict(ref_configs["c1"])
+    defs = write_definitions(m, tmp_path / "definitions.h", TSTR=150, TEND=420)
+    defs.write_text(defs.read_text() + "#define DT 50\n")
+    r = subprocess.run([str(BUDGET), "--plan"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    # budget-no-slip-mgrd.c: tst = TSTR .. TEND step DT, the fluctuation plane when tst % 200 == 0
+    assert r.stdout.splitlines() == ["0150 budget", "0200 budget fluctuation-plane", "0250 budget", "0300 budget",
+                                     "0350 budget", "0400 budget fluctuation-plane"]
+
+
+def test_budget_program_reports_a_failed_snapshot(ref_configs, tmp_path):
+    """No vel-* / den-* files (and, here, no GPU): status 1, the snapshot named."""
+    if not BUDGET.exists():
+        pytest.skip("dns_budget is not built")
+    write_definitions(ref_configs["t_odd"], tmp_path / "definitions.h", TEND=ref_configs["t_odd"]["TSTR"])
+    r = subprocess.run([str(BUDGET)], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 1 and "snapshot 0100" in r.stderr
+    assert not any(tmp_path.glob("turb-fld-2d.*"))

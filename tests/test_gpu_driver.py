@@ -158,3 +158,40 @@ def test_fp32_driver_run_tracks_fp64(pkg, ref_configs, tmp_path):
         v64 = np.loadtxt(a / n)[:, 1]
         v32 = np.loadtxt(b / n)[:, 1]
         np.testing.assert_allclose(v32, v64, rtol=0, atol=1e-3 * np.max(np.abs(v64)), err_msg=n)
+
+
+BUDGET = ROOT / PKG_NAME / "dns_budget"
+
+
+@pytest.mark.parametrize("name", ["t_odd", "c1"])
+def test_budget_program_matches_reference_program(pkg, ref_configs, tmp_path, name):
+    """dns_budget and the reference's budget program (TKE-budget/computations,
+    compiled unmodified) on the same vel-* / den-* snapshot: the three profile
+    files within 1e-11 of each profile's scale (test_gpu_tke.py's bar), the
+    fluctuation planes where the counter is a multiple of 200."""
+    exe = ref_binary(name, "tke_budget")
+    if exe is None or not BUDGET.exists():
+        pytest.skip("compiled reference budget program or dns_budget not available")
+    m = ref_configs[name]
+    cntr = int(m["TSTR"])
+    a, b = _dirs(tmp_path)
+    ch = pkg.Channel(params_for(pkg, m, "cfr"))
+    ch.init_seeded(42, 0.05, 0.005)
+    ch.step(6)
+    for d in (a, b):
+        ch.write_fields(d, cntr)
+    ch.close()
+    subprocess.run([str(exe)], cwd=a, check=True, capture_output=True, timeout=600)
+    write_definitions(m, b / "definitions.h", TEND=cntr)
+    r = subprocess.run([str(BUDGET)], cwd=b, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    for fname, n in pkg.TKE_FILES:
+        x = np.fromfile(b / f"{fname}.000.{cntr:04d}").reshape(n, -1)
+        y = np.fromfile(a / f"{fname}.000.{cntr:04d}").reshape(n, -1)
+        for row in range(n):
+            scale = float(np.max(np.abs(y[row])))
+            np.testing.assert_allclose(x[row], y[row], rtol=0, atol=1e-11 * scale + 1e-300, err_msg=f"{fname} {row}")
+    if cntr % 200 == 0:
+        for fn in ("ufl4", "vfl4"):
+            np.testing.assert_allclose(np.fromfile(b / f"{fn}.{cntr:04d}"), np.fromfile(a / f"{fn}.{cntr:04d}"),
+                                       rtol=0, atol=1e-15, err_msg=fn)
