@@ -110,26 +110,52 @@ static char *path_in(const char *dir, const char *name) {
   return p;
 }
 
-static int append_line(const char *dir, const char *name, double t, double v) {
-  char *p = path_in(dir, name);
-  FILE *fp = p ? fopen(p, "a") : NULL;
-  free(p);
-  if (!fp) return -1;
+/* the six per-step logs (encalc2.c:135-144, wshearstr.c:145-166), each
+   opened in append mode at its first line and kept open for the run */
+static const char *const kLogNames[6] = {"flowrate.txt", "density.txt", "str-up.txt",
+                                         "str-do.txt",   "w-str.txt",   "p-grad.txt"};
+typedef struct {
+  const char *dir;
+  FILE *fp[6];
+} logs;
+
+static int log_line(logs *L, int which, double t, double v) {
+  if (!L->fp[which]) {
+    char *p = path_in(L->dir, kLogNames[which]);
+    L->fp[which] = p ? fopen(p, "a") : NULL;
+    free(p);
+    if (!L->fp[which]) return -1;
+  }
   /* encalc2.c:138, wshearstr.c:149 */
-  const int ok = fprintf(fp, "%f %.12f\n", t, v) > 0;
-  return (fclose(fp) == 0 && ok) ? 0 : -1;
+  return fprintf(L->fp[which], "%f %.12f\n", t, v) > 0 ? 0 : -1;
 }
 
-/* the six per-step logs of one row */
-static int append_logs(const char *dir, const dns_step_log *r) {
+static int append_logs(logs *L, const dns_step_log *r) {
   int rc = 0;
-  rc |= append_line(dir, "flowrate.txt", r->time, r->flowrate);
-  rc |= append_line(dir, "density.txt", r->time, r->denst);
+  rc |= log_line(L, 0, r->time, r->flowrate);
+  rc |= log_line(L, 1, r->time, r->denst);
   if (!isfinite(r->stress)) return rc; /* the reference aborts before the wall logs */
-  rc |= append_line(dir, "str-up.txt", r->time, r->stup);
-  rc |= append_line(dir, "str-do.txt", r->time, r->stdown);
-  rc |= append_line(dir, "w-str.txt", r->time, r->stress);
-  rc |= append_line(dir, "p-grad.txt", r->time, r->pgrad);
+  rc |= log_line(L, 2, r->time, r->stup);
+  rc |= log_line(L, 3, r->time, r->stdown);
+  rc |= log_line(L, 4, r->time, r->stress);
+  rc |= log_line(L, 5, r->time, r->pgrad);
+  return rc;
+}
+
+static int flush_logs(logs *L) {
+  int rc = 0;
+  for (int q = 0; q < 6; q++)
+    if (L->fp[q] && fflush(L->fp[q]) != 0) rc = -1;
+  return rc;
+}
+
+static int close_logs(logs *L) {
+  int rc = 0;
+  for (int q = 0; q < 6; q++)
+    if (L->fp[q]) {
+      if (fclose(L->fp[q]) != 0) rc = -1;
+      L->fp[q] = NULL;
+    }
   return rc;
 }
 
@@ -306,6 +332,7 @@ int main(int argc, char **argv) {
     fprintf(stderr, "dns_run: out of host memory\n");
     return 1;
   }
+  logs L = {o.dir, {NULL, NULL, NULL, NULL, NULL, NULL}};
   const double t0 = now_seconds();
   int status = 0;
   for (long ss = 0; ss <= up && !status;) {
@@ -325,11 +352,9 @@ int main(int argc, char **argv) {
       while (done < n && isfinite(rows[done].stress)) done++;
       if (done < n) done++; /* the failing step's flow-rate logs are written, as encalc2 runs first */
     }
-    for (long q = 0; q < done; q++)
-      if (append_logs(o.dir, &rows[q])) {
-        status = fail_call("appending the logs", DNS_EIO);
-        break;
-      }
+    for (long q = 0; q < done && !status; q++)
+      if (append_logs(&L, &rows[q])) status = fail_call("appending the logs", DNS_EIO);
+    if (!status && flush_logs(&L)) status = fail_call("appending the logs", DNS_EIO);
     if (!status && rc == DNS_ENAN) {
       fprintf(stderr, "Error: NAN in wall shear stress (step %ld)\n", ss + done - 1);
       status = 1;
@@ -338,6 +363,7 @@ int main(int argc, char **argv) {
     }
     ss += n;
   }
+  if (close_logs(&L) && !status) status = fail_call("closing the logs", DNS_EIO);
   const double seconds = now_seconds() - t0;
   if (!status && write_statistics(h, &p, &g, o.dir, (long)p.TSTR + (up + 1) / ut))
     status = fail_call("writing the statistics", DNS_EIO);
