@@ -346,7 +346,7 @@ int main(int argc, char **argv) {
     /* steps up to the next output boundary (or the end of the loop) in one call */
     const long n = (up + 1 - ss) < (ut - ss % ut) ? (up + 1 - ss) : (ut - ss % ut);
     rc = dns_step(h, n, rows);
-    long done = n;
+    long done = rc == DNS_OK ? n : 0; /* any other failure leaves the rows unset */
     if (rc == DNS_ENAN) {
       done = 0;
       while (done < n && isfinite(rows[done].stress)) done++;
