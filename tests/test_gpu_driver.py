@@ -174,13 +174,13 @@ def test_budget_program_matches_reference_program(pkg, ref_configs, tmp_path, na
         pytest.skip("compiled reference budget program or dns_budget not available")
     m = ref_configs[name]
     cntr = int(m["TSTR"])
-    a, b = _dirs(tmp_path)
+    # both programs run in a subdirectory of the run and read its fields from ".."
     ch = pkg.Channel(params_for(pkg, m, "cfr"))
     ch.init_seeded(42, 0.05, 0.005)
     ch.step(6)
-    for d in (a, b):
-        ch.write_fields(d, cntr)
+    ch.write_fields(tmp_path, cntr)
     ch.close()
+    a, b = _dirs(tmp_path)
     subprocess.run([str(exe)], cwd=a, check=True, capture_output=True, timeout=600)
     write_definitions(m, b / "definitions.h", TEND=cntr)
     r = subprocess.run([str(BUDGET)], cwd=b, capture_output=True, text=True, timeout=600)
