@@ -239,20 +239,20 @@ def fp64_ms_per_step(pkg, torch, inst, cache, steps=8, device=0):
     return cache[key]
 
 
-def max_over_ranks(torch, dist, x: float) -> float:
+def max_over_ranks(torch, dist, x: float, group=None) -> float:
     """The largest x over all ranks (x itself without a process group)."""
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend(group) == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
 
 
-def sum_over_ranks(torch, dist, x: float) -> float:
+def sum_over_ranks(torch, dist, x: float, group=None) -> float:
     if dist is None:
         return x
-    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend() == "nccl" else "cpu")
-    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    t = torch.tensor([x], dtype=torch.float64, device="cuda" if dist.get_backend(group) == "nccl" else "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
     return float(t.item())
 
 

@@ -134,7 +134,7 @@ static int append_logs(logs *L, const dns_step_log *r) {
   int rc = 0;
   rc |= log_line(L, 0, r->time, r->flowrate);
   rc |= log_line(L, 1, r->time, r->denst);
-  if (!isfinite(r->stress)) return rc; /* the reference aborts before the wall logs */
+  if (isnan(r->stress)) return rc; /* the reference aborts before the wall logs (NaN only) */
   rc |= log_line(L, 2, r->time, r->stup);
   rc |= log_line(L, 3, r->time, r->stdown);
   rc |= log_line(L, 4, r->time, r->stress);
@@ -349,7 +349,7 @@ int main(int argc, char **argv) {
     long done = rc == DNS_OK ? n : 0; /* any other failure leaves the rows unset */
     if (rc == DNS_ENAN) {
       done = 0;
-      while (done < n && isfinite(rows[done].stress)) done++;
+      while (done < n && !isnan(rows[done].stress)) done++;
       if (done < n) done++; /* the failing step's flow-rate logs are written, as encalc2 runs first */
     }
     for (long q = 0; q < done && !status; q++)

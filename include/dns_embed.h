@@ -33,7 +33,7 @@ extern "C" {
 #define DNS_EINVAL (-1)   /* bad argument or unsupported parameter combination */
 #define DNS_ENOMEM (-2)   /* device or host allocation failed / over budget */
 #define DNS_EIO (-3)      /* restart or output file missing, short or unwritable */
-#define DNS_ENAN (-4)     /* non-finite wall shear stress (reference aborts) */
+#define DNS_ENAN (-4)     /* NaN wall shear stress (reference aborts); batched: non-finite */
 #define DNS_ETIMEOUT (-5) /* a bounded wait gave up (the request loop's deadline) */
 #define DNS_ECUDA (-6)    /* CUDA runtime error */
 
@@ -190,8 +190,9 @@ int dns_get_force(dns_handle *h, double *force);
    (dns-q-mgrd-all-patterns-xyc.c:1254-1375): encalc2, wshearstr, xcomputations,
    GR x (xfcomputations, tinterpolate_hrmt, derivative, ctfdtransfer_opt),
    ftcdtransfer, exchange/fexchange.  log (may be NULL) receives ncoarse rows.
-   Returns DNS_ENAN if a wall shear stress is not finite (the reference calls
-   MPI_Abort, wshearstr.c:139-143); the state is then left as computed. */
+   Returns DNS_ENAN if a wall shear stress is NaN (the reference calls
+   MPI_Abort on isnan, wshearstr.c:139-143; an infinite stress is logged and
+   stepping goes on, as there); the state is then left as computed. */
 int dns_step(dns_handle *h, long ncoarse, dns_step_log *log);
 
 /* ---- statistics ---------------------------------------------------------- */
@@ -238,9 +239,13 @@ int dns_kernel_times(dns_handle *h, double *ms, long *launches);
    Nothing is allocated: the per-block partial sums live in a 4 MiB array
    compiled into the library, which every GPU that loads the library holds
    until the process exits; a domain needing more than 262144 reduction blocks
-   is rejected with DNS_EINVAL.  The first call on a device looks up that
-   array's device address; make it before any stream capture.  All calls share
-   the array, so calls that overlap on the GPU race: serialise them. */
+   is rejected with DNS_EINVAL.  Only the FP64 layout is read: p->precision
+   must be DNS_FP64 (DNS_EINVAL otherwise).  Every call asks the runtime for the
+   array's device address on p->device (no allocation; after a cudaDeviceReset
+   the new context's address is used); the first call on a device may load the
+   library's device code, so make it before any stream capture.  The caller's
+   current device is restored before the call returns.  All calls share the
+   array, so calls that overlap on the GPU race: serialise them. */
 int dns_flow_sums_static(const dns_params *p, const double *fc, const double *ff, double *out4, void *cuda_stream);
 
 /* ---- batched FP32 engine --------------------------------------------------- */

@@ -29,7 +29,8 @@ multiply-add is formed (x86-64 baseline code has none anyway) and ``-fcommon``
 because ``definitions.h`` defines ``DP PI;`` in every translation unit.
 
 Run ``python oracle/build_ref.py [config ...]``; with no argument every
-configuration in ``REF_CONFIGS`` is built.  Needs the reference tree.
+configuration in ``REF_CONFIGS`` is built.  Needs the reference tree, found at
+``$DNS_REFERENCE_ROOT`` (default: the tree's mount point, ``REFERENCE_ROOT`` below).
 """
 from __future__ import annotations
 
@@ -42,8 +43,10 @@ import sys
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
-REF_SRC = Path("/root/reference/DNS-solver-with-grid-embedding/src")
-TKE_SRC = Path("/root/reference/TKE-budget/computations")
+# root of the reference project's tree (read-only); DNS_REFERENCE_ROOT overrides it
+REFERENCE_ROOT = Path(os.environ.get("DNS_REFERENCE_ROOT", "/root/reference"))
+REF_SRC = REFERENCE_ROOT / "DNS-solver-with-grid-embedding" / "src"
+TKE_SRC = REFERENCE_ROOT / "TKE-budget" / "computations"
 # macros of TKE-budget/computations/definitions.h:21-47 taken from the configuration
 TKE_MACROS = ("zdv", "ydv", "xdv", "CFL", "Rebs", "ub", "gratio", "zds", "TSTR", "TEND", "DT")
 OUT = HERE / "_ref"

@@ -17,12 +17,13 @@ import pytest
 
 ROOT = Path(__file__).resolve().parent.parent
 PKG_NAME = "dns-solvers-with-grid-embedding_b200"
-REF_TREE = Path("/root/reference/DNS-solver-with-grid-embedding/src")
 
 if str(ROOT) not in sys.path:
     sys.path.insert(0, str(ROOT))
 if str(ROOT / "oracle") not in sys.path:
     sys.path.insert(0, str(ROOT / "oracle"))
+
+from build_ref import REF_SRC as REF_TREE  # noqa: E402  (the reference's solver sources, where mounted)
 
 
 def pytest_configure(config):

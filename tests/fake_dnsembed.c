@@ -200,7 +200,7 @@ int dns_step(dns_handle *h, long n, dns_step_log *log) {
     o->stdown = pl[q].stdown;
     o->stress = pl[q].stress;
     o->pgrad = pl[q].pgrad;
-    if (rc == DNS_OK && !isfinite(o->stress)) rc = failf(DNS_ENAN, "fake: non-finite wall shear stress");
+    if (rc == DNS_OK && isnan(o->stress)) rc = failf(DNS_ENAN, "fake: NaN wall shear stress");
   }
   h->ss += n;
   free(pl);

@@ -138,3 +138,51 @@ def test_python_structs_match_the_header_layout(pkg, tmp_path):
         assert got[(cname, "sizeof")] == C.sizeof(py), cname
         for fname, _ in py._fields_:
             assert got[(cname, fname)] == getattr(py, fname).offset, (cname, fname)
+
+
+# ---- allocation-free reduction: the checks made before any device work ----
+STATIC_PAIRS = 262144  # slots of the scratch array compiled into the library
+
+
+def flow_sums_pairs(xdv, ydv, zdv, zds, gratio, bx=128, jb=2):
+    """Reduction blocks of the direct encalc2 pass: max(fine, coarse) x/y block
+    counts of the kernels' launch shape (bx threads along x, jb rows) times
+    the coarse planes plus both fine blocks' planes."""
+    nxf, nyf = gratio * xdv, gratio * ydv
+    gx = max(-(-nxf // bx), -(-xdv // bx))
+    gy = max(-(-nyf // jb), -(-ydv // jb))
+    return gx * gy * (zdv + 2 * zds)
+
+
+def _static_fn(pkg):
+    fn = pkg.lib().dns_flow_sums_static
+    fn.restype = C.c_int
+    fn.argtypes = [C.POINTER(pkg.Params), C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p]
+    return fn
+
+
+def test_static_scratch_covers_the_superhydrophobic_channel():
+    # the 384 x 128 x 192 channel (xdv 384, ydv 192, zdv 115, zds 16): 6 x 192 x 147 blocks
+    assert flow_sums_pairs(384, 192, 115, 16, 2) == 169344 <= STATIC_PAIRS
+    # the boundary cases the GPU test and the rejection test use
+    assert flow_sums_pairs(64, 4096, 48, 8, 2) == STATIC_PAIRS
+    assert flow_sums_pairs(2368, 109, 33, 16, 2) == STATIC_PAIRS + 1
+
+
+def test_static_reduction_refusals_touch_no_device(pkg):
+    fn = _static_fn(pkg)
+    dummy = C.c_double()
+    ptr = C.addressof(dummy)
+    # one slot beyond the array
+    p = pkg.make_params(xdv=2368, ydv=109, zdv=33, zds=16, gratio=2)
+    assert fn(C.byref(p), ptr, ptr, ptr, None) == pkg.DNS_EINVAL
+    assert b"262145 reduction slots" in pkg.lib().dns_last_error()
+    # the FP32 layout is not read
+    p = pkg.make_params(xdv=16, ydv=16, zdv=9, zds=4, gratio=2, precision=pkg.FP32)
+    assert fn(C.byref(p), ptr, ptr, ptr, None) == pkg.DNS_EINVAL
+    assert b"DNS_FP64" in pkg.lib().dns_last_error()
+    # invalid geometry: dns_geometry_of's own message is kept
+    p = pkg.make_params(xdv=16, ydv=16, zdv=9, zds=4, gratio=1)
+    assert fn(C.byref(p), ptr, ptr, ptr, None) == pkg.DNS_EINVAL
+    msg = pkg.lib().dns_last_error()
+    assert b"gratio" in msg and b"invalid parameters" not in msg
