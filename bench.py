@@ -62,6 +62,11 @@ CONFIGS = {
     "c3r": (dict(xdv=384, ydv=192, zdv=115, zds=16, gratio=2, Rebs=13585.0, ub=0.0866034, CFL=0.1, pattern="RSLIP",
                  gyplussize=24, wyplussize=24),
             "SHS channel 384x128x192 coarse, streamwise ridges pitch 48 GF 0.5, Re_tau~395"),
+    "c3p": (dict(xdv=384, ydv=192, zdv=115, zds=16, gratio=2, Rebs=13585.0, ub=0.0866034, CFL=0.1, pattern="PSLIP",
+                 gyplussize=16, wyplussize=16, gxplussize=16, wxplussize=16),
+            "SHS channel 384x128x192 coarse, square posts pitch 32 GF 0.75, Re_tau~395"),
+    "c3n": (dict(xdv=384, ydv=192, zdv=115, zds=16, gratio=2, Rebs=13585.0, ub=0.0866034, CFL=0.1, pattern=None),
+            "channel 384x128x192 coarse with no-slip walls: the drag reference of the SHS channels, Re_tau~395"),
 }
 METRIC = "MLUPS (coarse-step node updates, FP64 plain form)"
 
@@ -346,6 +351,56 @@ def bench_served(pkg, torch, args, peak, fp64_cache):
 PKG = "dns-solvers-with-grid-embedding_b200"
 
 
+def bench_longrun(pkg, args):
+    """BASELINE configs 2 and 3 run long: warm-up, then sampled steps whose
+    statistics are time-averaged on the device in FP64 (every step); FP64 plain
+    form against the FP32 deviation form, per statistic, with batch-means
+    standard errors; config 3 with a no-slip companion run for the drag
+    reduction.  Errors are relative to each profile's largest magnitude."""
+    W = importlib.import_module(PKG + ".workloads")
+    warm, windows, per = args.longrun_warmup, args.longrun_windows, args.longrun_steps // args.longrun_windows
+    out = {"warmup_steps": warm, "sampled_steps": windows * per, "windows": windows, "sample_every": 1,
+           "note": "errors: max over the profile of |FP32 - FP64| / max |FP64| (statistics); rel_uncertainty: "
+                   "the two runs' batch-means standard errors combined, same units; ok: error <= 1e-3 or "
+                   "within two standard errors", "cases": {}}
+    summaries = {}
+    for name in args.longrun_cases:
+        m, desc = CONFIGS[name]
+        g = pkg.geometry(pkg.make_params(**m))
+        case = {"description": desc}
+        t0 = time.perf_counter()
+        runs = {}
+        for prec in ("fp64", "fp32"):
+            cum, log, err = W.long_run(pkg, m, prec, warm, windows, per)
+            if err:
+                case[prec] = {"diverged": err}
+                continue
+            s = W.summarize_run(cum, log, windows, g.nyf, g.nzs, g.zdf, m["Rebs"])
+            runs[prec] = s
+            case[prec] = {"tau_w": s["tau_w"], "tau_w_stderr": s["tau_w_stderr"], "cf": s["cf"],
+                          "cf_stderr": s["cf_stderr"], "slip_length": s["slip_length"],
+                          "slip_length_stderr": s["slip_length_stderr"], "re_tau_realised": s["re_tau"],
+                          "samples": s["samples"],
+                          "u_centre": float(s["profiles"][1][len(s["profiles"][1]) // 2]),
+                          "uu_max": float(np.max(s["profiles"][5])), "uw_absmax": float(np.max(np.abs(s["profiles"][8])))}
+        if "fp64" in runs and "fp32" in runs:
+            case["fp32_vs_fp64"] = W.compare_runs(runs["fp32"], runs["fp64"])
+        case["seconds"] = time.perf_counter() - t0
+        summaries[name] = runs
+        out["cases"][name] = case
+    # drag reduction of the patterned walls against the no-slip companion
+    for name in args.longrun_cases:
+        if name in ("c3r", "c3p") and "c3n" in summaries:
+            dr = {}
+            for prec in ("fp64", "fp32"):
+                if prec in summaries[name] and prec in summaries["c3n"]:
+                    dr[prec] = W.drag_reduction_vs(summaries[name][prec]["cf"], summaries["c3n"][prec]["cf"])
+            if "fp64" in dr and "fp32" in dr:
+                dr["abs_err_pct_points"] = abs(dr["fp32"] - dr["fp64"])
+            out["cases"][name]["drag_reduction_pct_vs_noslip"] = dr
+    return out
+
+
 def bench_budget(pkg, ch, p, config: str):
     """The turbulence statistics / kinetic-energy budget of one snapshot of the
     channel's current state: on the device from the live state and from the
@@ -518,6 +573,9 @@ def run_ours(args, rank, world, local_rank):
     }
     if world == 1 and not args.no_budget:
         line["budget"] = bench_budget(pkg, ch, p, args.config)
+    if world == 1 and args.longrun_cases:
+        ch.close()
+        line["longrun"] = bench_longrun(pkg, args)
     # ---- the FP32 deviation-storage form on the same workload (same GPU), run
     # by the batched engine as a batch of one
     fp64_cache = {}
@@ -582,6 +640,11 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--c5-requests", type=int, default=16)
     ap.add_argument("--c5-rates", type=float, nargs="+", default=[2.0, 10.0, 50.0])
+    ap.add_argument("--longrun-cases", nargs="*", default=["c2", "c3n", "c3r", "c3p"],
+                    help="channels run long for the FP32-vs-FP64 statistics (none: skip)")
+    ap.add_argument("--longrun-warmup", type=int, default=10000)
+    ap.add_argument("--longrun-steps", type=int, default=20000, help="sampled steps after the warm-up")
+    ap.add_argument("--longrun-windows", type=int, default=10, help="windows for the batch-means errors")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))

@@ -143,6 +143,7 @@ def lib() -> C.CDLL:
         "dns_batch_run": (I, [P, C.c_longlong, C.POINTER(I)]),
         "dns_batch_info_of": (I, [P, I, C.POINTER(BatchInfo)]),
         "dns_batch_stats": (I, [P, I, P, C.POINTER(C.c_long)]),
+        "dns_batch_stats_reset": (I, [P, I]),
         "dns_batch_export_state": (I, [P, I, I, P]),
         "dns_batch_import_state": (I, [P, I, I, P]),
         "dns_batch_log": (I, [P, I, C.c_longlong, C.c_longlong, P]),
@@ -437,6 +438,9 @@ class Batch:
         ns = C.c_long()
         _check(lib().dns_batch_stats(self.h, i, out.ctypes.data, C.byref(ns)), "dns_batch_stats")
         return out, ns.value
+
+    def stats_reset(self, i: int):
+        _check(lib().dns_batch_stats_reset(self.h, i), "dns_batch_stats_reset")
 
     def export_state(self, i: int, level: int) -> np.ndarray:
         g = self.geoms[i]

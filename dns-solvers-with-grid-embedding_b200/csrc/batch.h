@@ -63,7 +63,7 @@ struct Inst {
   int8_t *wflag;          // [nyf][nxf]
   double *part;           // block partials
   long long pc, pf, pi, pw, psc, psf, pl2;  // region offsets (doubles) in part; pl2: finalize level 2
-  double *stats;          // [nzp][16] running sums
+  double *stats;          // [nzp][kStatRow] running statistics (kernels.h)
 };
 
 // Advanced on the device by the finalize kernel.

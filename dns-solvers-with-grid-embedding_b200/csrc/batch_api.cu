@@ -142,7 +142,7 @@ Layout layout_of(const Inst &I) {
   L.pl2 = o; o += (long long)kFinChunks * 18;
   L.npart = o;
   L.part = take(off, (size_t)o * 8);
-  L.stats = take(off, (size_t)I.nzp * 16 * 8);
+  L.stats = take(off, (size_t)I.nzp * kStatRow * 8);
   L.total = off;
   return L;
 }
@@ -378,7 +378,7 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
   std::vector<int8_t> wf = wall_flags(q, g);
   BTRY(cudaMemcpyAsync(I.wflag, wf.data(), wf.size(), cudaMemcpyHostToDevice, b->s));
   BTRY(cudaMemsetAsync(I.part, 0, (size_t)L.npart * 8, b->s));
-  BTRY(cudaMemsetAsync(I.stats, 0, (size_t)I.nzp * 16 * 8, b->s));
+  BTRY(cudaMemsetAsync(I.stats, 0, (size_t)I.nzp * kStatRow * 8, b->s));
   launch_seed_f32(I.fc[0], I.ff[0], I.hist, d, seed, uc, amp, b->s);
   // encalc2 of the seeded state -> force of the first step (as dns_init_seeded)
   if ((rc = refresh_flow(b, I, q, g, slot, 0, 0))) {
@@ -557,11 +557,20 @@ extern "C" int dns_batch_info_of(dns_batch *b, int id, dns_batch_info *out) {
   return DNS_OK;
 }
 
+extern "C" int dns_batch_stats_reset(dns_batch *b, int id) {
+  Record *r = record_of(b, id);
+  if (!r) return fail_with(DNS_EINVAL, "no such instance");
+  BTRY(cudaSetDevice(b->device));
+  // ordered on the batch's stream, between step groups
+  BTRY(cudaMemsetAsync(r->inst.stats, 0, (size_t)r->inst.nzp * kStatRow * 8, b->s));
+  return DNS_OK;
+}
+
 extern "C" int dns_batch_stats(dns_batch *b, int id, double *out, long *nsamples) {
   Record *r = record_of(b, id);
   if (!r || !out) return fail_with(DNS_EINVAL, "no such instance");
   BTRY(cudaSetDevice(b->device));
-  std::vector<double> acc((size_t)r->g.nz_profile * 16);
+  std::vector<double> acc((size_t)r->g.nz_profile * kStatRow);
   BTRY(cudaMemcpyAsync(acc.data(), r->inst.stats, acc.size() * 8, cudaMemcpyDeviceToHost, b->s));
   BTRY(cudaStreamSynchronize(b->s));
   stats_from_acc(r->g, acc.data(), out, nsamples);

@@ -40,11 +40,9 @@ __device__ __forceinline__ Dims dims_of(const Inst &I) {
   return Dims{I.nx, I.ny, I.nzc, I.nxf, I.nyf, I.zdf, I.zds, I.gr, 0};
 }
 
-__device__ __forceinline__ void stat_acc(const float (&f)[19], double (&sacc)[9]) {
+__device__ __forceinline__ void stat_acc(const float (&f)[19], PlaneStat &sacc) {
   const Mac32 m = macro_f32(f);
-  const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-  sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-  sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
+  sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
 }
 
 // ------------------------------------------------------------------ statistics
@@ -76,7 +74,8 @@ __global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, c
     const int i = bx * W + tx;
     const float *src = coarse ? I.fc[D.cc] : I.ff[D.cf];
     const size_t pstride = coarse ? (size_t)I.nzc * I.ny * I.nx : (size_t)2 * I.zds * I.nyf * I.nxf;
-    double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+    PlaneStat sacc;
+    sacc.init(I.stats, coarse ? profile_index_coarse(p, I.zdf) : profile_index_fine(p, I.zds, I.zdf, I.nzc), true);
     for (int r = 0; r < jb; r++) {
       const int j = (by * jb + r) * R + ty;
       if (i >= nx || j >= ny) continue;
@@ -85,13 +84,13 @@ __global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, c
       stat_acc(f, sacc);
     }
     const size_t blk = ((size_t)p * gy + by) * gx + bx;
-    block_reduce32<9>(sacc, I.part + (coarse ? I.psc : I.psf) + blk * 9);
+    block_reduce32<9>(sacc.s, I.part + (coarse ? I.psc : I.psf) + blk * 9);
   }
 }
 
 // per composite-profile plane: sum the plane's block partials (fixed order) and
-// add the sample into the running sums (layout of the single-channel form:
-// 0..8 plane sums, 9..13 per-sample plane variances, 14 nodes, 15 samples)
+// add the sample into the instance's running-statistics row (kernels.h layout,
+// the single-channel form's)
 __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
   __shared__ double sh[9][kThreads];
   const int n = M->n;
@@ -135,18 +134,9 @@ __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, 
       __syncthreads();
     }
     if (threadIdx.x == 0) {
-      double *o = I.stats + (size_t)idx * 16;
       double s9[9];
       for (int c = 0; c < 9; c++) s9[c] = sh[c][0];
-      for (int c = 0; c < 9; c++) o[c] += s9[c];
-      const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
-      o[9] += s9[4] / nn - mu * mu;
-      o[10] += s9[5] / nn - mv * mv;
-      o[11] += s9[6] / nn - mw * mw;
-      o[12] += s9[7] / nn - mu * mw;
-      o[13] += s9[8] / nn - mr * mr;
-      o[14] = nn;
-      o[15] += 1.0;
+      stat_row_add(I.stats + (size_t)idx * kStatRow, s9, nn);
     }
     __syncthreads();
   }
@@ -180,7 +170,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
     float *dst = I.fc[D.cc ^ 1];
     const float om = I.om_c, G = (float)state[I.slot].force;
     double acc[2] = {0., 0.};
-    double sacc[9];
+    PlaneStat sacc;
     for (int r = 0; r < I.cjb; r++) {
       const int j = (by * I.cjb + r) * R + ty;
       if (i >= I.nx || j >= I.ny) continue;
@@ -275,7 +265,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
         upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
     const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
     double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
-    double sacc[9];
+    PlaneStat sacc;
     float wz[3] = {0.f, 0.f, 0.f};
     {
 #pragma unroll

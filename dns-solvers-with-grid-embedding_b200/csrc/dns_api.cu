@@ -68,7 +68,7 @@ struct dns_handle {
   DevState *state = nullptr;
   DevLog *dlog = nullptr;              // kLogCap rows
   DevLog *hlog = nullptr;              // pinned mirror
-  double *stats_acc = nullptr;         // [nz_profile][16]
+  double *stats_acc = nullptr;         // [nz_profile][kStatRow] running statistics
   double *iface_mac = nullptr;         // FP64: interface rho, u [2][4][nyf][nxf]; FP32: corner data
   void *tke_ws = nullptr;              // statistics / budget work space (allocated on first use)
   size_t tke_ws_bytes = 0;
@@ -82,6 +82,7 @@ struct dns_handle {
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
   long sample_every = 0;
+  long nsampled = 0;                   // samples taken since the last statistics reset
   std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
   long wall_gen = 0;                     // bumped whenever wall_lo / wall_hi change
   Profiler prof;
@@ -259,7 +260,7 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   const long long esz = p->precision == DNS_FP32 ? 4 : 8;  // bytes per stored population
   const long long mac = esz == 4 ? 2LL * 23 * g->ny * g->nx * 4 : 8LL * g->nyf * g->nxf;  // elements of esz
   g->device_bytes = esz * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + mac) +
-                    8 * (pl.total + 16LL * g->nz_profile) +
+                    8 * (pl.total + (long long)kStatRow * g->nz_profile) +
                     (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
   return DNS_OK;
 }
@@ -360,7 +361,7 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   if ((rc = alloc((void **)&h->partials, (size_t)h->pl.total * 8))) return rc;
   if ((rc = alloc((void **)&h->state, sizeof(DevState)))) return rc;
   if ((rc = alloc((void **)&h->dlog, kLogCap * sizeof(DevLog)))) return rc;
-  if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * 16 * 8))) return rc;
+  if ((rc = alloc((void **)&h->stats_acc, (size_t)g.nz_profile * kStatRow * 8))) return rc;
   // FP64: interface rho, u at fine nodes; FP32: corner values and derivatives (float4)
   const size_t mac_bytes = esz == 4 ? 2ull * 23 * g.ny * g.nx * 16 : 8ull * g.nyf * g.nxf * esz;
   if ((rc = alloc((void **)&h->iface_mac, mac_bytes))) return rc;
@@ -389,7 +390,7 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   std::vector<int8_t> wf = wall_flags(*p, g);
   cudaMemcpy(h->wflag, wf.data(), wf.size(), cudaMemcpyHostToDevice);
   cudaMemset(h->partials, 0, (size_t)h->pl.total * 8);
-  cudaMemset(h->stats_acc, 0, (size_t)g.nz_profile * 16 * 8);
+  cudaMemset(h->stats_acc, 0, (size_t)g.nz_profile * kStatRow * 8);
   cudaMemset(h->state, 0, sizeof(DevState));
   h->wall_lo.assign((size_t)g.nxf * g.nyf * 19, 0.0);
   h->wall_hi.assign((size_t)g.nxf * g.nyf * 19, 0.0);
@@ -1060,10 +1061,10 @@ static size_t hslot_elems(const dns_handle *h) { return 2ull * 23 * h->d.ny * h-
 static void L_coarse(dns_handle *h, int src, int dst, bool sample, cudaStream_t st) {
   if (is_f32(h))
     launch_coarse_f32(F(h->fc[src]), F(h->fc[dst]), h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl,
-                      sample, st);
+                      sample, h->stats_acc, st);
   else
     launch_coarse_f64(h->fc[src], h->fc[dst], h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl, sample,
-                      st);
+                      h->stats_acc, st);
 }
 static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
   if (is_f32(h))
@@ -1074,10 +1075,10 @@ static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
 static void L_fine(dns_handle *h, int src, int dst, bool first, bool last, bool stats, cudaStream_t st) {
   if (is_f32(h))
     launch_fine_f32(F(h->ff[src]), F(h->ff[dst]), h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials,
-                    h->pl, first, last, stats, st);
+                    h->pl, first, last, stats, h->stats_acc, st);
   else
     launch_fine_f64(h->ff[src], h->ff[dst], h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials, h->pl,
-                    first, last, stats, st);
+                    first, last, stats, h->stats_acc, st);
 }
 static void L_iface(dns_handle *h, int fbuf, int it, cudaStream_t st) {
   const size_t hs = hslot_elems(h);
@@ -1289,7 +1290,16 @@ extern "C" int dns_step(dns_handle *h, long ncoarse, dns_step_log *log) {
     const long ss0 = h->ss;
     for (long q = 0; q < n; q++) {
       const bool sample = h->sample_every > 0 && (h->ss % h->sample_every) == 0;
+      if (sample && h->nsampled == 0) {
+        // the first sample after a reset: the plane means of this state become
+        // the shift every sample is summed about
+        if (is_f32(h))
+          launch_stat_shift_f32(F(h->fc[h->cur_c]), F(h->ff[h->cur_f]), h->d, h->stats_acc, h->stream);
+        else
+          launch_stat_shift_f64(h->fc[h->cur_c], h->ff[h->cur_f], h->d, h->stats_acc, h->stream);
+      }
       issue_step(h, h->dlog + q, sample);
+      if (sample) h->nsampled++;
       h->ss++;
     }
     CUDA_TRY(cudaGetLastError());
@@ -1331,8 +1341,9 @@ extern "C" int dns_set_sampling(dns_handle *h, long every) {
 extern "C" int dns_stats_reset(dns_handle *h) {
   if (!h) return fail(DNS_EINVAL, "null handle");
   CUDA_TRY(cudaSetDevice(h->p.device));
-  CUDA_TRY(cudaMemsetAsync(h->stats_acc, 0, (size_t)h->g.nz_profile * 16 * 8, h->stream));
+  CUDA_TRY(cudaMemsetAsync(h->stats_acc, 0, (size_t)h->g.nz_profile * kStatRow * 8, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->nsampled = 0;
   return DNS_OK;
 }
 
@@ -1352,32 +1363,34 @@ void dns::stats_from_acc(const dns_geometry &g, const double *acc, double *out, 
   std::vector<double> z;
   profile_z(g, z);
   long ns = 0;
-  for (int p = 0; p < NZ; p++) ns = std::max(ns, (long)acc[(size_t)p * 16 + 15]);
+  for (int p = 0; p < NZ; p++) ns = std::max(ns, (long)acc[(size_t)p * kStatRow + 15]);
   if (nsamples) *nsamples = ns;
   std::memset(out, 0, sizeof(double) * DNS_NSTAT * NZ);
   for (int p = 0; p < NZ; p++) {
-    const double *a = acc + (size_t)p * 16;
+    const double *a = acc + (size_t)p * kStatRow;
     out[0 * NZ + p] = z[p];
     const double S = a[15], N = a[14];
     if (S <= 0 || N <= 0) continue;
     const double T = S * N;  // samples x nodes
-    out[1 * NZ + p] = a[0] / T;
-    out[2 * NZ + p] = a[1] / T;
-    out[3 * NZ + p] = a[2] / T;
-    out[4 * NZ + p] = a[3] / T;
+    // sums are taken about the shift a[16..19]: the means add it back, the
+    // second moments about the mean do not depend on it
+    const double du = a[0] / T, dv = a[1] / T, dw = a[2] / T;
+    out[1 * NZ + p] = a[16] + du;
+    out[2 * NZ + p] = a[17] + dv;
+    out[3 * NZ + p] = a[18] + dw;
+    out[4 * NZ + p] = a[19] + a[3] / T;
     for (int c = 0; c < 5; c++) out[(5 + c) * NZ + p] = a[9 + c] / S;
-    const double mu = a[0] / T, mv = a[1] / T, mw = a[2] / T;
-    out[10 * NZ + p] = a[4] / T - mu * mu;
-    out[11 * NZ + p] = a[5] / T - mv * mv;
-    out[12 * NZ + p] = a[6] / T - mw * mw;
-    out[13 * NZ + p] = a[7] / T - mu * mw;
+    out[10 * NZ + p] = a[4] / T - du * du;
+    out[11 * NZ + p] = a[5] / T - dv * dv;
+    out[12 * NZ + p] = a[6] / T - dw * dw;
+    out[13 * NZ + p] = a[7] / T - du * dw;
   }
 }
 
 extern "C" int dns_stats(dns_handle *h, double *out, long *nsamples) {
   if (!h || !out) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
-  std::vector<double> acc((size_t)h->g.nz_profile * 16);
+  std::vector<double> acc((size_t)h->g.nz_profile * kStatRow);
   CUDA_TRY(cudaMemcpyAsync(acc.data(), h->stats_acc, acc.size() * 8, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   dns::stats_from_acc(h->g, acc.data(), out, nsamples);

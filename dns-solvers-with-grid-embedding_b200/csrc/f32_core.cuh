@@ -166,14 +166,10 @@ __device__ __forceinline__ void filtered_node_f32(const float *__restrict__ fs, 
 template <bool STATS>
 __device__ __forceinline__ void coarse_node_f32(float (&f)[19], int i, int j, int k, const Dims &d, float om,
                                                 float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
-                                                double (&sacc)[9]) {
+                                                PlaneStat &sacc) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc;
   const Mac32 m = collide_f32(f, om, G);
-  if (STATS) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
+  if (STATS) sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
   float mom = 0.f, den = 0.f;
@@ -195,14 +191,10 @@ __device__ __forceinline__ void coarse_node_f32(float (&f)[19], int i, int j, in
 template <bool STATS>
 __device__ __forceinline__ void coarse_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
                                                 float G, float *__restrict__ dst, size_t pstride, double (&acc)[2],
-                                                double (&sacc)[9]) {
+                                                PlaneStat &sacc) {
   const int nx = d.nx, ny = d.ny;
   const Mac32 m = collide_f32(f, om, G);
-  if (STATS) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
+  if (STATS) sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
   const int plane = ny * nx;
   const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
   const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
@@ -270,18 +262,14 @@ template <int MODE, int ZSKIP = 0>
 __device__ __forceinline__ void fine_bulk_f32(float (&f)[19], int i, int j, size_t idx0, const Dims &d, float om,
                                               float Gf, float *__restrict__ dst, size_t pstride, const float (&wz)[3],
                                               bool wall_sum_plane, bool wall_rho_plane, double (&acc)[2],
-                                              double (&wacc)[2], double (&sacc)[9]) {
+                                              double (&wacc)[2], PlaneStat &sacc) {
   const int nx = d.nxf, ny = d.nyf;
   const Mac32 m = macro_f32(f);
   if (MODE & 2) {
     if (wall_sum_plane) wacc[0] += (double)m.u0;
     if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
   }
-  if (MODE & 4) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
+  if (MODE & 4) sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
   const int plane = ny * nx;
   const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
   const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
@@ -311,18 +299,14 @@ __device__ __forceinline__ void fine_wall_f32(float (&f)[19], int i, int j, size
                                               float Gf, const int8_t *__restrict__ wf, float *__restrict__ dst,
                                               size_t pstride, const float (&wz)[3], bool wall_sum_plane,
                                               bool wall_rho_plane, double (&acc)[2], double (&wacc)[2],
-                                              double (&sacc)[9]) {
+                                              PlaneStat &sacc) {
   const int nx = d.nxf, ny = d.nyf;
   const Mac32 m = macro_f32(f);
   if (MODE & 2) {
     if (wall_sum_plane) wacc[0] += (double)m.u0;
     if (wall_rho_plane) wacc[1] += 1.0 + (double)m.drho;
   }
-  if (MODE & 4) {
-    const double u0 = m.u0, u1 = m.u1, u2 = m.u2, rho = 1.0 + (double)m.drho;
-    sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += rho;
-    sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += rho * rho;
-  }
+  if (MODE & 4) sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
   const int plane = ny * nx;
   const int dxm = i == 0 ? nx - 1 : -1, dxp = i == nx - 1 ? 1 - nx : 1;
   const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;

@@ -24,7 +24,7 @@ struct Range {
 
 // wall-plane flags [nyf][nxf] of the pattern in p (-1 solid, -2 slip)
 std::vector<int8_t> wall_flags(const dns_params &p, const dns_geometry &g);
-// running statistics sums acc[nz_profile][16] -> out[DNS_NSTAT][nz_profile]
+// running statistics rows acc[nz_profile][kStatRow] (kernels.h) -> out[DNS_NSTAT][nz_profile]
 void stats_from_acc(const dns_geometry &g, const double *acc, double *out, long *nsamples);
 // record msg for dns_last_error() and return code
 int fail_with(int code, const std::string &msg);

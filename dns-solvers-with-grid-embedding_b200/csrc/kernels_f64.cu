@@ -107,14 +107,17 @@ __device__ __forceinline__ void load19(const double *__restrict__ src, size_t id
 template <bool STATS>
 __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                             Dims d, int jb, double om, const DevState *st,
-                                                            double *__restrict__ part, double *__restrict__ spart) {
+                                                            double *__restrict__ part, double *__restrict__ spart,
+                                                            const double *__restrict__ srow) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = blockIdx.z;
   const size_t pstride = (size_t)nzc * ny * nx;
   const double G = st->force;
   double acc[2] = {0., 0.};
-  double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  PlaneStat sacc;
+  // planes 2..zdc-3 are profile points; the others' sums are not read
+  sacc.init(srow, profile_index_coarse(k, d.zdf), STATS && k >= 2 && k <= nzc - 3);
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   for (int r = 0; r < jb; r++) {
     const int j = blockIdx.y * jb + r;
@@ -123,10 +126,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(co
     load19(src, ((size_t)k * ny + j) * nx + i, pstride, f);
     double dens, u0, u1, u2;
     collide_f64(f, om, G, dens, u0, u1, u2);
-    if (STATS) {
-      sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += dens;
-      sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += dens * dens;
-    }
+    if (STATS) sacc.add(u0, u1, u2, dens);
     const int jm = j == 0 ? ny - 1 : j - 1, jp = j == ny - 1 ? 0 : j + 1;
 #pragma unroll
     for (int a = 0; a < 19; a++) {
@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(co
   }
   const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   block_reduce<2>(acc, part + blk * 2);
-  if (STATS) block_reduce<9>(sacc, spart + blk * 9);
+  if (STATS) block_reduce<9>(sacc.s, spart + blk * 9);
 }
 
 // Interface planes of the new coarse state into history level n
@@ -188,7 +188,8 @@ template <int MODE>
 __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                           const int8_t *__restrict__ wf, Dims d, int jb, double om,
                                                           const DevState *st, double *__restrict__ part,
-                                                          double *__restrict__ wpart, double *__restrict__ spart) {
+                                                          double *__restrict__ wpart, double *__restrict__ spart,
+                                                          const double *__restrict__ srow) {
   const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
   const int P = 2 * zds;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -213,7 +214,8 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   // sum_a e_x^2 BI_a = 1).  Other planes sum the pushes with their weights.
   const bool unit_plane = upper ? (k >= gr + 2 && k <= zdf - 3) : (k >= 2 && k <= zdf - gr - 2);
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
-  double sacc[9] = {0., 0., 0., 0., 0., 0., 0., 0., 0.};
+  PlaneStat sacc;
+  sacc.init(srow, profile_index_fine(p, zds, zdf, d.nzc), (MODE & 4) != 0);
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   for (int r = 0; r < jb; r++) {
     const int j = blockIdx.y * jb + r;
@@ -226,10 +228,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
       if (wall_sum_plane) wacc[0] += u0;
       if (wall_rho_plane) wacc[1] += dens;
     }
-    if (MODE & 4) {
-      sacc[0] += u0; sacc[1] += u1; sacc[2] += u2; sacc[3] += dens;
-      sacc[4] += u0 * u0; sacc[5] += u1 * u1; sacc[6] += u2 * u2; sacc[7] += u0 * u2; sacc[8] += dens * dens;
-    }
+    if (MODE & 4) sacc.add(u0, u1, u2, dens);
     if ((MODE & 1) && unit_plane) {
       acc[0] += dens * u0 + dens * Gf;
       acc[1] += dens;
@@ -267,7 +266,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce<2>(acc, part + blk * 2);
   if ((MODE & 2) && wall_sum_plane) block_reduce<2>(wacc, wpart + blk * 2);
-  if (MODE & 4) block_reduce<9>(sacc, spart + blk * 9);
+  if (MODE & 4) block_reduce<9>(sacc.s, spart + blk * 9);
 }
 
 // ------------------------------------------------------------------ interface
@@ -767,9 +766,8 @@ __global__ void __launch_bounds__(kFin2Threads) finalize2_kernel(DevState *st, D
   }
 }
 
-// per-plane statistics of one sample, accumulated over samples
-// acc[NZ][16]: 0..8 sums over samples of plane sums (u v w rho uu vv ww uw rr),
-// 9..13 sums over samples of per-sample plane variances, 14 nodes per plane, 15 samples
+// per-plane statistics of one sample, added to the running rows acc[NZ][kStatRow]
+// (layout in kernels.h)
 struct StatsArgs {
   int nzp;          // composite profile length
   int zdf, nzc, zds;
@@ -807,18 +805,34 @@ __global__ void __launch_bounds__(256) stats_finalize_kernel(double *acc, const 
     s9[c] = sh[0];
     __syncthreads();
   }
-  if (threadIdx.x == 0) {
-    double *o = acc + (size_t)idx * 16;
-    for (int c = 0; c < 9; c++) o[c] += s9[c];
-    const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
-    o[9] += s9[4] / nn - mu * mu;
-    o[10] += s9[5] / nn - mv * mv;
-    o[11] += s9[6] / nn - mw * mw;
-    o[12] += s9[7] / nn - mu * mw;
-    o[13] += s9[8] / nn - mr * mr;
-    o[14] = nn;
-    o[15] += 1.0;
+  if (threadIdx.x == 0) stat_row_add(acc + (size_t)idx * kStatRow, s9, nn);
+}
+
+// Shift of the running statistics: the plane means of u, v, w and rho of the
+// stored state, one block per composite-profile point, written into the rows'
+// entries 16..19 before the first sample after a reset.
+__global__ void __launch_bounds__(256) stat_shift_kernel(const double *__restrict__ fc, const double *__restrict__ ff,
+                                                         Dims d, double *__restrict__ rows) {
+  int level, plane;
+  profile_plane(blockIdx.x, d.zds, d.zdf, d.nzc, level, plane);
+  if (level < 0) return;
+  const int nx = level ? d.nxf : d.nx, ny = level ? d.nyf : d.ny;
+  const size_t pstride = level ? (size_t)2 * d.zds * d.nyf * d.nxf : (size_t)d.nzc * d.ny * d.nx;
+  const double *base = (level ? ff : fc) + (size_t)plane * ny * nx;
+  double v[4] = {0., 0., 0., 0.};
+  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
+    double f[19];
+    load19(base, (size_t)q, pstride, f);
+    double dens, mx, my, mz;
+    moments_f64(f, dens, mx, my, mz);
+    v[0] += mx / dens;
+    v[1] += my / dens;
+    v[2] += mz / dens;
+    v[3] += dens;
   }
+  __shared__ double out[4];
+  block_reduce_n<4, 256>(v, out);
+  if (threadIdx.x < 4) rows[(size_t)blockIdx.x * kStatRow + 16 + threadIdx.x] = out[threadIdx.x] / ((double)nx * ny);
 }
 
 // ------------------------------------------------------------------ seeded state
@@ -997,14 +1011,14 @@ PartialLayout partial_layout(const Dims &d, const LaunchShape &s) {
 
 void launch_coarse_f64(const double *src, double *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
-                       cudaStream_t stream) {
+                       const double *srow, cudaStream_t stream) {
   dim3 grid(s.cgx, s.cgy, d.nzc), block(s.bx);
   if (stats)
     coarse_kernel<true><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
-                                                    partials + pl.stats_c);
+                                                    partials + pl.stats_c, srow);
   else
     coarse_kernel<false><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
-                                                     partials + pl.stats_c);
+                                                     partials + pl.stats_c, srow);
 }
 
 void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream) {
@@ -1014,12 +1028,12 @@ void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const L
 
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
-                     bool last, bool stats, cudaStream_t stream) {
+                     bool last, bool stats, const double *srow, cudaStream_t stream) {
   dim3 grid(s.fgx, s.fgy, 2 * d.zds), block(s.bx);
   const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
   double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
 #define FINE_CASE(M) \
-  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps); break;
+  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps, srow); break;
   switch (mode) {
     FINE_CASE(0) FINE_CASE(1) FINE_CASE(2) FINE_CASE(3) FINE_CASE(4) FINE_CASE(5) FINE_CASE(6) FINE_CASE(7)
   }
@@ -1107,6 +1121,10 @@ void launch_stats_finalize(double *acc, const double *partials, const PartialLay
   a.nc = (double)d.nx * d.ny;
   a.nf = (double)d.nxf * d.nyf;
   stats_finalize_kernel<<<a.nzp, 256, 0, stream>>>(acc, partials + pl.stats_c, partials + pl.stats_f, a);
+}
+
+void launch_stat_shift_f64(const double *fc, const double *ff, const Dims &d, double *rows, cudaStream_t stream) {
+  stat_shift_kernel<<<2 * d.zdf + d.nzc - 4, 256, 0, stream>>>(fc, ff, d, rows);
 }
 
 void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,

@@ -16,6 +16,10 @@
 // sign of a zero that is later added to 1.
 #pragma once
 
+#include <cstddef>
+
+#include "kernels.h"
+
 namespace dns {
 
 __host__ __device__ constexpr int ex_of(int a) {
@@ -136,6 +140,85 @@ __device__ __forceinline__ void collide_f64(double (&f)[19], double om, double G
       f[a] = ex > 0 ? f[a] + (q - t) : f[a] - (q + t);   // f + (+-q - t)
     }
   }
+}
+
+
+// ------------------------------------------------------------------ sampled statistics
+// Composite-profile index of coarse plane k (k = 2..zdc-3) and of fine device
+// plane p (lower block k = p + 1, upper block k = p - zds), statistics.c:52-146;
+// profile_plane inverts them: level (0 coarse, 1 fine) and plane (coarse k or
+// fine device plane) of index idx, or level -1 for the two wall points.
+__host__ __device__ __forceinline__ int profile_index_coarse(int k, int zdf) { return zdf - 2 + k; }
+__host__ __device__ __forceinline__ int profile_index_fine(int p, int zds, int zdf, int nzc) {
+  return p < zds ? p + 1 : zdf + nzc - 4 + (p - zds);
+}
+__host__ __device__ __forceinline__ void profile_plane(int idx, int zds, int zdf, int nzc, int &level, int &plane) {
+  level = -1;
+  plane = 0;
+  if (idx >= 1 && idx <= zdf - 1) {
+    level = 1;
+    plane = idx - 1;
+  } else if (idx >= zdf && idx <= zdf + nzc - 5) {
+    level = 0;
+    plane = idx - zdf + 2;
+  } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {
+    level = 1;
+    plane = zds + idx - (zdf + nzc - 4);
+  }
+}
+
+// One block's sums of the sampled moments of its nodes, taken about the plane's
+// shift (the running-statistics row's entries 16..19).
+struct PlaneStat {
+  double s[9];
+  double sh[4];
+  __device__ __forceinline__ void init(const double *rows, int idx, bool on) {
+#pragma unroll
+    for (int c = 0; c < 9; c++) s[c] = 0.;
+#pragma unroll
+    for (int c = 0; c < 4; c++) sh[c] = on ? rows[(size_t)idx * kStatRow + 16 + c] : 0.;
+  }
+  __device__ __forceinline__ void add(double u0, double u1, double u2, double rho) {
+    const double a = u0 - sh[0], b = u1 - sh[1], c = u2 - sh[2], r = rho - sh[3];
+    s[0] += a; s[1] += b; s[2] += c; s[3] += r;
+    s[4] += a * a; s[5] += b * b; s[6] += c * c; s[7] += a * c; s[8] += r * r;
+  }
+};
+
+// Add one sample's plane sums s9 (taken about the row's shift) to the row o of
+// nn nodes.  A row without a shift (o[19], the mean density, still zero: the
+// single-channel forms set the shift from the state before their first sample,
+// the batched engine does not) took this sample about zero: its sums are
+// re-centred on its own plane means, which become the shift of every later
+// sample.  The per-sample variances do not depend on the shift.
+__device__ __forceinline__ void stat_row_add(double *o, const double (&s9)[9], double nn) {
+  const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
+  const double var[5] = {s9[4] / nn - mu * mu, s9[5] / nn - mv * mv, s9[6] / nn - mw * mw, s9[7] / nn - mu * mw,
+                         s9[8] / nn - mr * mr};
+  double t[9];
+#pragma unroll
+  for (int c = 0; c < 9; c++) t[c] = s9[c];
+  if (o[19] == 0.) {
+    t[0] = s9[0] - nn * mu;
+    t[1] = s9[1] - nn * mv;
+    t[2] = s9[2] - nn * mw;
+    t[3] = s9[3] - nn * mr;
+    t[4] = s9[4] - nn * (mu * mu);
+    t[5] = s9[5] - nn * (mv * mv);
+    t[6] = s9[6] - nn * (mw * mw);
+    t[7] = s9[7] - nn * (mu * mw);
+    t[8] = s9[8] - nn * (mr * mr);
+    o[16] = mu;
+    o[17] = mv;
+    o[18] = mw;
+    o[19] = mr;
+  }
+#pragma unroll
+  for (int c = 0; c < 9; c++) o[c] += t[c];
+#pragma unroll
+  for (int c = 0; c < 5; c++) o[9 + c] += var[c];
+  o[14] = nn;
+  o[15] += 1.0;
 }
 
 }  // namespace dns

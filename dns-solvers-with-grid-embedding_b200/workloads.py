@@ -210,3 +210,155 @@ def solve_result(inst: Instance, stats: np.ndarray, log: np.ndarray, zdf: int) -
     cf, dr = drag_reduction(log, inst.rebs, first=len(log) // 2)
     return {"z": stats[0].tolist(), "U": stats[1].tolist(), "slip_length": 0.5 * (lo + up),
             "slip_length_walls": (lo, up), "cf": cf, "drag_reduction_pct": dr}
+
+
+# ------------------------------------------------------------------ long-run statistics
+# Profiles of the running statistics (dns_stats rows) that are time means of
+# per-sample quantities, so that the mean over a window is linear in the
+# accumulated sums: 1 <U> 2 <V> 3 <W> 4 <rho> 5 <u'u'> 6 <v'v'> 7 <w'w'>
+# 8 <u'w'> 9 <rho'rho'> (per-sample plane moments, statistics.c:147-292,
+# averaged in time as TKE-budget/postprocessing/time_stat.c:161-200 does).
+LINEAR_ROWS = tuple(range(1, 10))
+STAT_NAMES = {1: "U", 5: "uu", 6: "vv", 7: "ww", 8: "uw"}
+
+
+def window_means(cum: list[tuple[np.ndarray, int]]) -> list[np.ndarray]:
+    """Per-window means from cumulative statistics read at window boundaries.
+
+    cum[q] = (stats, samples) as dns_stats returns them after window q
+    (cum[0] at the start of the first window).  Rows LINEAR_ROWS are averages
+    over all samples so far, so a window's own mean is the difference of the
+    two cumulative sums over its samples; row 0 (z/H) is copied."""
+    out = []
+    for (a, na), (b, nb) in zip(cum[:-1], cum[1:]):
+        if nb <= na:
+            raise ValueError("a window without samples")
+        m = np.array(b, dtype=np.float64, copy=True)
+        for r in LINEAR_ROWS:
+            m[r] = (b[r] * nb - a[r] * na) / (nb - na)
+        out.append(m)
+    return out
+
+
+def batch_mean_and_error(values: list) -> tuple[np.ndarray, np.ndarray]:
+    """Mean of equal-length batch means and its standard error
+    std(batch means, ddof=1) / sqrt(batches)."""
+    v = np.asarray(values, dtype=np.float64)
+    if len(v) < 2:
+        return v.mean(axis=0), np.full(v.shape[1:], np.nan)
+    return v.mean(axis=0), v.std(axis=0, ddof=1) / math.sqrt(len(v))
+
+
+def friction_coefficient(log: np.ndarray, nyf: int, nzs: int) -> float:
+    """Cf = <tau_w> / (ub^2 / 2) over the log rows given, as
+    TKE-budget/postprocessing/CFriction.c:33-59 forms it: ub is the mean of
+    the logged flow rate divided by ydf (NZs - 2) with the reference's per-rank
+    ydf = GR ydv + 1, and Cf the mean of w-str / (ub^2 / 2)."""
+    ub = float(np.mean(log[:, 4])) / ((nyf + 1) * (nzs - 2.0))
+    return float(np.mean(log[:, 7] / (0.5 * ub * ub)))
+
+
+def drag_reduction_vs(cf: float, cf_noslip: float) -> float:
+    """DR in percent against a no-slip run at the same bulk Reynolds number:
+    100 (Cf0 - Cf) / Cf0 (CFriction.c:46-57 with a measured Cf0)."""
+    return 100.0 * (cf_noslip - cf) / cf_noslip
+
+
+def friction_reynolds(log: np.ndarray, nzs: int, rebs: float, ub: float = UB) -> float:
+    """Re_tau = u_tau (NZs - 2) / 2 / nu with u_tau = sqrt(<p-grad>) over the
+    rows and nu from the fine relaxation time (time_stat.c:95-104)."""
+    tau = (3.0 / rebs) * ub * (nzs - 2.0) + 0.5
+    nu = (1.0 / 6.0) * (2.0 * tau - 1.0)
+    return math.sqrt(max(float(np.mean(log[:, 8])), 0.0)) * (nzs - 2.0) * 0.5 / nu
+
+
+def profile_error(p: np.ndarray, ref: np.ndarray, used: slice | None = None) -> float:
+    """Largest deviation of profile p from ref relative to ref's largest
+    magnitude (profiles such as <u'w'> cross zero)."""
+    u = slice(1, len(ref) - 1) if used is None else used
+    scale = float(np.max(np.abs(ref[u])))
+    return float(np.max(np.abs(p[u] - ref[u]))) / scale if scale > 0 else 0.0
+
+
+def compare_runs(a: dict, ref: dict) -> dict:
+    """Per-statistic error of run a against run ref (summaries from
+    summarize_run), with the combined batch-means uncertainty in the same
+    units and whether the error is within 1e-3 or within two standard errors."""
+    out = {}
+    used = slice(1, len(ref["profiles"][1]) - 1)
+    for r, name in STAT_NAMES.items():
+        scale = float(np.max(np.abs(ref["profiles"][r][used])))
+        err = profile_error(a["profiles"][r], ref["profiles"][r], used)
+        se = np.sqrt(np.square(a["stderr"][r][used]) + np.square(ref["stderr"][r][used]))
+        unc = float(np.max(se)) / scale if scale > 0 else 0.0
+        out[name] = {"rel_err": err, "rel_uncertainty": unc, "ok": bool(err <= 1e-3 or err <= 2.0 * unc)}
+    for key in ("tau_w", "slip_length", "cf"):
+        x, y = a[key], ref[key]
+        err = abs(x - y) / abs(y) if y else 0.0
+        se_key = key + "_stderr"
+        se = math.hypot(a.get(se_key) or 0.0, ref.get(se_key) or 0.0)
+        unc = se / abs(y) if y else 0.0
+        ok = err <= 1e-3 or abs(x - y) <= 2.0 * se
+        if key == "slip_length":  # near zero on a no-slip wall: also judged in fine units
+            ok = ok or abs(x - y) <= 1e-3
+        out[key] = {"value": x, "ref": y, "abs_err": abs(x - y), "rel_err": err, "rel_uncertainty": unc,
+                    "ok": bool(ok)}
+    return out
+
+
+def summarize_run(cum: list[tuple[np.ndarray, int]], log: np.ndarray, windows: int, nyf: int, nzs: int,
+                  zdf: int, rebs: float) -> dict:
+    """Time averages of one run's sampled window: profiles (mean of the window
+    means) with batch-means standard errors, the wall shear stress, Cf, the
+    slip length and the realised Re_tau.  log holds the window's step rows."""
+    wm = window_means(cum)
+    prof, err = batch_mean_and_error(wm)
+    rows = np.array_split(log, windows)
+    tw, tw_se = batch_mean_and_error([[float(np.mean(r[:, 7]))] for r in rows])
+    cf_b = [friction_coefficient(r, nyf, nzs) for r in rows]
+    cf, cf_se = batch_mean_and_error([[c] for c in cf_b])
+    slips = [0.5 * sum(slip_length(m, zdf)) for m in wm]
+    sl, sl_se = batch_mean_and_error([[x] for x in slips])
+    return {"profiles": prof, "stderr": err, "tau_w": float(tw[0]), "tau_w_stderr": float(tw_se[0]),
+            "cf": float(cf[0]), "cf_stderr": float(cf_se[0]), "slip_length": float(sl[0]),
+            "slip_length_stderr": float(sl_se[0]), "re_tau": friction_reynolds(log, nzs, rebs),
+            "samples": int(cum[-1][1] - cum[0][1])}
+
+
+def long_run(pkg, macros: dict, precision: str, warm: int, windows: int, per: int, seed: int = SEED,
+             device: int = 0):
+    """One channel (reference macros `macros`, constant flow rate) run long:
+    `warm` steps, then `windows` windows of `per` steps with the statistics
+    sampled every step.  precision "fp64": the FP64 plain form (a channel
+    handle); "fp32": the FP32 deviation form of the batched engine (a batch of
+    one).  Returns (cumulative statistics at the window boundaries, the
+    windows' log rows, None) or (None, None, reason) when the run stopped on a
+    non-finite wall shear stress."""
+    p = pkg.make_params(**macros, forcing=pkg.FORCING_CFR, device=device)
+    if precision == "fp64":
+        with pkg.Channel(p) as ch:
+            ch.init_seeded(seed, UC, AMP)
+            try:
+                ch.step(warm, log=False)
+                ch.stats_reset()
+                ch.set_sampling(1)
+                cum, logs = [ch.stats()], []
+                for _ in range(windows):
+                    logs.append(ch.step(per, log=True))
+                    cum.append(ch.stats())
+            except pkg.DnsError as e:
+                return None, None, str(e)
+        return cum, np.concatenate(logs), None
+    with pkg.Batch(device) as b:
+        i = b.add(p, steps=warm + windows * per, seed=seed, uc=UC, amp=AMP, sample_every=1)
+        b.run(warm)
+        b.stats_reset(i)
+        cum = [b.stats(i)]
+        for _ in range(windows):
+            b.run(per)
+            cum.append(b.stats(i))
+        inf = b.info(i)
+        if inf.status != 0:
+            return None, None, f"status {inf.status} after {inf.steps_done} steps (non-finite wall shear stress)"
+        log = b.log(i, first=warm, n=windows * per)
+    return cum, log, None

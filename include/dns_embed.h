@@ -305,6 +305,9 @@ int dns_batch_run(dns_batch *b, long long nsteps, int *active);
 int dns_batch_info_of(dns_batch *b, int id, dns_batch_info *out);
 /* The instance's statistics, as dns_stats. */
 int dns_batch_stats(dns_batch *b, int id, double *out, long *nsamples);
+/* Discard the instance's accumulated statistics (as dns_stats_reset), e.g.
+   after a warm-up; sampling goes on at the instance's cadence. */
+int dns_batch_stats_reset(dns_batch *b, int id);
 /* The instance's post-stream state, as dns_export_state. */
 int dns_batch_export_state(dns_batch *b, int id, int level, double *aos_out);
 /* Replace one level of the instance's post-stream state, as dns_import_state

@@ -128,26 +128,45 @@ def test_plane_stats_match_reference_definition(pkg, port, ref_configs):
     np.testing.assert_array_equal(ch.plane_stats(), p.plane_stats())
 
 
-def test_sampled_statistics(pkg, port, ref_configs):
-    ch, p = pair(pkg, port, ref_configs["t_odd"], "cfr")
-    ch.set_sampling(2)
+def _sampled_vs_two_pass(pkg, port, m, uc, amp, steps, every, rtol_mean, rtol_var):
+    """The device's sampled statistics against the time mean of the oracle's
+    per-sample plane records (statistics.c: plane means, then two-pass rms and
+    <u'w'> about them)."""
+    ch, p = pair(pkg, port, m, "cfr", uc=uc, amp=amp)
+    ch.set_sampling(every)
     snaps = []
-    for s in range(6):
-        if s % 2 == 0:
+    for s in range(steps):
+        if s % every == 0:
             snaps.append(p.plane_stats())
         p.step(1)
-    ch.step(6)
+    ch.step(steps)
     st, ns = ch.stats()
-    assert ns == 3
+    assert ns == len(snaps)
     ref = np.mean(snaps, axis=0)  # time mean of the per-sample plane records
     used = slice(1, st.shape[1] - 1)
     for name, row, col in (("U", 1, 0), ("V", 2, 1), ("W", 3, 2), ("rho", 4, 7)):
-        np.testing.assert_allclose(st[row, used], ref[col, used], rtol=1e-11, atol=1e-15, err_msg=name)
-    # per-sample variances: one-pass E[x^2]-E[x]^2 against the reference's two-pass
+        np.testing.assert_allclose(st[row, used], ref[col, used], rtol=rtol_mean, atol=1e-15, err_msg=name)
+    # per-sample variances: sums about the shift (the first sample's plane
+    # means) against the reference's two-pass definition
+    sq = np.mean(np.square(snaps), axis=0)
     for name, row, col in (("uu", 5, 3), ("vv", 6, 4), ("ww", 7, 5)):
-        np.testing.assert_allclose(st[row, used], np.mean(np.square(snaps), axis=0)[col, used], rtol=1e-6,
-                                   atol=1e-13, err_msg=name)
-    np.testing.assert_allclose(st[8, used], ref[6, used], rtol=1e-6, atol=1e-13)
+        np.testing.assert_allclose(st[row, used], sq[col, used], rtol=rtol_var, atol=0, err_msg=name)
+    scale = np.max(np.abs(ref[6, used]))
+    np.testing.assert_allclose(st[8, used], ref[6, used], rtol=0, atol=rtol_var * scale, err_msg="uw")
+
+
+def test_sampled_statistics(pkg, port, ref_configs):
+    _sampled_vs_two_pass(pkg, port, ref_configs["t_odd"], 0.05, 0.005, steps=6, every=2, rtol_mean=1e-11,
+                         rtol_var=1e-10)
+
+
+def test_sampled_variance_survives_cancellation(pkg, port, ref_configs):
+    """Perturbations of 1e-6 on a mean flow of 0.1: the plane variances are
+    ~1e-13 against squared means of ~1e-2, so E[x^2] - E[x]^2 taken about zero
+    would keep only ~5 significant digits; taken about the shift they keep the
+    two-pass result to 1e-8."""
+    _sampled_vs_two_pass(pkg, port, ref_configs["t_odd"], 0.1, 1e-6, steps=4, every=1, rtol_mean=1e-11,
+                         rtol_var=1e-8)
 
 
 def test_non_finite_state_is_reported(pkg, port, ref_configs):
