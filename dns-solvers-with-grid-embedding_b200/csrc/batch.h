@@ -30,12 +30,9 @@ constexpr int kFinChunks = 32;  // blocks per instance in the finalize
 enum Phase {
   PH_STATS = 0,  // plane statistics of the sampled state (coarse 2..zdc-3, every fine plane)
   PH_SFINAL,     // per-plane accumulation of those sums
-  PH_CBULK,      // coarse planes 2..zdc-3
-  PH_CEDGE,      // coarse planes 0, 1, zdc-2, zdc-1
+  PH_COARSE,     // every coarse plane
   PH_EXTRACT,    // interface history planes k = 1 and zdc-2
-  PH_FBULK,      // fine planes k = 2..zdf-3 of both blocks
-  PH_FEDGE,      // the wall-adjacent fine planes (lower k = 1, upper k = zdf-2)
-  PH_FADJ,       // the fine planes next to the interfaces (lower zdf-2, zdf-1; upper 0, 1)
+  PH_FINE,       // every fine plane of both blocks (wall-adjacent, interface-adjacent, then bulk)
   PH_ICORNER,    // interface corner data: tiles x walls x fields
   PH_IEVAL,      // interface evaluation: fine rows x walls
   PH_INJECT,     // fine-to-coarse injection rows
@@ -46,8 +43,10 @@ enum Phase {
 // Constant while the instance is resident.
 struct Inst {
   int nx, ny, nzc, nxf, nyf, zdf, zds, gr;
-  int cw, cjb, cgx, cgy;  // coarse tile: width (threads in x), row iterations, grid per plane
-  int fw, fjb, fgx, fgy;  // fine tile
+  // tiles of the stream-collide kernels: width (threads along x, each updating
+  // four consecutive nodes), row iterations, and items per plane in x and y
+  int cw, cjb, cgx, cgy;  // coarse
+  int fw, fjb, fgx, fgy;  // fine
   int igx, igy;           // interface corner tiles
   int egx;                // extraction / injection blocks per row
   int nzp;                // composite profile planes
@@ -92,7 +91,7 @@ constexpr int kCornerTX = 32, kCornerTY = 8;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
-  int stats, sfinal, cbulk, cedge, extract, fbulk, fedge, fadj, icorner, ieval, inject, final_;
+  int stats, sfinal, coarse, extract, fine, icorner, ieval, inject, final_;
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)

@@ -51,14 +51,17 @@ struct Record {
 using ShapeKey = std::tuple<int, int, int, int, int>;
 ShapeKey key_of(const dns_params &p) { return ShapeKey{p.xdv, p.ydv, p.zdv, p.zds, p.gratio}; }
 
+// threads along a row for n four-node groups: the widest power of two up to
+// 128 that divides n, else the widest that does not exceed it
 int pick_width(int n) {
-  if (n % 128 == 0) return 128;
-  if (n % 64 == 0) return 64;
-  if (n % 32 == 0) return 32;
-  return n >= 128 ? 128 : (n >= 64 ? 64 : 32);
+  for (int w = 128; w >= 8; w >>= 1)
+    if (n % w == 0) return w;
+  for (int w = 128; w >= 8; w >>= 1)
+    if (n >= w) return w;
+  return 8;
 }
 
-bool width_ok(int w) { return w == 32 || w == 64 || w == 128; }
+bool width_ok(int w) { return w == 8 || w == 16 || w == 32 || w == 64 || w == 128; }
 bool tile_ok(const dns_tile &t) {
   return width_ok(t.cw) && width_ok(t.fw) && t.cjb >= 1 && t.cjb <= 64 && t.fjb >= 1 && t.fjb <= 64;
 }
@@ -68,20 +71,26 @@ dns_tile default_tile(const dns_geometry &g) {
   // four row iterations per work item: on B200 the persistent loop's per-item
   // set-up and block reduction are amortised over 512 nodes (measured: 4
   // beats 2 by 4% and is within noise of 8 and 16 on mixed batches)
-  t.cw = pick_width(g.nx);
+  t.cw = pick_width(g.nx / 4);
   t.cjb = 4;
-  t.fw = pick_width(g.nxf);
+  t.fw = pick_width(g.nxf / 4);
   t.fjb = 4;
   return t;
 }
 
 int cdiv(long long a, long long b) { return (int)((a + b - 1) / b); }
 
-// FP32 geometry of p (the batch stores deviations in float whatever p asks)
+// FP32 geometry of p (the batch stores deviations in float whatever p asks).
+// The stream-collide kernels move four consecutive nodes along x with 16-byte
+// memory operations, so every row must start on a 16-byte boundary: xdv a
+// multiple of 4.
 int geometry32(const dns_params *p, dns_params &q, dns_geometry &g) {
   q = *p;
   q.precision = DNS_FP32;
-  return dns_geometry_of(&q, &g);
+  const int rc = dns_geometry_of(&q, &g);
+  if (rc) return rc;
+  if (q.xdv % 4 != 0) return fail_with(DNS_EINVAL, "the batched engine needs xdv a multiple of 4");
+  return DNS_OK;
 }
 
 void shape_inst(Inst &I, const dns_params &p, const dns_geometry &g, const dns_tile &t) {
@@ -96,11 +105,11 @@ void shape_inst(Inst &I, const dns_params &p, const dns_geometry &g, const dns_t
   I.gr = g.gr;
   I.cw = t.cw;
   I.cjb = t.cjb;
-  I.cgx = cdiv(g.nx, t.cw);
+  I.cgx = cdiv(g.nx, 4LL * t.cw);
   I.cgy = cdiv(g.ny, (long long)(128 / t.cw) * t.cjb);
   I.fw = t.fw;
   I.fjb = t.fjb;
-  I.fgx = cdiv(g.nxf, t.fw);
+  I.fgx = cdiv(g.nxf, 4LL * t.fw);
   I.fgy = cdiv(g.nyf, (long long)(128 / t.fw) * t.fjb);
   I.igx = cdiv(g.nx, kCornerTX);
   I.igy = cdiv(g.ny, kCornerTY);
@@ -137,8 +146,8 @@ Layout layout_of(const Inst &I) {
   L.pf = o; o += fb * 2;
   L.pi = o; o += ib * 2;
   L.pw = o; o += fb * 2;
-  L.psc = o; o += cb * 9;
-  L.psf = o; o += fb * 9;
+  L.psc = o; o += cb * kStatPart;
+  L.psf = o; o += fb * kStatPart;
   L.pl2 = o; o += (long long)kFinChunks * 18;
   L.npart = o;
   L.part = take(off, (size_t)o * 8);
@@ -281,7 +290,7 @@ extern "C" int dns_batch_tile_for(const dns_batch *b, const dns_params *p, dns_t
 
 extern "C" int dns_batch_set_tile(dns_batch *b, const dns_params *shape, const dns_tile *t) {
   if (!b || !shape || !t) return fail_with(DNS_EINVAL, "null argument");
-  if (!tile_ok(*t)) return fail_with(DNS_EINVAL, "tile widths must be 32, 64 or 128, row iterations 1..64");
+  if (!tile_ok(*t)) return fail_with(DNS_EINVAL, "tile widths must be 8, 16, 32, 64 or 128, row iterations 1..64");
   b->tuned[key_of(*shape)] = *t;
   return DNS_OK;
 }
@@ -706,7 +715,7 @@ extern "C" int dns_batch_autotune(dns_batch *b, const dns_params *shape, int ste
     }
     return DNS_OK;
   };
-  const int widths[3] = {32, 64, 128}, iters[4] = {1, 2, 4, 8};
+  const int widths[5] = {8, 16, 32, 64, 128}, iters[4] = {1, 2, 4, 8};
   dns_tile base = cur;
   for (int w : widths)
     for (int j : iters) {

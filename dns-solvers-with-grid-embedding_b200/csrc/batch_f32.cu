@@ -6,6 +6,7 @@
 // trajectory does not depend on which other instances share the batch.
 #include "batch.h"
 #include "f32_core.cuh"
+#include "quad_f32.cuh"
 #include "kernels.h"
 #include "lattice.cuh"
 
@@ -36,10 +37,6 @@ __device__ __forceinline__ bool sampling(const Inst &I, const Dyn &D) {
   return D.remaining > 0 && I.sample_every > 0 && D.step % I.sample_every == 0;
 }
 
-__device__ __forceinline__ Dims dims_of(const Inst &I) {
-  return Dims{I.nx, I.ny, I.nzc, I.nxf, I.nyf, I.zdf, I.zds, I.gr, 0};
-}
-
 __device__ __forceinline__ void stat_acc(const float (&f)[19], PlaneStat &sacc) {
   const Mac32 m = macro_f32(f);
   sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
@@ -47,7 +44,8 @@ __device__ __forceinline__ void stat_acc(const float (&f)[19], PlaneStat &sacc) 
 
 // ------------------------------------------------------------------ statistics
 // Sums of the state at the start of the step (the state the single-channel
-// form samples inside its coarse kernel and first fine substep).
+// form samples inside its coarse kernel and first fine substep), four nodes
+// per thread on the tiles of the stream-collide kernels.
 __global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
   const int n = M->n;
   const int *st = M->start[PH_STATS];
@@ -71,20 +69,26 @@ __global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, c
     const int z = local / (gx * gy), rem = local - z * gx * gy, by = rem / gx, bx = rem - by * gx;
     const int p = coarse ? z + 2 : z;  // coarse plane k, or fine device plane
     const int lw = log2i(W), tx = threadIdx.x & (W - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
-    const int i = bx * W + tx;
     const float *src = coarse ? I.fc[D.cc] : I.ff[D.cf];
     const size_t pstride = coarse ? (size_t)I.nzc * I.ny * I.nx : (size_t)2 * I.zds * I.nyf * I.nxf;
     PlaneStat sacc;
-    sacc.init(I.stats, coarse ? profile_index_coarse(p, I.zdf) : profile_index_fine(p, I.zds, I.zdf, I.nzc), true);
+    sacc.init();
     for (int r = 0; r < jb; r++) {
       const int j = (by * jb + r) * R + ty;
-      if (i >= nx || j >= ny) continue;
-      float f[19];
-      load19f(src, ((size_t)p * ny + j) * nx + i, pstride, f);
-      stat_acc(f, sacc);
+      const QuadPos P = quad_pos(tx, W, bx * 4 * W, nx, j < ny);
+      if (!P.ok) continue;  // no shuffles below
+      float q[19][4];
+      quad_load(src, ((size_t)p * ny + j) * nx + P.x0, pstride, true, q);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float f[19];
+#pragma unroll
+        for (int a = 0; a < 19; a++) f[a] = q[a][c];
+        stat_acc(f, sacc);
+      }
     }
     const size_t blk = ((size_t)p * gy + by) * gx + bx;
-    block_reduce32<9>(sacc.s, I.part + (coarse ? I.psc : I.psf) + blk * 9);
+    block_reduce_stat(sacc, I.part + (coarse ? I.psc : I.psf) + blk * kStatPart);
   }
 }
 
@@ -92,7 +96,6 @@ __global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, c
 // add the sample into the instance's running-statistics row (kernels.h layout,
 // the single-channel form's)
 __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
-  __shared__ double sh[9][kThreads];
   const int n = M->n;
   const int *st = M->start[PH_SFINAL];
   const int total = st[n];
@@ -109,45 +112,34 @@ __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, 
     const int zdf = I.zdf, nzc = I.nzc;
     const double *src = nullptr;
     long nb = 0;
-    double nn = 0.;
     const long bc = (long)I.cgx * I.cgy, bf = (long)I.fgx * I.fgy;
     if (idx >= 1 && idx <= zdf - 1) {  // lower fine k = idx (device plane idx - 1)
-      src = I.part + I.psf + (size_t)(idx - 1) * bf * 9; nb = bf; nn = (double)I.nxf * I.nyf;
+      src = I.part + I.psf + (size_t)(idx - 1) * bf * kStatPart; nb = bf;
     } else if (idx >= zdf && idx <= zdf + nzc - 5) {  // coarse k = idx - zdf + 2
-      src = I.part + I.psc + (size_t)(idx - zdf + 2) * bc * 9; nb = bc; nn = (double)I.nx * I.ny;
+      src = I.part + I.psc + (size_t)(idx - zdf + 2) * bc * kStatPart; nb = bc;
     } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {  // upper fine k
       const int k = idx - (zdf + nzc - 4);
-      src = I.part + I.psf + (size_t)(I.zds + k) * bf * 9; nb = bf; nn = (double)I.nxf * I.nyf;
+      src = I.part + I.psf + (size_t)(I.zds + k) * bf * kStatPart; nb = bf;
     }
     if (!src) continue;
-#pragma unroll
-    for (int c = 0; c < 9; c++) {
-      double a = 0.;
-      for (long q = threadIdx.x; q < nb; q += blockDim.x) a += src[q * 9 + c];
-      sh[c][threadIdx.x] = a;
-    }
-    __syncthreads();
-    for (int o = kThreads / 2; o > 0; o >>= 1) {
-      if (threadIdx.x < o)
-#pragma unroll
-        for (int c = 0; c < 9; c++) sh[c][threadIdx.x] += sh[c][threadIdx.x + o];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-      double s9[9];
-      for (int c = 0; c < 9; c++) s9[c] = sh[c][0];
-      stat_row_add(I.stats + (size_t)idx * kStatRow, s9, nn);
-    }
-    __syncthreads();
+    stat_plane_finalize(src, nb, I.stats + (size_t)idx * kStatRow);  // block-uniform; ends with a barrier
   }
 }
 
 // ------------------------------------------------------------------ coarse
-template <bool BULK>
-__global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
+// Every coarse plane in one launch (xcomputations.c:49-86 collision,
+// :135-204, 353-420 streaming), four nodes per thread.  Pushes into planes 0
+// and zdc-1 are dropped (the fine-to-coarse injection rewrites them): planes
+// 2..zdc-3 push everything and their flow-rate partials are the nodes'
+// post-collision moments; the four planes 0, 1, zdc-2, zdc-1 drop their
+// pushes past plane 1 / zdc-2 and sum what they keep.
+#ifndef DNS_F32_QUAD_MINB
+#define DNS_F32_QUAD_MINB 4
+#endif
+__global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     b_coarse(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state) {
   const int n = M->n;
-  const int *st = M->start[BULK ? PH_CBULK : PH_CEDGE];
+  const int *st = M->start[PH_COARSE];
   const int total = st[n];
   int s = 0;
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -160,27 +152,44 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0)
     }
     const int local = w - st[s];
     const int gxy = I.cgx * I.cgy;
-    const int z = local / gxy, rem = local - z * gxy, by = rem / I.cgx, bx = rem - by * I.cgx;
-    const int k = BULK ? 2 + z : (z < 2 ? z : I.nzc - 4 + z);
+    const int k = local / gxy, rem = local - k * gxy, by = rem / I.cgx, bx = rem - by * I.cgx;
+    const int nx = I.nx, ny = I.ny, nzc = I.nzc;
     const int lw = log2i(I.cw), tx = threadIdx.x & (I.cw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
-    const int i = bx * I.cw + tx;
-    const Dims d = dims_of(I);
-    const size_t pstride = (size_t)I.nzc * I.ny * I.nx;
+    const size_t pstride = (size_t)nzc * ny * nx;
     const float *src = I.fc[D.cc];
     float *dst = I.fc[D.cc ^ 1];
     const float om = I.om_c, G = (float)state[I.slot].force;
+    const float one[3] = {1.f, 1.f, 1.f};
+    const int plane = ny * nx;
     double acc[2] = {0., 0.};
-    PlaneStat sacc;
     for (int r = 0; r < I.cjb; r++) {
-      const int j = (by * I.cjb + r) * R + ty;
-      if (i >= I.nx || j >= I.ny) continue;
-      float fa[19];
-      const size_t idx0 = ((size_t)k * I.ny + j) * I.nx + i;
-      load19f(src, idx0, pstride, fa);
-      if (BULK)
-        coarse_bulk_f32<false>(fa, i, j, idx0, d, om, G, dst, pstride, acc, sacc);
-      else
-        coarse_node_f32<false>(fa, i, j, k, d, om, G, dst, pstride, acc, sacc);
+      const int jr = (by * I.cjb + r) * R + ty;
+      const bool row_ok = jr < ny;
+      const int j = row_ok ? jr : 0;
+      const QuadPos P = quad_pos(tx, I.cw, bx * 4 * I.cw, nx, row_ok);
+      const long long rowoff = ((long long)k * ny + j) * nx;
+      float q[19][4];
+      quad_load(src, (size_t)(rowoff + P.x0), pstride, P.ok, q);
+      Mac32 m[4];
+      quad_collide(q, om, G, m);
+      const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+      if (k >= 2 && k <= nzc - 3) {
+        if (P.ok)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            acc[0] += (double)(m[c].rho * m[c].u0 + m[c].rho * G);
+            acc[1] += (double)m[c].drho;
+          }
+        quad_push<0, 0, false>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+      } else if (k == 0) {
+        quad_push<-2, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+      } else if (k == 1) {
+        quad_push<-1, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+      } else if (k == nzc - 2) {
+        quad_push<1, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+      } else {
+        quad_push<2, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+      }
     }
     const size_t blk = ((size_t)k * I.cgy + by) * I.cgx + bx;
     block_reduce32<2>(acc, I.part + I.pc + blk * 2);
@@ -223,20 +232,30 @@ __global__ void __launch_bounds__(kThreads) b_extract(const Mix *__restrict__ M,
 }
 
 // ------------------------------------------------------------------ fine
-// device plane of item plane q: KIND 1 bulk (k = 2..zdf-3 of both blocks),
-// KIND 2 interface-adjacent (lower k = zdf-2, zdf-1; upper k = 0, 1),
-// KIND 0 wall-adjacent (lower k = 1, upper k = zdf-2)
-__device__ __forceinline__ int fine_plane(int kind, int q, int zds) {
-  if (kind == 1) return q < zds - 3 ? q + 1 : zds + 2 + (q - (zds - 3));
-  if (kind == 2) return zds - 2 + q;
-  return q == 0 ? 0 : 2 * zds - 1;
+// Both fine blocks' planes in one launch per substep (xfcomputations.c:43-214,
+// 599-712 collision with force G/GR; :215-442, 724-897 streaming), four nodes
+// per thread.  Work item plane order: the two wall-adjacent planes (lower
+// k = 1, upper k = zdf-2), then the four interface-adjacent planes (lower
+// zdf-2, zdf-1, upper 0, 1), then the bulk planes k = 2..zdf-3 of both
+// blocks: the slower items are taken first, so the launch ends on bulk items.
+// Interface-adjacent planes drop the pushes that land on or past the
+// interface plane (it belongs to the concurrently running coarse-to-fine
+// transfer); wall-adjacent planes send their five wall-bound populations
+// through the bounce-back / specular rule.  MODE bits as the single-channel
+// form: 1 flow-rate partials (last substep), 2 wall-shear sums (first).
+__device__ __forceinline__ int fine_plane(int q, int zds) {
+  if (q == 0) return 0;
+  if (q == 1) return 2 * zds - 1;
+  if (q < 6) return zds - 2 + (q - 2);
+  const int b = q - 6;
+  return b < zds - 3 ? b + 1 : zds + 2 + (b - (zds - 3));
 }
 
-template <int MODE, int KIND>
-__global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
+template <int MODE>
+__global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     b_fine(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state, int sub) {
   const int n = M->n;
-  const int *st = M->start[KIND == 1 ? PH_FBULK : (KIND == 2 ? PH_FADJ : PH_FEDGE)];
+  const int *st = M->start[PH_FINE];
   const int total = st[n];
   int s = 0;
   for (int w = blockIdx.x; w < total; w += gridDim.x) {
@@ -249,59 +268,93 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0)
     }
     const int local = w - st[s];
     const int gxy = I.fgx * I.fgy;
-    const int q = local / gxy, rem = local - q * gxy, by = rem / I.fgx, bx = rem - by * I.fgx;
-    const int zds = I.zds, zdf = I.zdf, gr = I.gr;
-    const int p = fine_plane(KIND, q, zds);
+    const int qp = local / gxy, rem = local - qp * gxy, by = rem / I.fgx, bx = rem - by * I.fgx;
+    const int zds = I.zds, zdf = I.zdf, gr = I.gr, nx = I.nxf, ny = I.nyf;
+    const int p = fine_plane(qp, zds);
     const bool upper = p >= zds;
     const int k = upper ? p - zds : p + 1;
     const int lw = log2i(I.fw), tx = threadIdx.x & (I.fw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
-    const int i = bx * I.fw + tx;
-    const Dims d = dims_of(I);
-    const size_t pstride = (size_t)2 * zds * I.nyf * I.nxf;
+    const size_t pstride = (size_t)2 * zds * ny * nx;
     const float *src = I.ff[D.cf ^ ((sub - 1) & 1)];
     float *dst = I.ff[D.cf ^ (sub & 1)];
     const float om = I.om_f, Gf = (float)((1. / (double)gr) * state[I.slot].force);
     const bool wall_sum_plane =
         upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
     const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
-    double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
-    PlaneStat sacc;
-    float wz[3] = {0.f, 0.f, 0.f};
-    {
+    // plane class: 0 bulk, 1 lower wall-adjacent, 2 upper wall-adjacent,
+    // 3..6 interface-adjacent with ZSKIP 1, 2, -1, -2
+    const int cls = (!upper && k == 1) ? 1
+                    : (upper && k == zdf - 2) ? 2
+                    : (!upper && k == zdf - 2) ? 3
+                    : (!upper && k == zdf - 1) ? 4
+                    : (upper && k == 1) ? 5
+                    : (upper && k == 0) ? 6 : 0;
+    float wz[3];
 #pragma unroll
-      for (int c = 0; c < 3; c++) {
-        const int kd = k + c - 1;
-        wz[c] = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
-                       : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
-      }
+    for (int c = 0; c < 3; c++) {
+      const int kd = k + c - 1;  // destination planes k - 1, k, k + 1 (encalc2.c:33-53, 86-107)
+      wz[c] = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
+                     : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
     }
+    const bool wuni = wz[0] == wz[1] && wz[1] == wz[2];
+    const int plane = ny * nx;
+    double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
     for (int r = 0; r < I.fjb; r++) {
-      const int j = (by * I.fjb + r) * R + ty;
-      if (i >= I.nxf || j >= I.nyf) continue;
-      float fa[19];
-      const size_t idx0 = ((size_t)p * I.nyf + j) * I.nxf + i;
-      load19f(src, idx0, pstride, fa);
-      if (KIND == 1)
-        fine_bulk_f32<MODE>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc, wacc,
-                            sacc);
-      else if (KIND == 2 && !upper && k == zdf - 1)
-        fine_bulk_f32<MODE, 2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
-                               wacc, sacc);
-      else if (KIND == 2 && upper && k == 0)
-        fine_bulk_f32<MODE, -2>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
-                                wacc, sacc);
-      else if (KIND == 2 && !upper)
-        fine_bulk_f32<MODE, 1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
-                               wacc, sacc);
-      else if (KIND == 2)
-        fine_bulk_f32<MODE, -1>(fa, i, j, idx0, d, om, Gf, dst, pstride, wz, wall_sum_plane, wall_rho_plane, acc,
-                                wacc, sacc);
-      else if (!upper)
-        fine_wall_f32<MODE, false>(fa, i, j, idx0, d, om, Gf, I.wflag, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
-                                   acc, wacc, sacc);
-      else
-        fine_wall_f32<MODE, true>(fa, i, j, idx0, d, om, Gf, I.wflag, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
-                                  acc, wacc, sacc);
+      const int jr = (by * I.fjb + r) * R + ty;
+      const bool row_ok = jr < ny;
+      const int j = row_ok ? jr : 0;
+      const QuadPos P = quad_pos(tx, I.fw, bx * 4 * I.fw, nx, row_ok);
+      const long long rowoff = ((long long)p * ny + j) * nx;
+      float q[19][4];
+      quad_load(src, (size_t)(rowoff + P.x0), pstride, P.ok, q);
+      Mac32 m[4];
+      quad_collide(q, om, Gf, m);
+      if (P.ok) {
+#pragma unroll
+        for (int c = 0; c < 4; c++) {
+          if ((MODE & 2) && wall_sum_plane) wacc[0] += (double)m[c].u0;
+          if ((MODE & 2) && wall_rho_plane) wacc[1] += 1.0 + (double)m[c].drho;
+        }
+      }
+      const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+      switch (cls) {
+        case 0:
+          if ((MODE & 1) && wuni) {
+            // every push lands on a plane of the same weight: the partials are
+            // the nodes' post-collision moments (collision keeps mass and
+            // momentum, the force adds rho G to sum e_x f)
+            if (P.ok)
+#pragma unroll
+              for (int c = 0; c < 4; c++) {
+                acc[0] += (double)(wz[1] * (m[c].rho * m[c].u0 + m[c].rho * Gf));
+                acc[1] += (double)(wz[1] * m[c].drho);
+              }
+            quad_push<0, 0, false>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          } else {
+            quad_push<0, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          }
+          break;
+        case 1:
+          quad_push<0, -1, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          quad_wall<false, (MODE & 1) != 0>(q, dst, pstride, rowoff, j, nx, ny, I.wflag, P, wz[1], acc);
+          break;
+        case 2:
+          quad_push<0, 1, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          quad_wall<true, (MODE & 1) != 0>(q, dst, pstride, rowoff, j, nx, ny, I.wflag, P, wz[1], acc);
+          break;
+        case 3:
+          quad_push<1, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          break;
+        case 4:
+          quad_push<2, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          break;
+        case 5:
+          quad_push<-1, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          break;
+        default:
+          quad_push<-2, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+          break;
+      }
     }
     const size_t blk = ((size_t)p * I.fgy + by) * I.fgx + bx;
     if (MODE & 1) block_reduce32<2>(acc, I.part + I.pf + blk * 2);
@@ -584,12 +637,9 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   const int cb = I.cgx * I.cgy, fb = I.fgx * I.fgy;
   c[PH_STATS] = (I.nzc - 4) * cb + 2 * I.zds * fb;
   c[PH_SFINAL] = I.nzp;
-  c[PH_CBULK] = (I.nzc - 4) * cb;
-  c[PH_CEDGE] = 4 * cb;
+  c[PH_COARSE] = I.nzc * cb;
   c[PH_EXTRACT] = 2 * I.ny * I.egx;
-  c[PH_FBULK] = 2 * (I.zds - 3) * fb;
-  c[PH_FEDGE] = 2 * fb;
-  c[PH_FADJ] = 4 * fb;
+  c[PH_FINE] = 2 * I.zds * fb;
   c[PH_ICORNER] = 2 * kCornerFieldGroups * I.igx * I.igy;
   const int etx = I.gr == 2 ? IfTile<2>::TX : (I.gr == 3 ? IfTile<3>::TX : IfTile<4>::TX);
   const int ety = I.gr == 2 ? IfTile<2>::TY : (I.gr == 3 ? IfTile<3>::TY : IfTile<4>::TY);
@@ -602,12 +652,9 @@ int query_grids(int gr, Grids *g) {
   int rc = 0;
   rc |= occupancy_grid(b_stats, &g->stats);
   rc |= occupancy_grid(b_sfinal, &g->sfinal);
-  rc |= occupancy_grid(b_coarse<true>, &g->cbulk);
-  rc |= occupancy_grid(b_coarse<false>, &g->cedge);
+  rc |= occupancy_grid(b_coarse, &g->coarse);
   rc |= occupancy_grid(b_extract, &g->extract);
-  rc |= occupancy_grid(b_fine<1, 1>, &g->fbulk);
-  rc |= occupancy_grid(b_fine<3, 0>, &g->fedge);
-  rc |= occupancy_grid(b_fine<3, 2>, &g->fadj);
+  rc |= occupancy_grid(b_fine<3>, &g->fine);
   rc |= occupancy_grid(b_icorner, &g->icorner);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
@@ -621,9 +668,7 @@ static void launch_fine(const Mix *m, Dyn *dyn, DevState *state, int mode, int s
                         cudaStream_t s) {
 #define DNS_BFINE(M)                                                      \
   case M:                                                                 \
-    b_fine<M, 1><<<g.fbulk, kThreads, 0, s>>>(m, dyn, state, sub);        \
-    b_fine<M, 2><<<g.fadj, kThreads, 0, s>>>(m, dyn, state, sub);         \
-    b_fine<M, 0><<<g.fedge, kThreads, 0, s>>>(m, dyn, state, sub);        \
+    b_fine<M><<<g.fine, kThreads, 0, s>>>(m, dyn, state, sub);            \
     break;
   switch (mode) {
     DNS_BFINE(0)
@@ -662,8 +707,7 @@ void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned 
     b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
     b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
   }
-  b_coarse<true><<<g.cbulk, kThreads, 0, s>>>(m, dyn, state);
-  b_coarse<false><<<g.cedge, kThreads, 0, s>>>(m, dyn, state);
+  b_coarse<<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
   b_extract<<<g.extract, kThreads, 0, s>>>(m, dyn);
   for (int sub = 1; sub <= gr; sub++) {
     const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);

@@ -82,7 +82,6 @@ struct dns_handle {
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
   long sample_every = 0;
-  long nsampled = 0;                   // samples taken since the last statistics reset
   std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
   long wall_gen = 0;                     // bumped whenever wall_lo / wall_hi change
   Profiler prof;
@@ -1061,10 +1060,10 @@ static size_t hslot_elems(const dns_handle *h) { return 2ull * 23 * h->d.ny * h-
 static void L_coarse(dns_handle *h, int src, int dst, bool sample, cudaStream_t st) {
   if (is_f32(h))
     launch_coarse_f32(F(h->fc[src]), F(h->fc[dst]), h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl,
-                      sample, h->stats_acc, st);
+                      sample, st);
   else
     launch_coarse_f64(h->fc[src], h->fc[dst], h->d, h->shape, h->g.omega_c, h->state, h->partials, h->pl, sample,
-                      h->stats_acc, st);
+                      st);
 }
 static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
   if (is_f32(h))
@@ -1075,10 +1074,10 @@ static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
 static void L_fine(dns_handle *h, int src, int dst, bool first, bool last, bool stats, cudaStream_t st) {
   if (is_f32(h))
     launch_fine_f32(F(h->ff[src]), F(h->ff[dst]), h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials,
-                    h->pl, first, last, stats, h->stats_acc, st);
+                    h->pl, first, last, stats, st);
   else
     launch_fine_f64(h->ff[src], h->ff[dst], h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials, h->pl,
-                    first, last, stats, h->stats_acc, st);
+                    first, last, stats, st);
 }
 static void L_iface(dns_handle *h, int fbuf, int it, cudaStream_t st) {
   const size_t hs = hslot_elems(h);
@@ -1290,16 +1289,7 @@ extern "C" int dns_step(dns_handle *h, long ncoarse, dns_step_log *log) {
     const long ss0 = h->ss;
     for (long q = 0; q < n; q++) {
       const bool sample = h->sample_every > 0 && (h->ss % h->sample_every) == 0;
-      if (sample && h->nsampled == 0) {
-        // the first sample after a reset: the plane means of this state become
-        // the shift every sample is summed about
-        if (is_f32(h))
-          launch_stat_shift_f32(F(h->fc[h->cur_c]), F(h->ff[h->cur_f]), h->d, h->stats_acc, h->stream);
-        else
-          launch_stat_shift_f64(h->fc[h->cur_c], h->ff[h->cur_f], h->d, h->stats_acc, h->stream);
-      }
       issue_step(h, h->dlog + q, sample);
-      if (sample) h->nsampled++;
       h->ss++;
     }
     CUDA_TRY(cudaGetLastError());
@@ -1343,7 +1333,6 @@ extern "C" int dns_stats_reset(dns_handle *h) {
   CUDA_TRY(cudaSetDevice(h->p.device));
   CUDA_TRY(cudaMemsetAsync(h->stats_acc, 0, (size_t)h->g.nz_profile * kStatRow * 8, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
-  h->nsampled = 0;
   return DNS_OK;
 }
 
@@ -1371,19 +1360,20 @@ void dns::stats_from_acc(const dns_geometry &g, const double *acc, double *out, 
     out[0 * NZ + p] = z[p];
     const double S = a[15], N = a[14];
     if (S <= 0 || N <= 0) continue;
-    const double T = S * N;  // samples x nodes
-    // sums are taken about the shift a[16..19]: the means add it back, the
-    // second moments about the mean do not depend on it
-    const double du = a[0] / T, dv = a[1] / T, dw = a[2] / T;
+    // plane means: the first sample's plus the mean offset; per-sample
+    // moments: their time means (statistics.c with time_stat.c's averaging);
+    // about the time-and-plane mean: the mean per-sample variance plus the
+    // variance of the plane means over the samples
+    const double du = a[0] / S, dv = a[1] / S, dw = a[2] / S;
     out[1 * NZ + p] = a[16] + du;
     out[2 * NZ + p] = a[17] + dv;
     out[3 * NZ + p] = a[18] + dw;
-    out[4 * NZ + p] = a[19] + a[3] / T;
+    out[4 * NZ + p] = a[19] + a[3] / S;
     for (int c = 0; c < 5; c++) out[(5 + c) * NZ + p] = a[9 + c] / S;
-    out[10 * NZ + p] = a[4] / T - du * du;
-    out[11 * NZ + p] = a[5] / T - dv * dv;
-    out[12 * NZ + p] = a[6] / T - dw * dw;
-    out[13 * NZ + p] = a[7] / T - du * dw;
+    out[10 * NZ + p] = a[9] / S + (a[4] / S - du * du);
+    out[11 * NZ + p] = a[10] / S + (a[5] / S - dv * dv);
+    out[12 * NZ + p] = a[11] / S + (a[6] / S - dw * dw);
+    out[13 * NZ + p] = a[12] / S + (a[7] / S - du * dw);
   }
 }
 

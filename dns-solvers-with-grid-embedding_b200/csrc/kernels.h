@@ -11,16 +11,22 @@
 
 namespace dns {
 
-// Running statistics of one composite-profile plane, kStatRow doubles:
-//   0..8   sums over samples of the plane sums of (u - su), (v - sv), (w - sw),
-//          (rho - sr) and of the products uu, vv, ww, uw, rr of those
-//          differences (moments about the shift);
+// Running statistics of one composite-profile plane, kStatRow doubles.  Each
+// sample's plane moments are exact two-pass quantities: every block keeps a
+// running (count, means, sums of squared deviations) per thread (Welford) and
+// merges them pairwise (Chan, Golub and LeVeque's parallel update), so a
+// plane's variance is never formed as E[x^2] - E[x]^2.  The row holds:
+//   0..3   sums over samples of (m - c) for the plane means m of u, v, w, rho;
+//   4..8   sums over samples of (mu - cu)^2, (mv - cv)^2, (mw - cw)^2,
+//          (mu - cu)(mw - cw), (mr - cr)^2 (the plane means' time variation);
 //   9..13  sums over samples of the per-sample plane variances of u, v, w, the
 //          covariance uw and the variance of rho;
 //   14     nodes per plane; 15 samples;
-//   16..19 the shift (su, sv, sw, sr): the plane means of the first sample after
-//          a reset.  Summing about a value near the mean keeps the one-pass
-//          variance E[x^2] - E[x]^2 from cancelling the mean's square away.
+//   16..19 c = (cu, cv, cw, cr): the plane means of the first sample after a
+//          reset, about which the plane means are summed.
+// Per-block partials of one sample: kStatPart doubles, (n, 4 means, 5 sums of
+// squared deviations).
+constexpr int kStatPart = 10;
 constexpr int kStatRow = 20;
 
 // Device-side scalar state carried between steps (one instance per handle).
@@ -75,16 +81,15 @@ struct StepParams {
 };
 
 // --- FP64 kernels (kernels_f64.cu) ---
-// stats: also the plane sums of the sampled statistics, about the shift held in
-// the running-statistics rows srow[nz_profile][kStatRow]
+// stats: also the per-block moments of the sampled statistics (kStatPart doubles per block)
 void launch_coarse_f64(const double *src, double *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
-                       const double *srow, cudaStream_t stream);
+                       cudaStream_t stream);
 void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s,
                         cudaStream_t stream);
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
-                     bool last, bool stats, const double *srow, cudaStream_t stream);
+                     bool last, bool stats, cudaStream_t stream);
 // two launches: macroscopic fields into mac[2 walls][4][nyf][nxf], then one
 // block per (tile, wall, population) into the interface planes of fdst
 void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *mac, double *fdst,
@@ -100,9 +105,6 @@ void launch_finalize(DevState *st, DevLog *log_row, double *partials, unsigned i
                      cudaStream_t stream);
 void launch_stats_finalize(double *acc, const double *partials, const PartialLayout &pl, const Dims &d,
                            const LaunchShape &s, cudaStream_t stream);
-// the statistics rows' shift (plane means of u, v, w, rho) from a stored state
-void launch_stat_shift_f64(const double *fc, const double *ff, const Dims &d, double *rows, cudaStream_t stream);
-void launch_stat_shift_f32(const float *fc, const float *ff, const Dims &d, double *rows, cudaStream_t stream);
 // direct encalc2 reduction of the stored state into st (momentum, denst, force)
 void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,
                           const PartialLayout &pl, const Dims &d, const LaunchShape &s, const StepParams &sp,
@@ -167,11 +169,11 @@ void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, in
 // --- FP32 deviation-storage kernels (kernels_f32.cu); same layouts in float ---
 void launch_coarse_f32(const float *src, float *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
-                       const double *srow, cudaStream_t stream);
+                       cudaStream_t stream);
 void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream);
 void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first, bool last,
-                     bool stats, const double *srow, cudaStream_t stream);
+                     bool stats, cudaStream_t stream);
 // corner: scratch of 2 x 23 x ny x nx float4 (corner values and derivatives)
 void launch_interface_f32(const float *hn, const float *hp, const float *hpp, float *corner, float *fdst,
                           const Dims &d, int substep, double omega_c, double omega_f, cudaStream_t stream);

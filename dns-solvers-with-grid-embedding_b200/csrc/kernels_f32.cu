@@ -17,7 +17,7 @@ template <bool STATS, bool BULK>
 __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) coarse_f32(const float *__restrict__ src, float *__restrict__ dst, Dims d,
                                                       int jb, float om, const DevState *st,
                                                       double *__restrict__ part, double *__restrict__ spart,
-                                                      int k0, const double *__restrict__ srow) {
+                                                      int k0) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   // BULK: planes k0 + z for z < gridDim.z (k0 = 2); edge: planes 0, 1, zdc-2, zdc-1
@@ -27,7 +27,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) coarse
   const float G = (float)st->force;
   double acc[2] = {0., 0.};
   PlaneStat sacc;
-  sacc.init(srow, profile_index_coarse(k, d.zdf), STATS && k >= 2 && k <= nzc - 3);
+  sacc.init();
   for (int r = 0; r < jb; r++) {
     const int j = blockIdx.y * jb + r;
     if (i >= nx || j >= ny) continue;
@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(kThreads, BULK ? DNS_F32_BULK_MINB : 0) coarse
   }
   const size_t blk = ((size_t)k * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   block_reduce32<2>(acc, part + blk * 2);
-  if (STATS) block_reduce32<9>(sacc.s, spart + blk * 9);
+  if (STATS) block_reduce_stat(sacc, spart + blk * kStatPart);
 }
 
 __global__ void __launch_bounds__(kThreads) extract_f32(const float *__restrict__ fc, float *__restrict__ hn, Dims d) {
@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
                                                     const int8_t *__restrict__ wf, Dims d, int jb, float om,
                                                     const DevState *st, double *__restrict__ part,
                                                     double *__restrict__ wpart, double *__restrict__ spart,
-                                                    PlaneList pls, const double *__restrict__ srow) {
+                                                    PlaneList pls) {
   const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
   const int P = 2 * zds;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -93,7 +93,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
   const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
   PlaneStat sacc;
-  sacc.init(srow, profile_index_fine(p, zds, zdf, d.nzc), (MODE & 4) != 0);
+  sacc.init();
   float wz[3] = {0.f, 0.f, 0.f};
   {
     // destination planes k - 1, k, k + 1 (encalc2.c:33-53, 86-107)
@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
   const size_t blk = ((size_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce32<2>(acc, part + blk * 2);
   if ((MODE & 2) && wall_sum_plane) block_reduce32<2>(wacc, wpart + blk * 2);
-  if (MODE & 4) block_reduce32<9>(sacc.s, spart + blk * 9);
+  if (MODE & 4) block_reduce_stat(sacc, spart + blk * kStatPart);
 }
 
 // ------------------------------------------------------------------ interface
@@ -395,63 +395,22 @@ __global__ void fields_f32_kernel(const float *__restrict__ soa, double *__restr
   den[o] = dens;
 }
 
-// Shift of the running statistics from the stored deviations (as
-// stat_shift_kernel in kernels_f64.cu): plane means of u, v, w and rho.
-__global__ void __launch_bounds__(256) stat_shift_f32_kernel(const float *__restrict__ fc, const float *__restrict__ ff,
-                                                             Dims d, double *__restrict__ rows) {
-  int level, plane;
-  profile_plane(blockIdx.x, d.zds, d.zdf, d.nzc, level, plane);
-  if (level < 0) return;
-  const int nx = level ? d.nxf : d.nx, ny = level ? d.nyf : d.ny;
-  const size_t pstride = level ? (size_t)2 * d.zds * d.nyf * d.nxf : (size_t)d.nzc * d.ny * d.nx;
-  const float *base = (level ? ff : fc) + (size_t)plane * ny * nx;
-  double v[4] = {0., 0., 0., 0.};
-  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-    float f[19];
-    load19f(base, (size_t)q, pstride, f);
-    const Mac32 m = macro_f32(f);
-    v[0] += m.u0;
-    v[1] += m.u1;
-    v[2] += m.u2;
-    v[3] += 1.0 + (double)m.drho;
-  }
-  __shared__ double red[4][8];
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-  for (int c = 0; c < 4; c++) {
-    double x = v[c];
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if (lane == 0) red[c][warp] = x;
-  }
-  __syncthreads();
-  if (threadIdx.x < 4) {
-    double x = 0.;
-    for (int w = 0; w < 8; w++) x += red[threadIdx.x][w];
-    rows[(size_t)blockIdx.x * kStatRow + 16 + threadIdx.x] = x / ((double)nx * ny);
-  }
-}
-
 }  // namespace
 
 // ====================================================================== host
 void launch_coarse_f32(const float *src, float *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
-                       const double *srow, cudaStream_t stream) {
+                       cudaStream_t stream) {
   dim3 gb(s.cgx, s.cgy, d.nzc - 4), ge(s.cgx, s.cgy, 4), block(s.bx);
   double *pc = partials + pl.coarse, *ps = partials + pl.stats_c;
   const float omf = (float)om;
   if (stats) {
-    coarse_f32<true, true><<<gb, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 2, srow);
-    coarse_f32<true, false><<<ge, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 0, srow);
+    coarse_f32<true, true><<<gb, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 2);
+    coarse_f32<true, false><<<ge, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 0);
   } else {
-    coarse_f32<false, true><<<gb, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 2, srow);
-    coarse_f32<false, false><<<ge, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 0, srow);
+    coarse_f32<false, true><<<gb, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 2);
+    coarse_f32<false, false><<<ge, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 0);
   }
-}
-
-void launch_stat_shift_f32(const float *fc, const float *ff, const Dims &d, double *rows, cudaStream_t stream) {
-  stat_shift_f32_kernel<<<2 * d.zdf + d.nzc - 4, 256, 0, stream>>>(fc, ff, d, rows);
 }
 
 void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream) {
@@ -461,7 +420,7 @@ void launch_extract_f32(const float *fc, float *hist_n, const Dims &d, const Lau
 
 void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first, bool last,
-                     bool stats, const double *srow, cudaStream_t stream) {
+                     bool stats, cudaStream_t stream) {
   PlaneList bulk{}, edge{}, adj{};
   for (int p = 0; p < 2 * d.zds; p++) {
     const bool upper = p >= d.zds;
@@ -476,9 +435,9 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
   dim3 gb(s.fgx, s.fgy, bulk.n), ge(s.fgx, s.fgy, edge.n), ga(s.fgx, s.fgy, adj.n), block(s.bx);
 #define FINE32_CASE(M)                                                                                       \
   case M:                                                                                                    \
-    if (bulk.n) fine_f32<M, 1><<<gb, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, bulk, srow); \
-    fine_f32<M, 2><<<ga, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, adj, srow);      \
-    fine_f32<M, 0><<<ge, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, edge, srow);     \
+    if (bulk.n) fine_f32<M, 1><<<gb, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, bulk); \
+    fine_f32<M, 2><<<ga, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, adj);      \
+    fine_f32<M, 0><<<ge, block, 0, stream>>>(src, dst, wflag, d, s.jb, omf, st, pf, pw, ps, edge);     \
     break;
   switch (mode) {
     FINE32_CASE(0) FINE32_CASE(1) FINE32_CASE(2) FINE32_CASE(3) FINE32_CASE(4) FINE32_CASE(5) FINE32_CASE(6)

@@ -107,17 +107,15 @@ __device__ __forceinline__ void load19(const double *__restrict__ src, size_t id
 template <bool STATS>
 __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                             Dims d, int jb, double om, const DevState *st,
-                                                            double *__restrict__ part, double *__restrict__ spart,
-                                                            const double *__restrict__ srow) {
+                                                            double *__restrict__ part, double *__restrict__ spart) {
   const int nx = d.nx, ny = d.ny, nzc = d.nzc;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const int k = blockIdx.z;
   const size_t pstride = (size_t)nzc * ny * nx;
   const double G = st->force;
   double acc[2] = {0., 0.};
-  PlaneStat sacc;
-  // planes 2..zdc-3 are profile points; the others' sums are not read
-  sacc.init(srow, profile_index_coarse(k, d.zdf), STATS && k >= 2 && k <= nzc - 3);
+  PlaneStat sacc;  // planes 2..zdc-3 are profile points; the others' moments are not read
+  sacc.init();
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   for (int r = 0; r < jb; r++) {
     const int j = blockIdx.y * jb + r;
@@ -142,7 +140,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_COARSE) coarse_kernel(co
   }
   const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   block_reduce<2>(acc, part + blk * 2);
-  if (STATS) block_reduce<9>(sacc.s, spart + blk * 9);
+  if (STATS) block_reduce_stat(sacc, spart + blk * kStatPart);
 }
 
 // Interface planes of the new coarse state into history level n
@@ -188,8 +186,7 @@ template <int MODE>
 __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                           const int8_t *__restrict__ wf, Dims d, int jb, double om,
                                                           const DevState *st, double *__restrict__ part,
-                                                          double *__restrict__ wpart, double *__restrict__ spart,
-                                                          const double *__restrict__ srow) {
+                                                          double *__restrict__ wpart, double *__restrict__ spart) {
   const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
   const int P = 2 * zds;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -215,7 +212,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   const bool unit_plane = upper ? (k >= gr + 2 && k <= zdf - 3) : (k >= 2 && k <= zdf - gr - 2);
   double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
   PlaneStat sacc;
-  sacc.init(srow, profile_index_fine(p, zds, zdf, d.nzc), (MODE & 4) != 0);
+  sacc.init();
   const int im = i == 0 ? nx - 1 : i - 1, ip = i == nx - 1 ? 0 : i + 1;
   for (int r = 0; r < jb; r++) {
     const int j = blockIdx.y * jb + r;
@@ -266,7 +263,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce<2>(acc, part + blk * 2);
   if ((MODE & 2) && wall_sum_plane) block_reduce<2>(wacc, wpart + blk * 2);
-  if (MODE & 4) block_reduce<9>(sacc.s, spart + blk * 9);
+  if (MODE & 4) block_reduce_stat(sacc, spart + blk * kStatPart);
 }
 
 // ------------------------------------------------------------------ interface
@@ -777,62 +774,20 @@ struct StatsArgs {
 
 __global__ void __launch_bounds__(256) stats_finalize_kernel(double *acc, const double *spc, const double *spf,
                                                             StatsArgs a) {
-  __shared__ double sh[256];
   const int idx = blockIdx.x;
   const double *src = nullptr;
   long nb = 0;
-  double nn = 0.;
   const int zdf = a.zdf, nzc = a.nzc;
   if (idx >= 1 && idx <= zdf - 1) {  // lower fine k = idx
-    src = spf + (size_t)(idx - 1) * a.bf * 9; nb = a.bf; nn = a.nf;
+    src = spf + (size_t)(idx - 1) * a.bf * kStatPart; nb = a.bf;
   } else if (idx >= zdf && idx <= zdf + nzc - 5) {  // coarse k = idx - zdf + 2
-    src = spc + (size_t)(idx - zdf + 2) * a.bc * 9; nb = a.bc; nn = a.nc;
+    src = spc + (size_t)(idx - zdf + 2) * a.bc * kStatPart; nb = a.bc;
   } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {  // upper fine k
     const int k = idx - (zdf + nzc - 4);
-    src = spf + (size_t)(a.zds + k) * a.bf * 9; nb = a.bf; nn = a.nf;
+    src = spf + (size_t)(a.zds + k) * a.bf * kStatPart; nb = a.bf;
   }
   if (!src) return;
-  double s9[9];
-  for (int c = 0; c < 9; c++) {
-    double s = 0.;
-    for (long q = threadIdx.x; q < nb; q += blockDim.x) s += src[q * 9 + c];
-    sh[threadIdx.x] = s;
-    __syncthreads();
-    for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
-      __syncthreads();
-    }
-    s9[c] = sh[0];
-    __syncthreads();
-  }
-  if (threadIdx.x == 0) stat_row_add(acc + (size_t)idx * kStatRow, s9, nn);
-}
-
-// Shift of the running statistics: the plane means of u, v, w and rho of the
-// stored state, one block per composite-profile point, written into the rows'
-// entries 16..19 before the first sample after a reset.
-__global__ void __launch_bounds__(256) stat_shift_kernel(const double *__restrict__ fc, const double *__restrict__ ff,
-                                                         Dims d, double *__restrict__ rows) {
-  int level, plane;
-  profile_plane(blockIdx.x, d.zds, d.zdf, d.nzc, level, plane);
-  if (level < 0) return;
-  const int nx = level ? d.nxf : d.nx, ny = level ? d.nyf : d.ny;
-  const size_t pstride = level ? (size_t)2 * d.zds * d.nyf * d.nxf : (size_t)d.nzc * d.ny * d.nx;
-  const double *base = (level ? ff : fc) + (size_t)plane * ny * nx;
-  double v[4] = {0., 0., 0., 0.};
-  for (int q = threadIdx.x; q < nx * ny; q += blockDim.x) {
-    double f[19];
-    load19(base, (size_t)q, pstride, f);
-    double dens, mx, my, mz;
-    moments_f64(f, dens, mx, my, mz);
-    v[0] += mx / dens;
-    v[1] += my / dens;
-    v[2] += mz / dens;
-    v[3] += dens;
-  }
-  __shared__ double out[4];
-  block_reduce_n<4, 256>(v, out);
-  if (threadIdx.x < 4) rows[(size_t)blockIdx.x * kStatRow + 16 + threadIdx.x] = out[threadIdx.x] / ((double)nx * ny);
+  stat_plane_finalize(src, nb, acc + (size_t)idx * kStatRow);
 }
 
 // ------------------------------------------------------------------ seeded state
@@ -1000,8 +955,8 @@ PartialLayout partial_layout(const Dims &d, const LaunchShape &s) {
   pl.fine = o; o += nbf * 2;
   pl.inject = o; o += nbi * 2;
   pl.wall = o; o += nbf * 2;
-  pl.stats_c = o; o += nbc * 9;
-  pl.stats_f = o; o += nbf * 9;
+  pl.stats_c = o; o += nbc * kStatPart;
+  pl.stats_f = o; o += nbf * kStatPart;
   const long gx = s.fgx > s.cgx ? s.fgx : s.cgx, gy = s.fgy > s.cgy ? s.fgy : s.cgy;
   pl.flow = o; o += gx * gy * (d.nzc + 2 * d.zds) * 2;
   pl.level2 = o; o += kFin2Blocks * kFin2Comp;
@@ -1011,14 +966,14 @@ PartialLayout partial_layout(const Dims &d, const LaunchShape &s) {
 
 void launch_coarse_f64(const double *src, double *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
-                       const double *srow, cudaStream_t stream) {
+                       cudaStream_t stream) {
   dim3 grid(s.cgx, s.cgy, d.nzc), block(s.bx);
   if (stats)
     coarse_kernel<true><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
-                                                    partials + pl.stats_c, srow);
+                                                    partials + pl.stats_c);
   else
     coarse_kernel<false><<<grid, block, 0, stream>>>(src, dst, d, s.jb, om, st, partials + pl.coarse,
-                                                     partials + pl.stats_c, srow);
+                                                     partials + pl.stats_c);
 }
 
 void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s, cudaStream_t stream) {
@@ -1028,12 +983,12 @@ void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const L
 
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
-                     bool last, bool stats, const double *srow, cudaStream_t stream) {
+                     bool last, bool stats, cudaStream_t stream) {
   dim3 grid(s.fgx, s.fgy, 2 * d.zds), block(s.bx);
   const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
   double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
 #define FINE_CASE(M) \
-  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps, srow); break;
+  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps); break;
   switch (mode) {
     FINE_CASE(0) FINE_CASE(1) FINE_CASE(2) FINE_CASE(3) FINE_CASE(4) FINE_CASE(5) FINE_CASE(6) FINE_CASE(7)
   }
@@ -1121,10 +1076,6 @@ void launch_stats_finalize(double *acc, const double *partials, const PartialLay
   a.nc = (double)d.nx * d.ny;
   a.nf = (double)d.nxf * d.nyf;
   stats_finalize_kernel<<<a.nzp, 256, 0, stream>>>(acc, partials + pl.stats_c, partials + pl.stats_f, a);
-}
-
-void launch_stat_shift_f64(const double *fc, const double *ff, const Dims &d, double *rows, cudaStream_t stream) {
-  stat_shift_kernel<<<2 * d.zdf + d.nzc - 4, 256, 0, stream>>>(fc, ff, d, rows);
 }
 
 void launch_flow_sums_f64(const double *fc, const double *ff, DevState *st, double *partials,

@@ -144,81 +144,137 @@ __device__ __forceinline__ void collide_f64(double (&f)[19], double om, double G
 
 
 // ------------------------------------------------------------------ sampled statistics
-// Composite-profile index of coarse plane k (k = 2..zdc-3) and of fine device
-// plane p (lower block k = p + 1, upper block k = p - zds), statistics.c:52-146;
-// profile_plane inverts them: level (0 coarse, 1 fine) and plane (coarse k or
-// fine device plane) of index idx, or level -1 for the two wall points.
-__host__ __device__ __forceinline__ int profile_index_coarse(int k, int zdf) { return zdf - 2 + k; }
-__host__ __device__ __forceinline__ int profile_index_fine(int p, int zds, int zdf, int nzc) {
-  return p < zds ? p + 1 : zdf + nzc - 4 + (p - zds);
-}
-__host__ __device__ __forceinline__ void profile_plane(int idx, int zds, int zdf, int nzc, int &level, int &plane) {
-  level = -1;
-  plane = 0;
-  if (idx >= 1 && idx <= zdf - 1) {
-    level = 1;
-    plane = idx - 1;
-  } else if (idx >= zdf && idx <= zdf + nzc - 5) {
-    level = 0;
-    plane = idx - zdf + 2;
-  } else if (idx >= zdf + nzc - 4 && idx <= 2 * zdf + nzc - 6) {
-    level = 1;
-    plane = zds + idx - (zdf + nzc - 4);
-  }
-}
-
-// One block's sums of the sampled moments of its nodes, taken about the plane's
-// shift (the running-statistics row's entries 16..19).
+// Moments of a set of nodes' u, v, w, rho: count n, means m and sums of
+// squared deviations from the means q = (uu, vv, ww, uw, rr).  add() is
+// Welford's update, merge() the pairwise combination of Chan, Golub and
+// LeVeque (1979); neither forms E[x^2] - E[x]^2, so a small variance under a
+// large mean keeps its digits.
 struct PlaneStat {
-  double s[9];
-  double sh[4];
-  __device__ __forceinline__ void init(const double *rows, int idx, bool on) {
+  double n, m[4], q[5];
+  __device__ __forceinline__ void init() {
+    n = 0.;
 #pragma unroll
-    for (int c = 0; c < 9; c++) s[c] = 0.;
+    for (int c = 0; c < 4; c++) m[c] = 0.;
 #pragma unroll
-    for (int c = 0; c < 4; c++) sh[c] = on ? rows[(size_t)idx * kStatRow + 16 + c] : 0.;
+    for (int c = 0; c < 5; c++) q[c] = 0.;
   }
   __device__ __forceinline__ void add(double u0, double u1, double u2, double rho) {
-    const double a = u0 - sh[0], b = u1 - sh[1], c = u2 - sh[2], r = rho - sh[3];
-    s[0] += a; s[1] += b; s[2] += c; s[3] += r;
-    s[4] += a * a; s[5] += b * b; s[6] += c * c; s[7] += a * c; s[8] += r * r;
+    n += 1.;
+    const double inv = 1. / n;
+    const double d0 = u0 - m[0], d1 = u1 - m[1], d2 = u2 - m[2], d3 = rho - m[3];
+    m[0] += d0 * inv;
+    m[1] += d1 * inv;
+    m[2] += d2 * inv;
+    m[3] += d3 * inv;
+    q[0] += d0 * (u0 - m[0]);
+    q[1] += d1 * (u1 - m[1]);
+    q[2] += d2 * (u2 - m[2]);
+    q[3] += d0 * (u2 - m[2]);
+    q[4] += d3 * (rho - m[3]);
+  }
+  __device__ __forceinline__ void merge(double nb, const double (&mb)[4], const double (&qb)[5]) {
+    if (nb == 0.) return;
+    if (n == 0.) {
+      n = nb;
+#pragma unroll
+      for (int c = 0; c < 4; c++) m[c] = mb[c];
+#pragma unroll
+      for (int c = 0; c < 5; c++) q[c] = qb[c];
+      return;
+    }
+    const double nt = n + nb, f = nb / nt, g = n * f;
+    const double d0 = mb[0] - m[0], d1 = mb[1] - m[1], d2 = mb[2] - m[2], d3 = mb[3] - m[3];
+    q[0] += qb[0] + d0 * d0 * g;
+    q[1] += qb[1] + d1 * d1 * g;
+    q[2] += qb[2] + d2 * d2 * g;
+    q[3] += qb[3] + d0 * d2 * g;
+    q[4] += qb[4] + d3 * d3 * g;
+    m[0] += d0 * f;
+    m[1] += d1 * f;
+    m[2] += d2 * f;
+    m[3] += d3 * f;
+    n = nt;
+  }
+  __device__ __forceinline__ void merge(const double *p) {  // a stored (n, m[4], q[5])
+    const double mb[4] = {p[1], p[2], p[3], p[4]}, qb[5] = {p[5], p[6], p[7], p[8], p[9]};
+    merge(p[0], mb, qb);
+  }
+  __device__ __forceinline__ void store(double *p) const {
+    p[0] = n;
+#pragma unroll
+    for (int c = 0; c < 4; c++) p[1 + c] = m[c];
+#pragma unroll
+    for (int c = 0; c < 5; c++) p[5 + c] = q[c];
   }
 };
 
-// Add one sample's plane sums s9 (taken about the row's shift) to the row o of
-// nn nodes.  A row without a shift (o[19], the mean density, still zero: the
-// single-channel forms set the shift from the state before their first sample,
-// the batched engine does not) took this sample about zero: its sums are
-// re-centred on its own plane means, which become the shift of every later
-// sample.  The per-sample variances do not depend on the shift.
-__device__ __forceinline__ void stat_row_add(double *o, const double (&s9)[9], double nn) {
-  const double mu = s9[0] / nn, mv = s9[1] / nn, mw = s9[2] / nn, mr = s9[3] / nn;
-  const double var[5] = {s9[4] / nn - mu * mu, s9[5] / nn - mv * mv, s9[6] / nn - mw * mw, s9[7] / nn - mu * mw,
-                         s9[8] / nn - mr * mr};
-  double t[9];
+// Merge the block's PlaneStats in a fixed order (warp shuffles, then the
+// warps in order) and store the result (kStatPart doubles) at out.  Every
+// thread of the block must call it; blockDim.x is a multiple of 32, at most 1024.
+__device__ __forceinline__ void block_reduce_stat(PlaneStat st, double *out) {
+  __shared__ double red[32][kStatPart];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 #pragma unroll
-  for (int c = 0; c < 9; c++) t[c] = s9[c];
-  if (o[19] == 0.) {
-    t[0] = s9[0] - nn * mu;
-    t[1] = s9[1] - nn * mv;
-    t[2] = s9[2] - nn * mw;
-    t[3] = s9[3] - nn * mr;
-    t[4] = s9[4] - nn * (mu * mu);
-    t[5] = s9[5] - nn * (mv * mv);
-    t[6] = s9[6] - nn * (mw * mw);
-    t[7] = s9[7] - nn * (mu * mw);
-    t[8] = s9[8] - nn * (mr * mr);
-    o[16] = mu;
-    o[17] = mv;
-    o[18] = mw;
-    o[19] = mr;
+  for (int o = 16; o > 0; o >>= 1) {
+    const double nb = __shfl_down_sync(0xffffffffu, st.n, o);
+    double mb[4], qb[5];
+#pragma unroll
+    for (int c = 0; c < 4; c++) mb[c] = __shfl_down_sync(0xffffffffu, st.m[c], o);
+#pragma unroll
+    for (int c = 0; c < 5; c++) qb[c] = __shfl_down_sync(0xffffffffu, st.q[c], o);
+    if (lane + o < 32) st.merge(nb, mb, qb);
   }
+  if (lane == 0) st.store(red[warp]);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    PlaneStat t;
+    t.init();
+    for (int w = 0; w < nw; w++) t.merge(red[w]);
+    t.store(out);
+  }
+  __syncthreads();
+}
+
+// Add one sample's plane moments s (n, means, sums of squared deviations) to
+// the running-statistics row o (layout in kernels.h).  The first sample after
+// a reset sets the reference c of the plane means.
+__device__ __forceinline__ void stat_row_add(double *o, const PlaneStat &s) {
+  if (o[15] == 0.) {
 #pragma unroll
-  for (int c = 0; c < 9; c++) o[c] += t[c];
+    for (int c = 0; c < 4; c++) o[16 + c] = s.m[c];
+  }
+  const double d0 = s.m[0] - o[16], d1 = s.m[1] - o[17], d2 = s.m[2] - o[18], d3 = s.m[3] - o[19];
+  o[0] += d0;
+  o[1] += d1;
+  o[2] += d2;
+  o[3] += d3;
+  o[4] += d0 * d0;
+  o[5] += d1 * d1;
+  o[6] += d2 * d2;
+  o[7] += d0 * d2;
+  o[8] += d3 * d3;
+  const double inv = 1. / s.n;
 #pragma unroll
-  for (int c = 0; c < 5; c++) o[9 + c] += var[c];
-  o[14] = nn;
+  for (int c = 0; c < 5; c++) o[9 + c] += s.q[c] * inv;
+  o[14] = s.n;
   o[15] += 1.0;
+}
+
+// Per-plane finalize of one sample: merge the plane's nb block partials (each
+// kStatPart doubles) in a fixed order (thread t takes blocks t, t + T, ...,
+// then the threads in order) and add the plane's moments to the row.
+__device__ __forceinline__ void stat_plane_finalize(const double *parts, long nb, double *row) {
+  PlaneStat st;
+  st.init();
+  for (long q = threadIdx.x; q < nb; q += blockDim.x) st.merge(parts + q * kStatPart);
+  __shared__ double part[kStatPart];
+  block_reduce_stat(st, part);
+  if (threadIdx.x == 0) {
+    PlaneStat t;
+    t.init();
+    t.merge(part);
+    stat_row_add(row, t);
+  }
 }
 
 }  // namespace dns

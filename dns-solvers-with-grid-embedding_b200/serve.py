@@ -133,6 +133,38 @@ class Server:
         return recs
 
 
+def serve_one_at_a_time(pkg, requests, clock=time.perf_counter, sleep=time.sleep, sample_every: int = 20,
+                        device: int = 0):
+    """The baseline the continuous-batching loop is compared with: the same
+    requests served one at a time, first come first served, each by the FP64
+    plain form on its own channel handle (allocated on arrival at the head of
+    the queue, stepped through its whole budget, results read back, freed).
+    Latency = completion - arrival on the host clock, as Server.run."""
+    recs = [Record(inst=r, arrival=r.arrival) for r in sorted(requests, key=lambda r: r.arrival)]
+    t0 = clock()
+    for rec in recs:
+        now = clock() - t0
+        if now < rec.arrival:
+            sleep(rec.arrival - now)
+        rec.admitted = clock() - t0
+        p = rec.inst.params(pkg, precision=pkg.FP64)
+        p.device = device
+        with pkg.Channel(p) as ch:
+            ch.init_seeded(rec.inst.seed, workloads.UC, workloads.AMP)
+            ch.set_sampling(sample_every)
+            try:
+                log = ch.step(rec.inst.steps)
+            except pkg.DnsError as e:
+                rec.status = e.code
+                log = None
+            if rec.status == 0:
+                stats, _ = ch.stats()
+                rec.result = workloads.solve_result(rec.inst, stats, log, ch.geom.zdf)
+            rec.result["steps"] = int(rec.inst.steps)
+        rec.finished = clock() - t0
+    return recs
+
+
 def latency_summary(recs) -> dict:
     lat = np.array([r.latency for r in recs if r.status == 0])
     if lat.size == 0:
@@ -144,7 +176,8 @@ def latency_summary(recs) -> dict:
 
 def fifo_latencies(arrivals, services) -> np.ndarray:
     """Latencies of a single server taking requests one at a time, first come
-    first served: finish_i = max(arrival_i, finish_{i-1}) + service_i."""
+    first served: finish_i = max(arrival_i, finish_{i-1}) + service_i (a
+    model, used by the host tests to check serve_one_at_a_time's clock)."""
     fin = 0.0
     out = []
     for a, s in zip(arrivals, services):

@@ -260,8 +260,9 @@ int dns_flow_sums_static(const dns_params *p, const double *fc, const double *ff
    other instances share the batch. */
 typedef struct dns_batch dns_batch;
 
-/* Tile shape of one instance: threads per row along x (32, 64 or 128) and row
-   iterations per work item of the coarse (cw, cjb) and fine (fw, fjb) kernels. */
+/* Tile shape of one instance: threads per row along x (8, 16, 32, 64 or 128;
+   each thread updates four consecutive nodes) and row iterations per work item
+   of the coarse (cw, cjb) and fine (fw, fjb) kernels. */
 typedef struct dns_tile {
   int cw, cjb;
   int fw, fjb;
@@ -281,7 +282,9 @@ typedef struct dns_batch_info {
 
 int dns_batch_create(int device, dns_batch **out);
 void dns_batch_destroy(dns_batch *b);
-/* Device bytes an instance of these parameters holds (FP32 form). */
+/* Device bytes an instance of these parameters holds (FP32 form).  The
+   batched engine needs xdv a multiple of 4 (DNS_EINVAL otherwise): its
+   stream-collide kernels move four consecutive nodes with 16-byte accesses. */
 int dns_batch_footprint(const dns_params *p, long long *bytes);
 /* Tile shape an instance of these parameters gets: the batch's tuning-table
    entry for its shape if any (b may be NULL), else a fixed default. */

@@ -11,7 +11,12 @@ mode -i starts of the unmodified reference main from a uniform-grid file, and
 ``tke_golden.json`` the output profiles of the reference's offline budget
 program (TKE-budget/computations) on the fields of a seeded state.
 
-Run from the repository root: ``python tests/golden/make_golden.py``.
+``c1_1000_golden.json`` (``--c1-long``, about four minutes of CPU) holds the
+plain FP64 channel c1 after its stated 1000 coarse steps, run by the
+reference's own routines.
+
+Run from the repository root: ``python tests/golden/make_golden.py`` and
+``python tests/golden/make_golden.py --c1-long``.
 """
 from __future__ import annotations
 
@@ -133,7 +138,67 @@ def run_tke_case(name, steps):
     return {"config": name, "seed": SEED, "uc": UC, "amp": AMP, "g": GCONST, "steps": steps, "profiles": prof}
 
 
+# the plain FP64 channel of the parity configuration (c1: reference macros xdv
+# 64, ydv 64, zdv 27, zds 8, GR 2) run for its stated 1000 coarse steps by the
+# reference's own routines: with the constant body force of Re_tau = 180
+# (g_c = GR u_tau^2 / h_f) the digests of the lattices, which the FP64 form
+# reproduces bit for bit; at constant flow rate, whose whole-domain flow-rate
+# sum is associated differently, per-population plane sums of each lattice
+# and the logged flow rate, compared at 1e-12
+C1_LONG_STEPS = 1000
+
+
+def c1_force(m):
+    nzs = 2 * (int(m["zds"]) + 1) + int(m["gratio"]) * (int(m["zdv"]) - 4) + int(m["gratio"]) - 1
+    tau_f = (3.0 / float(m["Rebs"])) * float(m["ub"]) * (nzs - 2.0) + 0.5
+    nu_f = (tau_f - 0.5) / 3.0
+    h_f = (nzs - 2) / 2.0
+    u_tau = 180.0 * nu_f / h_f
+    return int(m["gratio"]) * u_tau * u_tau / h_f
+
+
+def plane_sums(s: np.ndarray) -> list:
+    """(nx, ny, nz, 19) lattice -> sums over x and y per (z, population), [nz][19]."""
+    return s.sum(axis=(0, 1)).tolist()
+
+
+def run_c1_long(mode):
+    name, n = "c1", C1_LONG_STEPS
+    m = REF_CONFIGS[name]
+    p = port.Port(m)
+    g = c1_force(m) if mode == "const" else 0.0
+    p.init_seeded(SEED, UC, AMP, g)
+    p.set_forcing(mode == "cfr", g)
+    with tempfile.TemporaryDirectory() as d:
+        din, dout = Path(d, "in"), Path(d, "out")
+        din.mkdir()
+        dout.mkdir()
+        p.save(din, 100)
+        exe = ROOT / "oracle" / "_ref" / name / "ref_harness"
+        subprocess.run([str(exe), str(din), "100", str(dout), "101", str(n), mode, g.hex()], check=True,
+                       capture_output=True)
+        nx, ny, zdc, nxf, nyf, zdf = p.nx, p.ny, p.zdc, p.nxf, p.nyf, p.zdf
+        out = {"config": name, "mode": mode, "steps": n, "seed": SEED, "uc": UC, "amp": AMP, "g": g}
+        shapes = {"lbf-c": (nx, ny, zdc, 19), "lbf-slf": (nxf, nyf, zdf, 19), "lbf-suf": (nxf, nyf, zdf, 19)}
+        for fn, sh in shapes.items():
+            a = np.fromfile(dout / f"{fn}.0101")
+            s = a[: a.size // 2].reshape(sh)
+            out[fn] = {"sha256": digest(s), "plane_sums": plane_sums(s)}
+        for w in ("lin", "uin"):
+            h = np.fromfile(dout / f"lbf-{w}.0101").reshape(3, nx, ny, 23)
+            out[f"lbf-{w}"] = {"sha256": digest(h)}
+        out["force_next"] = float(np.fromfile(dout / "force.0101")[0])
+        fl = np.loadtxt(dout / "flowrate.txt")
+        out["flowrate_log"] = [float(x) for x in np.atleast_2d(fl)[:, 1]]
+    return out
+
+
 def main():
+    if "--c1-long" in sys.argv:
+        long_cases = [run_c1_long(mode) for mode in ("const", "cfr")]
+        (Path(__file__).parent / "c1_1000_golden.json").write_text(json.dumps(long_cases))
+        print("wrote the c1 1000-step cases")
+        return
     cases = [run_case(*c) for c in CASES]
     (Path(__file__).parent / "oracle_golden.json").write_text(json.dumps(cases, indent=1))
     print(f"wrote {len(cases)} cases")

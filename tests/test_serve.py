@@ -203,3 +203,57 @@ def test_server_deadline_times_out_resident_and_queued(pkg):
     assert len(never) == 4 and all(r.admitted != r.admitted for r in never)  # NaN: not admitted
     assert all(r.finished >= 0.9 for r in recs[4:])
     assert srv.used == 0 and not fb.inst
+
+
+class FakeChannel:
+    """Stand-in FP64 channel: step(n) moves the virtual clock by 2 ms a step."""
+
+    def __init__(self, clock, p, fail_seed=None):
+        self.clock = clock
+        self.geom = type("G", (), {"zdf": p.zds + 1})
+        self.fail_seed = fail_seed
+        self.seed = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+    def init_seeded(self, seed, uc, amp):
+        self.seed = seed
+
+    def set_sampling(self, every):
+        pass
+
+    def step(self, n):
+        self.clock.t += 2e-3 * n
+        if self.seed == self.fail_seed:
+            raise self.err(-4, "fake: NaN wall shear stress")
+        x = np.ones((n, 9))
+        x[:, 7] = 1e-5
+        return x
+
+    def stats(self):
+        s = np.zeros((14, 20))
+        s[1] = np.linspace(0.01, 0.02, 20)
+        return s, 5
+
+
+def test_one_at_a_time_server_is_first_come_first_served(pkg):
+    import types
+
+    clk = Clock()
+    reqs = W.request_stream(rate=2.0, n=5, seed=8, budget=(300, 600))
+    fail = reqs[3].seed
+    fake = types.SimpleNamespace(FP64=pkg.FP64, DnsError=pkg.DnsError, make_params=pkg.make_params,
+                                 FORCING_CFR=pkg.FORCING_CFR,
+                                 Channel=lambda p: FakeChannel(clk, p, fail_seed=fail))
+    FakeChannel.err = pkg.DnsError
+    recs = S.serve_one_at_a_time(fake, reqs, clock=clk, sleep=clk.sleep)
+    # the same latencies as a single first-come-first-served server with
+    # service = 2 ms x budget
+    lat = S.fifo_latencies([r.arrival for r in recs], [2e-3 * r.inst.steps for r in recs])
+    np.testing.assert_allclose([r.latency for r in recs], lat, rtol=1e-12, atol=1e-12)
+    assert recs[3].status == -4 and "cf" not in recs[3].result
+    assert all(r.status == 0 and "slip_length" in r.result for r in recs if r is not recs[3])
