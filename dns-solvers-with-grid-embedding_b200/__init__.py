@@ -13,12 +13,15 @@ loaded, :func:`lib` raises instead of falling back to any CPU path.
 from __future__ import annotations
 
 import ctypes as C
+import os
 from pathlib import Path
 
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-LIBPATH = HERE / "libdnsembed.so"
+# the in-tree build; DNS_EMBED_LIBRARY selects another build of the same
+# sources (e.g. one compiled with different tuning macros)
+LIBPATH = Path(os.environ["DNS_EMBED_LIBRARY"]) if os.environ.get("DNS_EMBED_LIBRARY") else HERE / "libdnsembed.so"
 
 DNS_OK, DNS_EINVAL, DNS_ENOMEM, DNS_EIO, DNS_ENAN, DNS_ETIMEOUT, DNS_ECUDA = 0, -1, -2, -3, -4, -5, -6
 PATTERN_NONE, PATTERN_RSLIP, PATTERN_PSLIP, PATTERN_SSLIP = 0, 1, 2, 3

@@ -82,8 +82,16 @@ struct dns_handle {
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
   long sample_every = 0;
-  std::vector<double> wall_lo, wall_hi;  // wall-plane populations kept for file round trips
-  long wall_gen = 0;                     // bumped whenever wall_lo / wall_hi change
+  // Wall-plane populations (the step never reads or writes them; files carry
+  // them): wall_dev [2 walls][GR xdv][GR ydv][19] on the device is the primary
+  // copy, which the AoS transfers fill and read without a host pass;
+  // wall_lo / wall_hi mirror it on the host for the field files, refreshed
+  // when stale
+  double *wall_dev = nullptr;
+  std::vector<double> wall_lo, wall_hi;
+  bool wall_host_stale = false;
+  long wall_gen = 0;                     // bumped whenever the wall planes change
+  double *stage = nullptr;               // FP32 form: one level in reference AoS doubles (allocated on first use)
   Profiler prof;
 };
 
@@ -259,7 +267,7 @@ extern "C" int dns_geometry_of(const dns_params *p, dns_geometry *g) {
   const long long esz = p->precision == DNS_FP32 ? 4 : 8;  // bytes per stored population
   const long long mac = esz == 4 ? 2LL * 23 * g->ny * g->nx * 4 : 8LL * g->nyf * g->nxf;  // elements of esz
   g->device_bytes = esz * (2 * nc + 2 * nf + 3LL * 2 * 23 * g->ny * g->nx + mac) +
-                    8 * (pl.total + (long long)kStatRow * g->nz_profile) +
+                    8 * (pl.total + (long long)kStatRow * g->nz_profile + 2LL * 19 * g->nyf * g->nxf) +
                     (long long)g->nyf * g->nxf + (long long)kLogCap * sizeof(DevLog) + sizeof(DevState);
   return DNS_OK;
 }
@@ -305,6 +313,8 @@ extern "C" void dns_destroy(dns_handle *h) {
   cudaFree(h->iface_mac);
   cudaFree(h->tke_ws);
   cudaFree(h->tke_wall);
+  cudaFree(h->wall_dev);
+  cudaFree(h->stage);
   cudaFree(h->fin_counter);
   if (h->hlog) cudaFreeHost(h->hlog);
   for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
@@ -366,6 +376,8 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   if ((rc = alloc((void **)&h->iface_mac, mac_bytes))) return rc;
   if ((rc = alloc((void **)&h->fin_counter, 256))) return rc;
   cudaMemset(h->fin_counter, 0, 256);
+  if ((rc = alloc((void **)&h->wall_dev, 2ull * g.nxf * g.nyf * 19 * 8))) return rc;
+  cudaMemset(h->wall_dev, 0, 2ull * g.nxf * g.nyf * 19 * 8);
   if (cudaMallocHost((void **)&h->hlog, kLogCap * sizeof(DevLog)) != cudaSuccess) {
     dns_destroy(h);
     return fail(DNS_ENOMEM, "cudaMallocHost failed");
@@ -428,114 +440,88 @@ extern "C" int dns_get_geometry(const dns_handle *h, dns_geometry *g) {
 static bool is_f32(const dns_handle *h) { return h->p.precision == DNS_FP32; }
 static float *F(double *p) { return reinterpret_cast<float *>(p); }
 
-// FP32 form: float deviations on the device <-> reference AoS doubles, through
-// a temporary device staging buffer (an I/O path, not the step)
-static int export_level_f32(dns_handle *h, int level, double *out) {
-  const dns_geometry &g = h->g;
-  const int zds = h->p.zds;
-  const size_t n = level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
-  double *stage = nullptr;
-  if (cudaMalloc(&stage, n * 8) != cudaSuccess) return fail(DNS_ENOMEM, "staging buffer for export");
-  if (level == 0)
-    launch_dev_to_aos_f32(F(h->fc[h->cur_c]), stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-  else if (level == 1)
-    launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
-  else
-    launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
-  cudaError_t e = cudaMemcpyAsync(out, stage, n * 8, cudaMemcpyDeviceToHost, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(stage);
-  if (e != cudaSuccess) return fail(DNS_ECUDA, cudaGetErrorString(e));
-  if (level > 0) {
-    const std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
-    const int kw = level == 1 ? 0 : g.zdf - 1;
-    for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
-      std::memcpy(out + (c * g.zdf + kw) * 19, wall.data() + c * 19, 19 * 8);
-  }
+// the host mirror of the wall planes, brought up to date from the device
+static int sync_wall_host(dns_handle *h) {
+  if (!h->wall_host_stale) return DNS_OK;
+  const size_t n = h->wall_lo.size();
+  CUDA_TRY(cudaMemcpyAsync(h->wall_lo.data(), h->wall_dev, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(h->wall_hi.data(), h->wall_dev + n, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(h->stream));
+  h->wall_host_stale = false;
   return DNS_OK;
 }
 
-static int import_level_f32(dns_handle *h, int level, const double *in) {
-  const dns_geometry &g = h->g;
-  const int zds = h->p.zds;
-  const size_t n = level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
-  double *stage = nullptr;
-  if (cudaMalloc(&stage, n * 8) != cudaSuccess) return fail(DNS_ENOMEM, "staging buffer for import");
-  cudaError_t e = cudaMemcpyAsync(stage, in, n * 8, cudaMemcpyHostToDevice, h->stream);
-  if (level == 0)
-    launch_aos_to_dev_f32(stage, F(h->fc[h->cur_c]), g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-  else if (level == 1)
-    launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
-  else
-    launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
-  cudaFree(stage);
-  if (e != cudaSuccess) return fail(DNS_ECUDA, cudaGetErrorString(e));
-  if (level > 0) {
-    std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
-    h->wall_gen++;
-    const int kw = level == 1 ? 0 : g.zdf - 1;
-    for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
-      std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
-  }
-  return DNS_OK;
+static size_t level_doubles(const dns_geometry &g, int level) {
+  return level == 0 ? 19ull * g.nzc * g.ny * g.nx : 19ull * g.zdf * g.nyf * g.nxf;
 }
 
-static int export_level(dns_handle *h, int level, double *out) {
-  if (is_f32(h)) return export_level_f32(h, level, out);
-  const dns_geometry &g = h->g;
-  const int zds = h->p.zds;
-  if (level == 0) {
-    double *stage = h->fc[1 - h->cur_c];
-    launch_soa_to_aos(h->fc[h->cur_c], stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(out, stage, 19ull * g.nzc * g.ny * g.nx * 8, cudaMemcpyDeviceToHost, h->stream));
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
+// Device staging for one level in reference AoS doubles: the idle ping-pong
+// buffer of the FP64 form (it holds as many doubles as a level with its wall
+// plane: zds planes stored per block, zdf = zds + 1 in a level, and two blocks);
+// for the FP32 form a buffer kept by the handle after its first use.
+static int staging(dns_handle *h, int level, double **out) {
+  if (!is_f32(h)) {
+    *out = level == 0 ? h->fc[1 - h->cur_c] : h->ff[1 - h->cur_f];
     return DNS_OK;
   }
-  double *stage = h->ff[1 - h->cur_f];
-  const size_t n = 19ull * g.zdf * g.nyf * g.nxf;
-  // lower block: device planes 0..zds-1 are k = 1..zdf-1; upper: zds.. are k = 0..zdf-2
-  if (level == 1)
-    launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
-  else
-    launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
+  if (!h->stage) {
+    const size_t n = std::max(level_doubles(h->g, 0), level_doubles(h->g, 1));
+    if (cudaMalloc(&h->stage, n * 8) != cudaSuccess) return fail(DNS_ENOMEM, "AoS staging buffer");
+  }
+  *out = h->stage;
+  return DNS_OK;
+}
+
+// One level of the post-stream state: device SoA (FP64, or FP32 deviations)
+// <-> reference AoS doubles on the host, through the device staging buffer:
+// the transpose and the wall plane (from / into wall_dev) are device kernels,
+// the host sees one copy of the whole level and one synchronisation.
+static int export_level(dns_handle *h, int level, double *out) {
+  const dns_geometry &g = h->g;
+  const int zds = h->p.zds;
+  double *stage = nullptr;
+  int rc = staging(h, level, &stage);
+  if (rc) return rc;
+  const bool f32 = is_f32(h);
+  if (level == 0) {
+    if (f32) launch_dev_to_aos_f32(F(h->fc[h->cur_c]), stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+    else launch_soa_to_aos(h->fc[h->cur_c], stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+  } else {
+    // lower block: device planes 0..zds-1 are k = 1..zdf-1; upper: zds.. are k = 0..zdf-2
+    const int p0 = level == 1 ? 0 : zds, k0 = level == 1 ? 1 : 0, kw = level == 1 ? 0 : g.zdf - 1;
+    if (f32) launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+    else launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+    launch_wall_plane(stage, h->wall_dev + (size_t)(level - 1) * g.nxf * g.nyf * 19, (long long)g.nxf * g.nyf,
+                      g.zdf, kw, true, h->stream);
+  }
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(out, stage, n * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaMemcpyAsync(out, stage, level_doubles(g, level) * 8, cudaMemcpyDeviceToHost, h->stream));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
-  const std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
-  const int kw = level == 1 ? 0 : g.zdf - 1;
-  for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
-    std::memcpy(out + (c * g.zdf + kw) * 19, wall.data() + c * 19, 19 * 8);
   return DNS_OK;
 }
 
 static int import_level(dns_handle *h, int level, const double *in) {
-  if (is_f32(h)) return import_level_f32(h, level, in);
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
+  double *stage = nullptr;
+  int rc = staging(h, level, &stage);
+  if (rc) return rc;
+  const bool f32 = is_f32(h);
+  CUDA_TRY(cudaMemcpyAsync(stage, in, level_doubles(g, level) * 8, cudaMemcpyHostToDevice, h->stream));
   if (level == 0) {
-    double *stage = h->fc[1 - h->cur_c];
-    CUDA_TRY(cudaMemcpyAsync(stage, in, 19ull * g.nzc * g.ny * g.nx * 8, cudaMemcpyHostToDevice, h->stream));
-    launch_aos_to_soa(stage, h->fc[h->cur_c], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-    CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaStreamSynchronize(h->stream));
-    return DNS_OK;
+    if (f32) launch_aos_to_dev_f32(stage, F(h->fc[h->cur_c]), g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+    else launch_aos_to_soa(stage, h->fc[h->cur_c], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
+  } else {
+    const int p0 = level == 1 ? 0 : zds, k0 = level == 1 ? 1 : 0, kw = level == 1 ? 0 : g.zdf - 1;
+    if (f32) launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+    else launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+    launch_wall_plane(stage, h->wall_dev + (size_t)(level - 1) * g.nxf * g.nyf * 19, (long long)g.nxf * g.nyf,
+                      g.zdf, kw, false, h->stream);
+    h->wall_host_stale = true;
+    h->wall_gen++;
   }
-  double *stage = h->ff[1 - h->cur_f];
-  const size_t n = 19ull * g.zdf * g.nyf * g.nxf;
-  CUDA_TRY(cudaMemcpyAsync(stage, in, n * 8, cudaMemcpyHostToDevice, h->stream));
-  if (level == 1)
-    launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, 0, zds, g.zdf, 1, h->stream);
-  else
-    launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, zds, zds, g.zdf, 0, h->stream);
   CUDA_TRY(cudaGetLastError());
   CUDA_TRY(cudaStreamSynchronize(h->stream));
-  std::vector<double> &wall = level == 1 ? h->wall_lo : h->wall_hi;
-  h->wall_gen++;
-  const int kw = level == 1 ? 0 : g.zdf - 1;
-  for (size_t c = 0; c < (size_t)g.nxf * g.nyf; c++)
-    std::memcpy(wall.data() + c * 19, in + (c * g.zdf + kw) * 19, 19 * 8);
   return DNS_OK;
 }
 
@@ -661,6 +647,8 @@ extern "C" int dns_init_seeded(dns_handle *h, uint64_t seed, double uc, double a
   CUDA_TRY(cudaGetLastError());
   std::fill(h->wall_lo.begin(), h->wall_lo.end(), 0.0);
   std::fill(h->wall_hi.begin(), h->wall_hi.end(), 0.0);
+  CUDA_TRY(cudaMemsetAsync(h->wall_dev, 0, 2 * h->wall_lo.size() * 8, h->stream));
+  h->wall_host_stale = false;
   h->wall_gen++;
   h->ss = 0;
   h->tm = h->p.TSTR;
@@ -836,6 +824,7 @@ extern "C" int dns_write_fields(dns_handle *h, const char *dir, int cntr) {
   Range range("dns_write_fields");
   if (!h || !dir) return fail(DNS_EINVAL, "bad argument");
   CUDA_TRY(cudaSetDevice(h->p.device));
+  if (const int r = sync_wall_host(h)) return r;
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
   const size_t nmax = std::max((size_t)g.nx * g.ny * g.nzc, (size_t)g.nxf * g.nyf * g.zdf);
@@ -901,6 +890,7 @@ static size_t level_nodes(const dns_geometry &g, int lv) {
 static int fields_planar(dns_handle *h, double *const q[3]) {
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
+  if (const int r = sync_wall_host(h)) return r;
   for (int lv = 0; lv < 3; lv++) {
     const int nx = lv == 0 ? g.nx : g.nxf, ny = lv == 0 ? g.ny : g.nyf, nz = lv == 0 ? g.nzc : g.zdf;
     const int P = lv == 0 ? g.nzc : 2 * zds, p0 = lv == 2 ? zds : 0, np = lv == 0 ? g.nzc : zds;

@@ -160,6 +160,9 @@ int tke_budget_device(const dns_params &p, const dns_geometry &g, const double *
 size_t tke_workspace_bytes(const dns_geometry &g);
 int tke_budget_planar(const dns_params &p, const dns_geometry &g, const double *const q[3], double *prof,
                       double *ufl, double *vfl, cudaStream_t st, void *work = nullptr);
+// wall plane kw of a level in reference AoS order [nodes = nx ny][nz][19] to
+// (to_aos) or from the compact wall array [nodes][19]
+void launch_wall_plane(double *aos, double *wall, long long nodes, int nz, int kw, bool to_aos, cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
                        int k0_aos, cudaStream_t stream);

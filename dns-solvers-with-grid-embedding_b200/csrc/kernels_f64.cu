@@ -892,6 +892,21 @@ __global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__rest
   for (int a = 0; a < 19; a++) soa[s + (size_t)a * stride] = o[a];
 }
 
+// Wall plane kw of an AoS level [nx][ny][nz][19] <-> the compact wall array
+// [nx][ny][19] (TO_AOS: wall -> aos).
+template <bool TO_AOS>
+__global__ void wall_plane_kernel(double *__restrict__ aos, double *__restrict__ wall, long long nodes, int nz,
+                                  int kw) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nodes * 19) return;
+  const long long c = t / 19, a = t - c * 19;
+  double *o = aos + (c * nz + kw) * 19 + a;
+  if (TO_AOS)
+    *o = wall[t];
+  else
+    wall[t] = *o;
+}
+
 // ------------------------------------------------------------------ field output
 // vel_print.c:86-125: per node u = (sum E f) / rho, rho = sum f, both summed in
 // population order (moments_f64 is that order); zero where rho <= 0
@@ -1153,6 +1168,14 @@ void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, in
                        cudaStream_t stream) {
   dim3 grid((nx + 127) / 128, ny, np), block(128);
   aos_to_soa_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos);
+}
+
+void launch_wall_plane(double *aos, double *wall, long long nodes, int nz, int kw, bool to_aos, cudaStream_t stream) {
+  const unsigned blocks = (unsigned)((nodes * 19 + 255) / 256);
+  if (to_aos)
+    wall_plane_kernel<true><<<blocks, 256, 0, stream>>>(aos, wall, nodes, nz, kw);
+  else
+    wall_plane_kernel<false><<<blocks, 256, 0, stream>>>(aos, wall, nodes, nz, kw);
 }
 
 void launch_fields_f64(const double *soa, double *vel, double *den, int nx, int ny, int P, int p0, int np, int nz_aos,

@@ -49,8 +49,11 @@ def test_batch_instance_tracks_fp64_oracle(pkg, port, ref_configs, name, mode):
 
 
 def test_batch_matches_single_fp32_channel(pkg, ref_configs):
-    """Same kernels, same tiles: the batch and the single-channel FP32 form
-    differ only in the order of the final reduction sums."""
+    """The batch and the single-channel FP32 form compute the same deviation
+    arithmetic with different kernels (the batch moves four nodes per thread
+    and sums its flow-rate partials per node group): they agree to FP32
+    rounding, states within 5e-7 and the logged quantities within 1e-5 (the
+    wall shear stresses, differences of near-wall velocities, within 1e-3)."""
     m = ref_configs["t_ridges"]
     p = params_for(pkg, m, "cfr")
     q = params_for(pkg, m, "cfr")
@@ -63,12 +66,14 @@ def test_batch_matches_single_fp32_channel(pkg, ref_configs):
         i = b.add(p, steps=20, seed=SEED, uc=UC, amp=AMP, sample_every=2, tile=(128, 2, 128, 2))
         b.run(20)
         for lvl in range(3):
-            np.testing.assert_allclose(b.export_state(i, lvl), ch.export_state(lvl), rtol=0, atol=1e-7)
-        np.testing.assert_allclose(b.log(i)[:, 1:], la[:, 1:], rtol=1e-6, atol=1e-10)
+            np.testing.assert_allclose(b.export_state(i, lvl), ch.export_state(lvl), rtol=0, atol=5e-7)
+        lb = b.log(i)
+        np.testing.assert_allclose(lb[:, 1:5], la[:, 1:5], rtol=1e-5, atol=1e-9)
+        np.testing.assert_allclose(lb[:, 5:], la[:, 5:], rtol=1e-3, atol=1e-8)
         sa, na = b.stats(i)
         sb, nb = ch.stats()
         assert na == nb == 10
-        np.testing.assert_allclose(sa, sb, rtol=1e-6, atol=1e-9)
+        np.testing.assert_allclose(sa, sb, rtol=1e-5, atol=1e-9)
     ch.close()
 
 
