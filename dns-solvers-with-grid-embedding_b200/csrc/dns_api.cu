@@ -1200,28 +1200,33 @@ extern "C" int dns_load_uniform(dns_handle *h, const char *dir, int cntr) {
   return refresh_flow(h, p.forcing == DNS_FORCING_CFR ? 0.0 : p.force_const);
 }
 
-// One coarse step on two (or three) streams.  The interface transfer of
-// substep s writes only the interface planes of the buffer whose other planes
-// the fine kernel of substep s writes, so the two run concurrently; the coarse
-// kernel and the extraction run beside the first fine substep.
-//   main:  coarse, extract, iface(1), [wait fine(s-1)] iface(s) ..., [wait inject] finalize
-//   aux:   [wait start] fine(1), [wait iface(s-1)] fine(s) ..., inject
-// Schedule (compile-time): 0 one stream in order, 1 interface transfers on the
-// main stream, 2 interface transfers on their own high-priority stream.
+// One coarse step on three streams.  The interface transfer of substep s
+// writes only the interface planes of the buffer whose other planes the fine
+// kernel of substep s writes, so the two run concurrently.  The extraction
+// and the interface transfers are short, latency-bound kernels on the path
+// from the coarse kernel to the next fine substep: they go on a stream of the
+// highest priority, so that their blocks are dispatched ahead of the pending
+// blocks of the bandwidth-bound fine kernel (on equal priority they waited
+// behind it, measured on B200: ~70 us of a 700 us step with the GPU's
+// bandwidth idle).
+//   main (S):  coarse, [wait inject, iface(GR)] finalize
+//   high (H):  [wait coarse] extract, iface(1), [wait fine(1)] iface(2) ...
+//   aux  (T):  [wait start] fine(1), [wait iface(1)] fine(2) ..., inject
+// Schedule (compile-time): 0 one stream in order, 1 this schedule.
 #ifndef DNS_SCHED
 #define DNS_SCHED 1
 #endif
 static void issue_step_overlapped(dns_handle *h, DevLog *log_row, bool sample) {
   const Dims &d = h->d;
-  cudaStream_t S = h->stream, T = h->aux, H = DNS_SCHED == 2 ? h->hip : h->stream;
+  cudaStream_t S = h->stream, T = h->aux, H = h->hip;
   const int nc = 1 - h->cur_c;
   cudaEventRecord(h->ev_start, S);
   cudaStreamWaitEvent(T, h->ev_start, 0);
   L_coarse(h, h->cur_c, nc, sample, S);
-  rotate_history(h);
-  L_extract(h, nc, h->hn, S);
   cudaEventRecord(h->ev_ext, S);
   cudaStreamWaitEvent(H, h->ev_ext, 0);
+  rotate_history(h);
+  L_extract(h, nc, h->hn, H);
   int cur = h->cur_f;
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - cur;
