@@ -92,15 +92,12 @@ constexpr int kCornerTX = 32, kCornerTY = 8;
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
   int stats, sfinal, coarse, extract, fine, icorner, ieval, inject, final_;
-  int prio_high;  // the device's greatest stream priority (interface and extraction launches)
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)
 // stats: launch the statistics phases (some resident instance samples)
-// s: the batch's stream; aux, hi: its side streams (hi at the greatest priority);
-// ev: 11 events (fork / join of the three streams)
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
-                 cudaStream_t s, cudaStream_t aux, cudaStream_t hi, cudaEvent_t *ev, bool stats);
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats);  // ev: 10 events (fork/join of the two streams)
 void tile_counts(const Inst &I, int counts[PH_NPHASE]);
 
 }  // namespace batch

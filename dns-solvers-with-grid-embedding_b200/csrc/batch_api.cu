@@ -33,7 +33,7 @@ namespace {
   } while (0)
 
 constexpr int kGroup = kLogRows / 2;  // steps per graph replay: two groups fit the log ring
-constexpr int kNumEvents = 11;
+constexpr int kNumEvents = 10;
 
 struct Record {
   dns_params p{};
@@ -161,7 +161,7 @@ Layout layout_of(const Inst &I) {
 struct dns_batch {
   int device = 0;
   int gr = 0;
-  cudaStream_t s = nullptr, aux = nullptr, hi = nullptr;
+  cudaStream_t s = nullptr, aux = nullptr;
   cudaEvent_t ev[kNumEvents] = {};
   cudaEvent_t done[2] = {};
   Mix *dmix = nullptr;
@@ -205,7 +205,6 @@ static void release(dns_batch *b) {
   for (cudaEvent_t e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->aux) cudaStreamDestroy(b->aux);
-  if (b->hi) cudaStreamDestroy(b->hi);
   if (b->s) cudaStreamDestroy(b->s);
   delete b;
 }
@@ -223,11 +222,8 @@ extern "C" int dns_batch_create(int device, dns_batch **out) {
   b->device = device;
   b->hmix.reset(new Mix());
   std::memset(b->hmix.get(), 0, sizeof(Mix));
-  int prio_low = 0, prio_high = 0;
-  cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
   bool ok = cudaStreamCreateWithFlags(&b->s, cudaStreamNonBlocking) == cudaSuccess &&
-            cudaStreamCreateWithPriority(&b->aux, cudaStreamNonBlocking, prio_low) == cudaSuccess &&
-            cudaStreamCreateWithPriority(&b->hi, cudaStreamNonBlocking, prio_high) == cudaSuccess;
+            cudaStreamCreateWithFlags(&b->aux, cudaStreamNonBlocking) == cudaSuccess;
   for (cudaEvent_t &e : b->ev) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
   for (cudaEvent_t &e : b->done) ok = ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
   ok = ok && cudaMalloc(&b->dmix, sizeof(Mix)) == cudaSuccess &&
@@ -461,11 +457,10 @@ static int capture(dns_batch *b, int steps, bool stats, cudaGraphExec_t *out) {
   cudaGraph_t graph = nullptr;
   BTRY(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
   for (int q = 0; q < steps; q++)
-    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->dcount, b->gr, b->grids, b->s, b->aux, b->hi, b->ev, stats);
+    launch_step(b->dmix, b->ddyn, b->dstate, b->dlog, b->dcount, b->gr, b->grids, b->s, b->aux, b->ev, stats);
   cudaError_t e = cudaStreamEndCapture(b->s, &graph);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-  // per-node priorities: the interface kernels' launches carry the greatest
-  e = cudaGraphInstantiateWithFlags(out, graph, cudaGraphInstantiateFlagUseNodePriority);
+  e = cudaGraphInstantiate(out, graph, 0);
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return fail_with(DNS_ECUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
   return DNS_OK;

@@ -136,10 +136,6 @@ __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, 
 #ifndef DNS_F32_QUAD_MINB
 #define DNS_F32_QUAD_MINB 4
 #endif
-// block slots per SM the stream-collide grids leave to the interface kernels
-#ifndef DNS_STREAM_SPARE
-#define DNS_STREAM_SPARE 1
-#endif
 __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     b_coarse(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state) {
   const int n = M->n;
@@ -625,37 +621,14 @@ __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, D
   }
 }
 
-// Persistent grid: resident blocks per SM x SMs, less `spare` blocks per SM
-// (kept at least one): the bandwidth-bound stream-collide kernels leave one
-// block slot of every SM to the latency-bound interface kernels that run beside
-// them on the high-priority stream.
 template <class K>
-int occupancy_grid(K kernel, int *grid, int spare = 0) {
+int occupancy_grid(K kernel, int *grid) {
   int dev = 0, sms = 0, per = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0) != cudaSuccess) return -1;
-  per = per > spare ? per - spare : 1;
-  *grid = sms * per;
+  *grid = sms * (per > 0 ? per : 1);
   return 0;
-}
-
-// Launch on stream st with an explicit scheduling priority (kept by a captured
-// graph instantiated with per-node priorities): the interface and extraction
-// kernels run at the device's greatest priority, so their blocks are
-// dispatched ahead of the pending blocks of the stream-collide kernels.
-template <class... P, class... A>
-void launch_prio(void (*kernel)(P...), int grid, int prio, cudaStream_t st, A... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(grid);
-  cfg.blockDim = dim3(kThreads);
-  cfg.stream = st;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributePriority;
-  at[0].val.priority = prio;
-  cfg.attrs = at;
-  cfg.numAttrs = 1;
-  cudaLaunchKernelEx(&cfg, kernel, args...);
 }
 
 }  // namespace
@@ -679,16 +652,14 @@ int query_grids(int gr, Grids *g) {
   int rc = 0;
   rc |= occupancy_grid(b_stats, &g->stats);
   rc |= occupancy_grid(b_sfinal, &g->sfinal);
-  rc |= occupancy_grid(b_coarse, &g->coarse, DNS_STREAM_SPARE);
+  rc |= occupancy_grid(b_coarse, &g->coarse);
   rc |= occupancy_grid(b_extract, &g->extract);
-  rc |= occupancy_grid(b_fine<3>, &g->fine, DNS_STREAM_SPARE);
+  rc |= occupancy_grid(b_fine<3>, &g->fine);
   rc |= occupancy_grid(b_icorner, &g->icorner);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
   else rc |= occupancy_grid(b_ieval<4>, &g->ieval);
   rc |= occupancy_grid(b_inject, &g->inject);
-  int prio_low = 0;
-  if (cudaDeviceGetStreamPriorityRange(&prio_low, &g->prio_high) != cudaSuccess) rc |= 1;
   rc |= occupancy_grid(b_final, &g->final_);
   return rc;
 }
@@ -714,53 +685,42 @@ static TimeW time_weights(int sub, int gr) {
   return TimeW{(float)(0.5 * h2 + h3 + 1.5 * h4), (float)(h1 - 2. * h4), (float)(-0.5 * h2 + 0.5 * h4)};
 }
 
-static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, int prio, cudaStream_t s) {
+static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, cudaStream_t s) {
   const TimeW tw = time_weights(sub, gr);
-  launch_prio(b_icorner, g.icorner, prio, s, m, dyn, sub, tw);
-  if (gr == 2) launch_prio(b_ieval<2>, g.ieval, prio, s, m, dyn, sub, tw);
-  else if (gr == 3) launch_prio(b_ieval<3>, g.ieval, prio, s, m, dyn, sub, tw);
-  else launch_prio(b_ieval<4>, g.ieval, prio, s, m, dyn, sub, tw);
+  b_icorner<<<g.icorner, kThreads, 0, s>>>(m, dyn, sub, tw);
+  if (gr == 2) b_ieval<2><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else if (gr == 3) b_ieval<3><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
+  else b_ieval<4><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
 }
 
-// One coarse step of every resident instance on three streams.  The
-// stream-collide kernels are persistent grids that fill the machine less one
-// block slot per SM, and run one after another; the extraction and the
-// interface transfers, short and latency-bound, run beside them at the
-// greatest priority in the spare slots:
-//   aux: [start] stats, sfinal, coarse, fine(1), [iface(1)] fine(2) ..., inject
-//   hi:  [coarse] extract, iface(1), [fine(1)] iface(2) ...
-//   s:   [inject, iface(GR)] final
-// The interface transfer of substep s writes only the interface planes of the
-// buffer fine(s) writes (and fine(s) drops its pushes into them); it must wait
-// for fine(s-1), which reads that buffer.  The statistics read the step's
-// starting state, which fine(2) overwrites: both are on aux.
-// ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject, [10] coarse.
+// One coarse step of every resident instance on two streams, with the
+// dependency structure of the single-channel schedule:
+//   s:   stats, sfinal, coarse, extract, iface(1), [fine(1)] iface(2) ..., [inject] final
+//   aux: [start] fine(1), [iface(1)] fine(2) ..., inject
+// The statistics read the state fine(2) and iface(2) overwrite; both follow
+// iface(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject.
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
-                 cudaStream_t s, cudaStream_t aux, cudaStream_t hi, cudaEvent_t *ev, bool stats) {
-  const int prio_high = g.prio_high;
+                 cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats) {
   cudaEventRecord(ev[0], s);
   cudaStreamWaitEvent(aux, ev[0], 0);
   if (stats) {
-    b_stats<<<g.stats, kThreads, 0, aux>>>(m, dyn);
-    b_sfinal<<<g.sfinal, kThreads, 0, aux>>>(m, dyn);
+    b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
+    b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
   }
-  b_coarse<<<g.coarse, kThreads, 0, aux>>>(m, dyn, state);
-  cudaEventRecord(ev[10], aux);
-  cudaStreamWaitEvent(hi, ev[10], 0);
-  launch_prio(b_extract, g.extract, prio_high, hi, m, (const Dyn *)dyn);
+  b_coarse<<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
+  b_extract<<<g.extract, kThreads, 0, s>>>(m, dyn);
   for (int sub = 1; sub <= gr; sub++) {
     const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);
     if (sub > 1) cudaStreamWaitEvent(aux, ev[5 + sub - 2], 0);
     launch_fine(m, dyn, state, mode, sub, g, aux);
     cudaEventRecord(ev[1 + sub - 1], aux);
-    if (sub > 1) cudaStreamWaitEvent(hi, ev[1 + sub - 2], 0);
-    launch_iface(m, dyn, gr, sub, g, prio_high, hi);
-    cudaEventRecord(ev[5 + sub - 1], hi);
+    if (sub > 1) cudaStreamWaitEvent(s, ev[1 + sub - 2], 0);
+    launch_iface(m, dyn, gr, sub, g, s);
+    cudaEventRecord(ev[5 + sub - 1], s);
   }
   b_inject<<<g.inject, kThreads, 0, aux>>>(m, dyn);
   cudaEventRecord(ev[9], aux);
   cudaStreamWaitEvent(s, ev[9], 0);
-  cudaStreamWaitEvent(s, ev[5 + gr - 1], 0);
   b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log, count);
 }
 

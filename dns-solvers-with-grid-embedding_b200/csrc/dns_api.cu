@@ -76,8 +76,7 @@ struct dns_handle {
   long tke_wall_gen = -1;              // wall_gen they were made from
   unsigned int *fin_counter = nullptr; // finalize's block counter
   cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
-  cudaStream_t hip = nullptr;          // interface transfers (highest priority)
-  cudaEvent_t ev_start = nullptr, ev_inj = nullptr, ev_ext = nullptr, ev_fine[4] = {}, ev_if[4] = {};
+  cudaEvent_t ev_start = nullptr, ev_inj = nullptr, ev_fine[4] = {}, ev_if[4] = {};
   int cur_c = 0, cur_f = 0;
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
@@ -320,8 +319,7 @@ extern "C" void dns_destroy(dns_handle *h) {
   for (cudaEvent_t e : h->prof.ev) cudaEventDestroy(e);
   if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
   if (h->aux) cudaStreamDestroy(h->aux);
-  if (h->hip) cudaStreamDestroy(h->hip);
-  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_ext, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
+  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
                         &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
   for (cudaEvent_t *e : evs)
     if (*e) cudaEventDestroy(*e);
@@ -389,9 +387,8 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   h->own_stream = true;
   int prio_low = 0, prio_high = 0;
   cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high);
-  bool ev_ok = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_low) == cudaSuccess &&
-               cudaStreamCreateWithPriority(&h->hip, cudaStreamNonBlocking, prio_high) == cudaSuccess;
-  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_ext, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
+  bool ev_ok = cudaStreamCreateWithPriority(&h->aux, cudaStreamNonBlocking, prio_low) == cudaSuccess;
+  cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
                         &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
   for (cudaEvent_t *e : evs) ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
   if (!ev_ok) {
@@ -1200,48 +1197,43 @@ extern "C" int dns_load_uniform(dns_handle *h, const char *dir, int cntr) {
   return refresh_flow(h, p.forcing == DNS_FORCING_CFR ? 0.0 : p.force_const);
 }
 
-// One coarse step on three streams.  The interface transfer of substep s
+// One coarse step on two streams.  The interface transfer of substep s
 // writes only the interface planes of the buffer whose other planes the fine
-// kernel of substep s writes, so the two run concurrently.  The extraction
-// and the interface transfers are short, latency-bound kernels on the path
-// from the coarse kernel to the next fine substep: they go on a stream of the
-// highest priority, so that their blocks are dispatched ahead of the pending
-// blocks of the bandwidth-bound fine kernel (on equal priority they waited
-// behind it, measured on B200: ~70 us of a 700 us step with the GPU's
-// bandwidth idle).
-//   main (S):  coarse, [wait inject, iface(GR)] finalize
-//   high (H):  [wait coarse] extract, iface(1), [wait fine(1)] iface(2) ...
-//   aux  (T):  [wait start] fine(1), [wait iface(1)] fine(2) ..., inject
+// kernel of substep s writes, so the two run concurrently; the coarse kernel
+// and the extraction run beside the first fine substep.
+//   main:  coarse, extract, iface(1), [wait fine(s-1)] iface(s) ..., [wait inject] finalize
+//   aux:   [wait start] fine(1), [wait iface(s-1)] fine(s) ..., inject
+// (Measured on B200 with per-kernel device timestamps: the FP64 interface
+// transfer is bound by FP64 issue; moved with the extraction to a stream of
+// the greatest priority it ran beside the fine kernels but slowed them by as
+// much as it hid, 711 against 705 us per step, so it stays in order here.)
 // Schedule (compile-time): 0 one stream in order, 1 this schedule.
 #ifndef DNS_SCHED
 #define DNS_SCHED 1
 #endif
 static void issue_step_overlapped(dns_handle *h, DevLog *log_row, bool sample) {
   const Dims &d = h->d;
-  cudaStream_t S = h->stream, T = h->aux, H = h->hip;
+  cudaStream_t S = h->stream, T = h->aux;
   const int nc = 1 - h->cur_c;
   cudaEventRecord(h->ev_start, S);
   cudaStreamWaitEvent(T, h->ev_start, 0);
   L_coarse(h, h->cur_c, nc, sample, S);
-  cudaEventRecord(h->ev_ext, S);
-  cudaStreamWaitEvent(H, h->ev_ext, 0);
   rotate_history(h);
-  L_extract(h, nc, h->hn, H);
+  L_extract(h, nc, h->hn, S);
   int cur = h->cur_f;
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - cur;
     if (it > 1) cudaStreamWaitEvent(T, h->ev_if[it - 2], 0);
     L_fine(h, cur, nf, it == 1, it == d.gr, sample && it == 1, T);
     cudaEventRecord(h->ev_fine[it - 1], T);
-    if (it > 1) cudaStreamWaitEvent(H, h->ev_fine[it - 2], 0);
-    L_iface(h, nf, it, H);
-    cudaEventRecord(h->ev_if[it - 1], H);
+    if (it > 1) cudaStreamWaitEvent(S, h->ev_fine[it - 2], 0);
+    L_iface(h, nf, it, S);
+    cudaEventRecord(h->ev_if[it - 1], S);
     cur = nf;
   }
   L_inject(h, cur, nc, T);
   cudaEventRecord(h->ev_inj, T);
   cudaStreamWaitEvent(S, h->ev_inj, 0);
-  cudaStreamWaitEvent(S, h->ev_if[d.gr - 1], 0);
   launch_finalize(h->state, log_row, h->partials, h->fin_counter, h->pl, d, h->shape, h->sp, S);
   if (sample) launch_stats_finalize(h->stats_acc, h->partials, h->pl, d, h->shape, S);
   h->cur_f = cur;
