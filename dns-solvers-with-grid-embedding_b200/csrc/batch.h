@@ -2,8 +2,9 @@
 // persistent kernels over a per-instance block table (internal to
 // libdnsembed; the C ABI is dns_batch_* in include/dns_embed.h).
 //
-// Every phase of the coarse step (statistics, coarse collide-stream, plane
-// extraction, fine substeps, interface transfer, injection, finalize) is one
+// Every phase of the coarse step (statistics, coarse collide-stream, interface
+// history and corner data, fine substeps, interface evaluation, injection,
+// finalize) is one
 // persistent kernel: a grid sized to the machine walks the phase's work items
 // of all resident instances.  Instance s owns items [start[ph][s],
 // start[ph][s+1]); an item is one tile of one instance, decoded against that
@@ -31,9 +32,8 @@ enum Phase {
   PH_STATS = 0,  // plane statistics of the sampled state (coarse 2..zdc-3, every fine plane)
   PH_SFINAL,     // per-plane accumulation of those sums
   PH_COARSE,     // every coarse plane
-  PH_EXTRACT,    // interface history planes k = 1 and zdc-2
   PH_FINE,       // every fine plane of both blocks (wall-adjacent, interface-adjacent, then bulk)
-  PH_ICORNER,    // interface corner data: tiles x walls x fields
+  PH_ICORNER,    // interface history level n and every substep's corner data: tiles x walls x field groups
   PH_IEVAL,      // interface evaluation: fine rows x walls
   PH_INJECT,     // fine-to-coarse injection rows
   PH_FINAL,      // reduction chunks of the finalize
@@ -48,7 +48,7 @@ struct Inst {
   int cw, cjb, cgx, cgy;  // coarse
   int fw, fjb, fgx, fgy;  // fine
   int igx, igy;           // interface corner tiles
-  int egx;                // extraction / injection blocks per row
+  int egx;                // injection blocks per row
   int nzp;                // composite profile planes
   int slot;               // row of the batch-level dyn / state / log arrays
   long long sample_every; // statistics every n steps of the instance (0: none)
@@ -58,7 +58,7 @@ struct Inst {
   int cfr, fltr;          // constant flow rate; filtered fine-to-coarse transfer (FLTR)
   float *fc[2], *ff[2];   // coarse / fine SoA deviations, ping-pong
   float *hist;            // 3 ring slots x [2 walls][23][ny][nx]
-  float4 *corner;         // interface corner data [2 walls][23][ny][nx]
+  float4 *corner;         // interface corner data of each substep [GR][2 walls][23][ny][nx]
   int8_t *wflag;          // [nyf][nxf]
   double *part;           // block partials
   long long pc, pf, pi, pw, psc, psf, pl2;  // region offsets (doubles) in part; pl2: finalize level 2
@@ -91,7 +91,7 @@ constexpr int kCornerTX = 32, kCornerTY = 8;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
-  int stats, sfinal, coarse, extract, fine, icorner, ieval, inject, final_;
+  int stats, sfinal, coarse, fine, icorner, ieval, inject, final_;
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)

@@ -137,7 +137,7 @@ Layout layout_of(const Inst &I) {
   L.ff[0] = take(off, nf);
   L.ff[1] = take(off, nf);
   L.hist = take(off, 3ull * 2 * 23 * I.ny * I.nx * 4);
-  L.corner = take(off, 2ull * 23 * I.ny * I.nx * 16);
+  L.corner = take(off, (size_t)I.gr * 2 * 23 * I.ny * I.nx * 16);
   L.wflag = take(off, (size_t)I.nyf * I.nxf);
   const long long cb = (long long)I.nzc * I.cgy * I.cgx, fb = 2LL * I.zds * I.fgy * I.fgx,
                   ib = 2LL * I.ny * I.egx;

@@ -196,41 +196,6 @@ __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
   }
 }
 
-// ------------------------------------------------------------------ extraction
-// new history level n (ring slot of the old pp) from the coarse state just streamed
-__global__ void __launch_bounds__(kThreads) b_extract(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
-  const int n = M->n;
-  const int *st = M->start[PH_EXTRACT];
-  const int total = st[n];
-  int s = 0;
-  for (int w = blockIdx.x; w < total; w += gridDim.x) {
-    s = owner(st, n, w, s);
-    const Inst &I = M->inst[s];
-    const Dyn D = dyn[I.slot];
-    if (D.remaining <= 0) {
-      w = past(w, st[s + 1], gridDim.x);
-      continue;
-    }
-    const int local = w - st[s];
-    const int row = local / I.egx, bx = local - row * I.egx;
-    const int wall = row / I.ny, j = row - wall * I.ny;
-    const int i = bx * kThreads + threadIdx.x;
-    if (i >= I.nx) continue;
-    const int k = wall == 0 ? 1 : I.nzc - 2;
-    const size_t pstride = (size_t)I.nzc * I.ny * I.nx, plane = (size_t)I.ny * I.nx;
-    float f[19];
-    load19f(I.fc[D.cc ^ 1], ((size_t)k * I.ny + j) * I.nx + i, pstride, f);
-    const Mac32 m = macro_f32(f);
-    float *o = I.hist + (size_t)D.hpp * 2 * 23 * plane + (size_t)wall * 23 * plane + (size_t)j * I.nx + i;
-    o[0] = m.drho;
-    o[plane] = m.u0;
-    o[2 * plane] = m.u1;
-    o[3 * plane] = m.u2;
-#pragma unroll
-    for (int a = 0; a < 19; a++) o[(size_t)(4 + a) * plane] = f[a] - deq_f32(a, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
-  }
-}
-
 // ------------------------------------------------------------------ fine
 // Both fine blocks' planes in one launch per substep (xfcomputations.c:43-214,
 // 599-712 collision with force G/GR; :215-442, 724-897 streaming), four nodes
@@ -370,7 +335,7 @@ __device__ __forceinline__ void iface_params_of(IfParams32 &P, const Inst &I, co
   P.hn = I.hist + (size_t)D.hpp * hs;
   P.hp = I.hist + (size_t)D.hn * hs;
   P.hpp = I.hist + (size_t)D.hp * hs;
-  P.corner = I.corner;
+  P.corner = I.corner + (size_t)(sub - 1) * 2 * 23 * I.ny * I.nx;  // substep sub's corner data
   P.fdst = I.ff[D.cf ^ (sub & 1)];
   P.nx = I.nx;
   P.ny = I.ny;
@@ -383,10 +348,113 @@ __device__ __forceinline__ void iface_params_of(IfParams32 &P, const Inst &I, co
   P.fac = I.fac_if;
 }
 
-__global__ void __launch_bounds__(kThreads) b_icorner(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
-                                                      TimeW tw) {
-  __shared__ IfCornerSmem S;
-  __shared__ IfParams32 P;
+// Interface corner data of every substep of the step, with the extraction of
+// the new interface history level folded in.  One item: tile (tx, ty) of
+// CTX x CTY coarse interface nodes, wall w, field group G.  The level-n values
+// of the tile and its two-node halo are formed from the coarse state just
+// streamed (xcomputations.c:558-625: [drho, u, f - feq] at k = 1 / zdc - 2) and
+// the tile's own nodes are written to the history (the slot that becomes
+// level n); levels p and pp come from the history.  Then, for every substep
+// t = 1..GR, the Hermite-in-time value (tinterpolate_hrmt.c), the fourth-order
+// derivatives (derivative.c) and the corner float4s of substep t's array.
+// Every substep's interface depends only on the three history levels, so the
+// whole step's corner data is made right after the coarse kernel.
+struct CornerTimes {
+  int gr;
+  TimeW w[4];  // substeps 1..gr
+};
+constexpr int kCQX = CTX + 4, kCQY = CTY + 4, kCNV = (kCQX * kCQY + kThreads - 1) / kThreads;
+static_assert(kCornerFieldGroups == 3, "field groups of b_icorner_all");
+constexpr int kCornerFieldsMax = 8;  // fields per group: 7, 8, 8
+struct CornerAllSmem {
+  IfCornerSmem S;
+  float N[kCornerFieldsMax][kCQX * kCQY];  // level n of the group's fields, tile and halo
+};
+
+template <int G>
+__device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &I, const Dyn &D, int tx, int ty,
+                                                  int w, const CornerTimes &ct) {
+  constexpr int F0 = corner_field(G), F1 = corner_field(G + 1);
+  const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
+  const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
+  const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
+  const int k = w == 0 ? 1 : I.nzc - 2;
+  const size_t pstride = (size_t)I.nzc * plane;
+  const float *fc = I.fc[D.cc ^ 1] + (size_t)k * plane;  // the coarse state just streamed
+  // ring after this step's rotation: level n in the old pp slot, p in old n, pp in old p
+  float *hn = I.hist + (size_t)D.hpp * hs + (size_t)w * 23 * plane;
+  const float *hp = I.hist + (size_t)D.hn * hs + (size_t)w * 23 * plane;
+  const float *hpp = I.hist + (size_t)D.hp * hs + (size_t)w * 23 * plane;
+  int off[kCNV];
+#pragma unroll
+  for (int s = 0; s < kCNV; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    off[s] = -1;
+    if (q < kCQX * kCQY) off[s] = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
+    if (off[s] < 0) continue;
+    float d[19];
+    load19f(fc, (size_t)off[s], pstride, d);
+    const Mac32 m = macro_f32(d);
+    const int qi = q % kCQX - 2, qj = q / kCQX - 2;
+    const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < CTY && i0 + qi < nx && j0 + qj < ny;
+#pragma unroll
+    for (int f = F0; f < F1; f++) {
+      const float v = f == 0 ? m.drho
+                      : f == 1 ? m.u0
+                      : f == 2 ? m.u1
+                      : f == 3 ? m.u2 : d[f - 4] - deq_f32(f - 4, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+      C.N[f - F0][q] = v;
+      if (own) hn[(size_t)f * plane + off[s]] = v;
+    }
+  }
+  __syncthreads();
+  float *V = &C.S.V[0][0];
+  for (int f = F0; f < F1; f++) {
+    float vp[kCNV], vpp[kCNV];
+#pragma unroll
+    for (int s = 0; s < kCNV; s++)
+      if (off[s] >= 0) {
+        vp[s] = __ldg(hp + (size_t)f * plane + off[s]);
+        vpp[s] = __ldg(hpp + (size_t)f * plane + off[s]);
+      }
+    for (int t = 0; t < ct.gr; t++) {
+      const TimeW tw = ct.w[t];
+#pragma unroll
+      for (int s = 0; s < kCNV; s++) {
+        const int q = threadIdx.x + s * kThreads;
+        if (off[s] >= 0) V[q] = tw.an * C.N[f - F0][q] + tw.ap * vp[s] + tw.app * vpp[s];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int s = 0; s < (kCQX * CTY + kThreads - 1) / kThreads; s++) {
+        const int q = threadIdx.x + s * kThreads;
+        if (q < kCQX * CTY) {
+          const int pi = q % kCQX, r = q / kCQX;
+          C.S.DY[r][pi] = c2o3 * (C.S.V[r + 3][pi] - C.S.V[r + 1][pi]) - c1o12 * (C.S.V[r + 4][pi] - C.S.V[r][pi]);
+        }
+      }
+      __syncthreads();
+      float4 *out = I.corner + (size_t)t * 2 * 23 * plane + ((size_t)w * 23 + f) * plane;
+#pragma unroll
+      for (int s = 0; s < CTX * CTY / kThreads; s++) {
+        const int q = threadIdx.x + s * kThreads;
+        const int c = q % CTX, r = q / CTX;
+        if (i0 + c < nx && j0 + r < ny) {
+          const float dx = c2o3 * (C.S.V[r + 2][c + 3] - C.S.V[r + 2][c + 1]) -
+                           c1o12 * (C.S.V[r + 2][c + 4] - C.S.V[r + 2][c]);
+          const float dxy =
+              c2o3 * (C.S.DY[r][c + 3] - C.S.DY[r][c + 1]) - c1o12 * (C.S.DY[r][c + 4] - C.S.DY[r][c]);
+          out[(size_t)(j0 + r) * nx + i0 + c] = make_float4(C.S.V[r + 2][c + 2], dx, C.S.DY[r][c + 2], dxy);
+        }
+      }
+      __syncthreads();  // V and DY are rewritten for the next substep or field
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
+                                                          CornerTimes ct) {
+  __shared__ CornerAllSmem C;
   const int n = M->n;
   const int *st = M->start[PH_ICORNER];
   const int total = st[n];
@@ -405,9 +473,10 @@ __global__ void __launch_bounds__(kThreads) b_icorner(const Mix *__restrict__ M,
     const int ty = local % I.igy;
     local /= I.igy;
     const int wall = local / kCornerFieldGroups, g = local - wall * kCornerFieldGroups;
-    if (threadIdx.x == 0) iface_params_of(P, I, D, sub, tw);
-    __syncthreads();
-    iface_corner_tile32(S, P, tx, ty, wall, corner_field(g), corner_field(g + 1));  // ends with a barrier
+    // block-uniform; each ends with a barrier
+    if (g == 0) corner_all_tile32<0>(C, I, D, tx, ty, wall, ct);
+    else if (g == 1) corner_all_tile32<1>(C, I, D, tx, ty, wall, ct);
+    else corner_all_tile32<2>(C, I, D, tx, ty, wall, ct);
   }
 }
 
@@ -638,7 +707,6 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   c[PH_STATS] = (I.nzc - 4) * cb + 2 * I.zds * fb;
   c[PH_SFINAL] = I.nzp;
   c[PH_COARSE] = I.nzc * cb;
-  c[PH_EXTRACT] = 2 * I.ny * I.egx;
   c[PH_FINE] = 2 * I.zds * fb;
   c[PH_ICORNER] = 2 * kCornerFieldGroups * I.igx * I.igy;
   const int etx = I.gr == 2 ? IfTile<2>::TX : (I.gr == 3 ? IfTile<3>::TX : IfTile<4>::TX);
@@ -653,9 +721,8 @@ int query_grids(int gr, Grids *g) {
   rc |= occupancy_grid(b_stats, &g->stats);
   rc |= occupancy_grid(b_sfinal, &g->sfinal);
   rc |= occupancy_grid(b_coarse, &g->coarse);
-  rc |= occupancy_grid(b_extract, &g->extract);
   rc |= occupancy_grid(b_fine<3>, &g->fine);
-  rc |= occupancy_grid(b_icorner, &g->icorner);
+  rc |= occupancy_grid(b_icorner_all, &g->icorner);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
   else rc |= occupancy_grid(b_ieval<4>, &g->ieval);
@@ -685,9 +752,8 @@ static TimeW time_weights(int sub, int gr) {
   return TimeW{(float)(0.5 * h2 + h3 + 1.5 * h4), (float)(h1 - 2. * h4), (float)(-0.5 * h2 + 0.5 * h4)};
 }
 
-static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, cudaStream_t s) {
+static void launch_eval(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g, cudaStream_t s) {
   const TimeW tw = time_weights(sub, gr);
-  b_icorner<<<g.icorner, kThreads, 0, s>>>(m, dyn, sub, tw);
   if (gr == 2) b_ieval<2><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
   else if (gr == 3) b_ieval<3><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
   else b_ieval<4><<<g.ieval, kThreads, 0, s>>>(m, dyn, sub, tw);
@@ -695,10 +761,11 @@ static void launch_iface(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g
 
 // One coarse step of every resident instance on two streams, with the
 // dependency structure of the single-channel schedule:
-//   s:   stats, sfinal, coarse, extract, iface(1), [fine(1)] iface(2) ..., [inject] final
-//   aux: [start] fine(1), [iface(1)] fine(2) ..., inject
-// The statistics read the state fine(2) and iface(2) overwrite; both follow
-// iface(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] iface(sub), [9] inject.
+//   s:   stats, sfinal, coarse, corners (every substep, with the extraction),
+//        eval(1), [fine(1)] eval(2) ..., [inject] final
+//   aux: [start] fine(1), [eval(1)] fine(2) ..., inject
+// The statistics read the state fine(2) and eval(2) overwrite; both follow
+// eval(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] eval(sub), [9] inject.
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
                  cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats) {
   cudaEventRecord(ev[0], s);
@@ -708,14 +775,17 @@ void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned 
     b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
   }
   b_coarse<<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
-  b_extract<<<g.extract, kThreads, 0, s>>>(m, dyn);
+  CornerTimes ct{};
+  ct.gr = gr;
+  for (int t = 0; t < gr && t < 4; t++) ct.w[t] = time_weights(t + 1, gr);
+  b_icorner_all<<<g.icorner, kThreads, 0, s>>>(m, dyn, ct);
   for (int sub = 1; sub <= gr; sub++) {
     const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);
     if (sub > 1) cudaStreamWaitEvent(aux, ev[5 + sub - 2], 0);
     launch_fine(m, dyn, state, mode, sub, g, aux);
     cudaEventRecord(ev[1 + sub - 1], aux);
     if (sub > 1) cudaStreamWaitEvent(s, ev[1 + sub - 2], 0);
-    launch_iface(m, dyn, gr, sub, g, s);
+    launch_eval(m, dyn, gr, sub, g, s);
     cudaEventRecord(ev[5 + sub - 1], s);
   }
   b_inject<<<g.inject, kThreads, 0, aux>>>(m, dyn);
