@@ -257,3 +257,30 @@ def test_one_at_a_time_server_is_first_come_first_served(pkg):
     np.testing.assert_allclose([r.latency for r in recs], lat, rtol=1e-12, atol=1e-12)
     assert recs[3].status == -4 and "cf" not in recs[3].result
     assert all(r.status == 0 and "slip_length" in r.result for r in recs if r is not recs[3])
+
+
+def test_server_bounds_the_resident_work_per_step(pkg):
+    """With the per-step work bound, requests are admitted while the resident
+    set's node updates per step stay under it (a request is always admitted
+    to an idle GPU), so a backlog completes in arrival order instead of every
+    request sharing the GPU until the end."""
+    reqs = W.request_stream(rate=1000.0, n=10, seed=9, budget=(300, 300))
+    fp = {r.seed: 1 for r in reqs}
+    clk = Clock()
+    fb = FakeBatch(clk)
+    per = max(r.updates_per_step() for r in reqs)
+    srv = S.Server(pkg, batch=fb, hbm_budget=1e12, group=32, max_updates=2.5 * per)
+    srv.footprint = lambda inst: fp[inst.seed]
+    recs = srv.run(reqs, clock=clk, sleep=clk.sleep)
+    assert all(r.status == 0 for r in recs)
+    least = min(r.updates_per_step() for r in reqs)
+    assert fb.resident_max <= int(2.5 * per / least) and fb.resident_max < 10 and srv.active_updates == 0
+    fin = [r.finished for r in recs]
+    assert fin == sorted(fin)
+    # unbounded, all ten are resident at once
+    clk2 = Clock()
+    fb2 = FakeBatch(clk2)
+    srv2 = S.Server(pkg, batch=fb2, hbm_budget=1e12, group=32, max_updates=None)
+    srv2.footprint = lambda inst: fp[inst.seed]
+    srv2.run(reqs, clock=clk2, sleep=clk2.sleep)
+    assert fb2.resident_max == 10
