@@ -358,7 +358,7 @@ def bench_served(pkg, torch, args, peak):
                    "Admission: first come first served while the footprint fits the HBM budget and the resident "
                    "requests do at most max_resident_updates_per_step node updates a step (the GPU is saturated "
                    "by one production-size channel; beyond that, more residents only share it).",
-           "max_resident_updates_per_step": 32e6, "rates": {}}
+           "max_resident_updates_per_step": 64e6, "rates": {}}
     for rate in args.c5_rates:
         reqs = W.request_stream(rate, args.c5_requests, seed=7)
         srv = S.Server(pkg, hbm_budget=150e9, group=32, sample_every=20)

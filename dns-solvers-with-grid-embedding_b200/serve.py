@@ -47,14 +47,17 @@ class Server:
     max_updates: node updates per coarse step the resident instances may do
     together (None: no bound).  The batched kernels reach their throughput
     with one production-size channel resident (c2, 11 M updates a step, runs
-    within 4% of 96 channels' 378 M), so admitting beyond a few times that
-    only shares the GPU among more requests: every one of them then finishes
-    near the end of the backlog instead of in arrival order.  The default
-    bound, 32 M, keeps the GPU saturated and completions in arrival order.
+    within 4% of 96 channels' 378 M), so admitting far beyond that only
+    shares the GPU among more requests: every one of them then finishes near
+    the end of the backlog instead of in arrival order (measured on B200 at 10
+    requests/s: p50 99 s unbounded, 62 s at 32 M).  Small drawn channels run
+    less efficiently than one large one, so the bound keeps several resident:
+    at 32 M the aggregate fell to 26.9 from 28.9 GLUPS; the default, 64 M,
+    keeps the throughput.
     """
 
     def __init__(self, pkg, batch=None, hbm_budget: float = 150e9, group: int = 32, sample_every: int = 20,
-                 device: int = 0, max_updates: float | None = 32e6):
+                 device: int = 0, max_updates: float | None = 64e6):
         self.pkg = pkg
         self.batch = batch if batch is not None else pkg.Batch(device)
         self.budget = hbm_budget
