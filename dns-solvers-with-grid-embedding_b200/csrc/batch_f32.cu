@@ -364,8 +364,15 @@ struct CornerTimes {
   TimeW w[4];  // substeps 1..gr
 };
 constexpr int kCQX = CTX + 4, kCQY = CTY + 4, kCNV = (kCQX * kCQY + kThreads - 1) / kThreads;
-static_assert(kCornerFieldGroups == 3, "field groups of b_icorner_all");
-constexpr int kCornerFieldsMax = 8;  // fields per group: 7, 8, 8
+// work items per (tile, wall) of b_icorner_all: field groups (each also forms
+// the level-n moments of its tile and halo)
+#ifndef DNS_ALL_CORNER_GROUPS
+#define DNS_ALL_CORNER_GROUPS 3
+#endif
+constexpr int kAllCornerGroups = DNS_ALL_CORNER_GROUPS;
+static_assert(kAllCornerGroups >= 1 && kAllCornerGroups <= 8, "field groups of b_icorner_all");
+__host__ __device__ constexpr int all_corner_field(int g) { return 23 * g / kAllCornerGroups; }
+constexpr int kCornerFieldsMax = (23 + kAllCornerGroups - 1) / kAllCornerGroups;
 struct CornerAllSmem {
   IfCornerSmem S;
   float N[kCornerFieldsMax][kCQX * kCQY];  // level n of the group's fields, tile and halo
@@ -374,7 +381,8 @@ struct CornerAllSmem {
 template <int G>
 __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &I, const Dyn &D, int tx, int ty,
                                                   int w, const CornerTimes &ct) {
-  constexpr int F0 = corner_field(G), F1 = corner_field(G + 1);
+  constexpr int F0 = all_corner_field(G), F1 = all_corner_field(G + 1);
+  static_assert(F1 - F0 <= kCornerFieldsMax, "group size");
   const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
   const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
   const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
@@ -472,11 +480,17 @@ __global__ void __launch_bounds__(kThreads) b_icorner_all(const Mix *__restrict_
     local /= I.igx;
     const int ty = local % I.igy;
     local /= I.igy;
-    const int wall = local / kCornerFieldGroups, g = local - wall * kCornerFieldGroups;
+    const int wall = local / kAllCornerGroups, g = local - wall * kAllCornerGroups;
     // block-uniform; each ends with a barrier
-    if (g == 0) corner_all_tile32<0>(C, I, D, tx, ty, wall, ct);
-    else if (g == 1) corner_all_tile32<1>(C, I, D, tx, ty, wall, ct);
-    else corner_all_tile32<2>(C, I, D, tx, ty, wall, ct);
+    switch (g) {
+#define DNS_CORNER_GROUP(G) \
+  case G:                   \
+    if (G < kAllCornerGroups) corner_all_tile32<(G < kAllCornerGroups ? G : 0)>(C, I, D, tx, ty, wall, ct); \
+    break;
+      DNS_CORNER_GROUP(0) DNS_CORNER_GROUP(1) DNS_CORNER_GROUP(2) DNS_CORNER_GROUP(3)
+      DNS_CORNER_GROUP(4) DNS_CORNER_GROUP(5) DNS_CORNER_GROUP(6) DNS_CORNER_GROUP(7)
+#undef DNS_CORNER_GROUP
+    }
   }
 }
 
@@ -708,7 +722,7 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   c[PH_SFINAL] = I.nzp;
   c[PH_COARSE] = I.nzc * cb;
   c[PH_FINE] = 2 * I.zds * fb;
-  c[PH_ICORNER] = 2 * kCornerFieldGroups * I.igx * I.igy;
+  c[PH_ICORNER] = 2 * kAllCornerGroups * I.igx * I.igy;
   const int etx = I.gr == 2 ? IfTile<2>::TX : (I.gr == 3 ? IfTile<3>::TX : IfTile<4>::TX);
   const int ety = I.gr == 2 ? IfTile<2>::TY : (I.gr == 3 ? IfTile<3>::TY : IfTile<4>::TY);
   c[PH_IEVAL] = 2 * kEvalPopGroups * ((I.nx + etx - 1) / etx) * ((I.ny + ety - 1) / ety);
