@@ -196,11 +196,15 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
   const int kwall = upper ? zdf - 1 : 0;
   const size_t pstride = (size_t)P * ny * nx;
   const double Gf = (1. / ((double)gr)) * st->force;
-  // encalc2 weight of a destination plane (block-uniform)
-  auto weight = [&](int kd) -> double {
-    if (!upper) return (kd >= 1 && kd < zdf - gr) ? 1.0 : 0.0;
-    return (kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5 : 1.0) : 0.0;
-  };
+  // encalc2 weights of the destination planes k - 1, k, k + 1 (block-uniform;
+  // a push into the wall plane stays on plane k)
+  double wz[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int kd = k + c - 1;
+    wz[c] = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.0 : 0.0)
+                   : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5 : 1.0) : 0.0);
+  }
   const bool wall_sum_plane =
       upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
   const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
@@ -237,7 +241,8 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
       const int k2 = k + ez_of(a);
       const int i2 = ex_of(a) > 0 ? ip : (ex_of(a) < 0 ? im : i);
       const int j2 = ey_of(a) > 0 ? jp : (ey_of(a) < 0 ? jm : j);
-      int pd, id, jd, ad, kd, exd;
+      int pd, id, jd, ad, exd;
+      double wgt;  // encalc2 weight of the destination plane
       if (k2 == kwall) {
         const int8_t sld = wf[(size_t)j2 * nx + i2];
         if (sld == -1 && own == -1) {
@@ -245,15 +250,15 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
         } else {
           pd = p; id = i2; jd = j2; ad = mir_of(a); exd = ex_of(a);
         }
-        kd = k;
+        wgt = wz[1];
       } else {
         if (!upper && k2 >= zdf - 1) continue;
         if (upper && k2 <= 0) continue;
-        pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; kd = k2; exd = ex_of(a);
+        pd = upper ? zds + k2 : k2 - 1; id = i2; jd = j2; ad = a; exd = ex_of(a);
+        wgt = wz[ez_of(a) + 1];
       }
       dst[(size_t)ad * pstride + ((size_t)pd * ny + jd) * nx + id] = f[a];
       if ((MODE & 1) && !unit_plane) {
-        const double wgt = weight(kd);
         acc[1] += wgt * f[a];
         if (exd > 0) acc[0] += wgt * f[a];
         if (exd < 0) acc[0] -= wgt * f[a];
