@@ -647,14 +647,18 @@ def run_ours(args, rank, world, local_rank):
         tile32 = b1.autotune(p32, steps=5)[0] if args.autotune else None
         b1.add(p32, steps=10 ** 9, seed=42 + rank)
         b1.run(args.warmup)
-        ms32 = timed_batch_run(torch, b1, args.steps)
+        # the batched engine replays 32-step graphs and single-step graphs for
+        # the rest: timed over whole groups (at least 128 steps) so that the
+        # figure is the replayed step's, not the single-step graphs'
+        n32 = max(128, -(-args.steps // 32) * 32)
+        ms32 = max_over_ranks(torch, dist, timed_batch_run(torch, b1, n32))
         b1.close()
-        v32 = U * args.steps * world / (ms32 * 1e-3) / 1e6
-        line["fp32"] = {"value": v32, "unit": "MLUPS", "ms_per_step": ms32 / args.steps,
+        v32 = U * n32 * world / (ms32 * 1e-3) / 1e6
+        line["fp32"] = {"value": v32, "unit": "MLUPS", "steps": n32, "ms_per_step": ms32 / n32,
                         "dtype": "f32 (deviation storage, FP64 reductions)", "engine": "batched, one instance",
                         "tile": tile32 if tile32 else "default",
                         "over_fp64": v32 / value,
-                        "whole_step_hbm_frac": (U * args.steps * 152 / (ms32 * 1e-3) / 1e9) / peak}
+                        "whole_step_hbm_frac": (U * n32 * 152 / (ms32 * 1e-3) / 1e9) / peak}
     if world == 1 and not args.no_batched:
         line["batched"] = bench_batched(pkg, torch, args, peak)
     if batched_multi is not None:
