@@ -95,56 +95,111 @@ def traffic_from_profiles(kernel: str, config: str):
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+    """SM clocks and throttle reasons sampled during the timed region: NVML
+    read every millisecond or so on a thread (nvidia-smi's 200 ms loop when
+    NVML is missing).  mark() brackets the timed region on the host clock;
+    the summary keeps the samples inside it (all of them if none fell inside)."""
 
     FIELDS = ("clocks.sm,clocks.max.sm,clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap,power.draw")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index: int):
-        self.index = index
-        self.rows = []
+    def __init__(self, index: int, bus_id: str | None = None):
+        self.index, self.bus_id = index, bus_id
+        self.rows = []  # (host time, sm MHz, max sm MHz, 4 reason flags)
+        self.window = None
         self.proc = None
         self.thread = None
+        self.stop = threading.Event()
+        self.source = None
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
-                 "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.thread = threading.Thread(target=self._read, daemon=True)
+            import pynvml
+
+            pynvml.nvmlInit()
+            h = None
+            if self.bus_id:
+                try:
+                    h = pynvml.nvmlDeviceGetHandleByPciBusId(self.bus_id)
+                except pynvml.NVMLError:
+                    h = None
+            if h is None:
+                h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.thread = threading.Thread(target=self._nvml, args=(pynvml, h), daemon=True)
+            self.source = "nvml"
+        except Exception:
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                     "-i", str(self.index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.thread = threading.Thread(target=self._smi, daemon=True)
+                self.source = "nvidia-smi"
+            except FileNotFoundError:
+                self.proc = None
+        if self.thread:
             self.thread.start()
-        except FileNotFoundError:
-            self.proc = None
         return self
 
-    def _read(self):
+    def _nvml(self, nv, h):
+        bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        try:
+            mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+            while not self.stop.is_set():
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((time.perf_counter(), float(sm), float(mx)) + tuple(bool(r & b) for b in bits))
+                time.sleep(0.001)
+        except Exception:
+            pass
+
+    def _smi(self):
         for line in self.proc.stdout:
             parts = [x.strip() for x in line.split(",")]
-            if len(parts) >= 7:
-                self.rows.append(parts)
+            if len(parts) >= 7 and parts[0].replace(".", "").isdigit():
+                self.rows.append((time.perf_counter(), float(parts[0]), float(parts[1]))
+                                 + tuple(parts[2 + q].lower() == "active" for q in range(4)))
+
+    def mark(self, t0: float, t1: float):
+        self.window = (t0, t1)
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        if self.thread and self.source == "nvml":
+            self.thread.join(timeout=2)
 
     def summary(self):
-        if not self.rows:
+        rows = list(self.rows)
+        if self.window:
+            inside = [r for r in rows if self.window[0] <= r[0] <= self.window[1]]
+            rows = inside or rows
+        if not rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
-        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        reasons = sorted({names[q] for r in self.rows for q in range(4) if r[2 + q].lower() == "active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+        reasons = sorted({self.NAMES[q] for r in rows for q in range(4) if r[3 + q]})
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                "reasons": reasons, "samples": len(rows), "source": self.source}
 
 
-def reference_cpu(config: str, steps: int, processes: int, timeout: float = 900.0):
+def bus_id_of(torch, device: int):
+    """PCI bus id of a CUDA device in NVML's form, or None."""
+    try:
+        pr = torch.cuda.get_device_properties(device)
+        return f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+    except Exception:
+        return None
+
+
+def reference_cpu(config: str, steps: int, processes: int, timeout: float = 900.0, warmup: int = 0):
     """Time the reference's own routines (oracle/_ref/<config>/ref_harness, one
     rank per process, from rest, constant-force mode with zero force) on the host.
+    Each process runs warmup + steps steps and clocks the last `steps`.
     Returns each process's step-loop seconds (its own clock), or None when the
     binary is missing or a process gave no time."""
     exe = ROOT / "oracle" / "_ref" / config / "ref_harness"
@@ -155,7 +210,8 @@ def reference_cpu(config: str, steps: int, processes: int, timeout: float = 900.
         for q in range(processes):
             od = Path(d) / f"p{q}"
             od.mkdir()
-            procs.append(subprocess.Popen([str(exe), "-", "0", str(od), "-1", str(steps), "const", "0"],
+            procs.append(subprocess.Popen([str(exe), "-", "0", str(od), "-1", str(steps + warmup), "const", "0", "0", "0",
+                                           str(warmup)],
                                           stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True))
         secs = []
         for pr in procs:
@@ -184,6 +240,17 @@ def updates_per_step(m):
     return m["xdv"] * m["ydv"] * m["zdv"] + 2 * gr * (gr * m["xdv"]) * (gr * m["ydv"]) * m["zds"]
 
 
+def arm_config(args, world: int) -> dict:
+    """The workload description both arms print (same keys, same values)."""
+    m, desc = CONFIGS[args.config]
+    U = updates_per_step(m)
+    state = U * 2 * 19 * 8  # both ping-pong copies of every population, FP64
+    return {"workload": args.config, "description": desc, "updates_per_step": U,
+            "l2": (f"state {state / 1e9:.1f} GB of populations >> 126 MB L2 (no flush needed)"
+                   if state > 8 * 126e6 else f"state {state / 1e9:.2f} GB: not enough to defeat L2"),
+            "parallelism": f"replicas x{world}"}
+
+
 def run_reference_arm(args, rank, world):
     if rank != 0:
         return 0
@@ -192,12 +259,14 @@ def run_reference_arm(args, rank, world):
     # about 2.3 GB of AoS arrays per process at the default config
     per_proc = 19 * 8 * 2.2 * (U + 2 * (m["gratio"] * m["xdv"]) * (m["gratio"] * m["ydv"]))
     nproc = host_parallelism(per_proc)
-    steps = max(1, min(args.steps, args.ref_steps))
-    secs = reference_cpu(args.config, steps, nproc)
+    # the reference spends about 2.3 s per c2 step per process: K and W are
+    # capped so that the run stays within a few minutes
+    steps = max(1, min(args.steps, 40))
+    warm = max(0, min(args.warmup, 5))
+    secs = reference_cpu(args.config, steps, nproc, warmup=warm)
     line = {"impl": "reference", "metric": METRIC, "unit": "MLUPS", "n_gpus": world, "steps": steps,
-            "warmup": 0, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (reference cold start from rest)",
-            "config": {"workload": args.config, "description": desc}}
+            "warmup": warm, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (reference cold start from rest)", "config": arm_config(args, world)}
     if secs is None:
         line["unavailable"] = "compiled reference binary missing (oracle/_ref not built)"
         print(json.dumps(line), flush=True)
@@ -206,7 +275,8 @@ def run_reference_arm(args, rank, world):
     line.update({"value": mlups, "ms_per_step": 1e3 * max(secs) / steps})
     line["cpu_baseline"] = {"value": mlups, "unit": "MLUPS", "cores": len(secs), "kind": "reference",
                             "sample": f"{len(secs)} concurrent single-rank reference processes x {steps} coarse "
-                                      f"steps of {args.config} (own step-loop clock, main's t2-t4)"}
+                                      f"steps of {args.config} after {warm} untimed ones (own step-loop clock, "
+                                      f"main's t2-t4)"}
     line["e2e"] = {"value": mlups, "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
     return 0
@@ -539,13 +609,15 @@ def run_ours(args, rank, world, local_rank):
 
     # ---- timed region: K coarse steps, state resident in HBM
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with ClockSampler(local_rank) as clk:
-        time.sleep(0.5)  # let the sampler start before the timed region
+    with ClockSampler(local_rank, bus_id_of(torch, local_rank)) as clk:
+        time.sleep(0.2)  # let the sampler start before the timed region
         barrier()
+        t_host0 = time.perf_counter()
         start.record(stream)
         log = ch.step(args.steps, log=True)
         end.record(stream)
         barrier()
+        clk.mark(t_host0, time.perf_counter())
     ms = start.elapsed_time(end)
     # ---- per-kernel device time: the same steps again with CUDA events around
     # every launch on the library's stream (recording them slows the step a
@@ -615,11 +687,7 @@ def run_ours(args, rank, world, local_rank):
         "metric": METRIC, "value": value, "unit": "MLUPS", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (Philox-seeded laminar profile + noise)",
-        "config": {"workload": args.config, "description": desc, "updates_per_step": U,
-                   "l2": (f"state {geom.device_bytes / 1e9:.1f} GB >> 126 MB L2 (no flush needed)"
-                          if geom.device_bytes > 8 * 126e6 else
-                          f"state {geom.device_bytes / 1e9:.2f} GB: not enough to defeat L2"),
-                   "parallelism": f"replicas x{world}"},
+        "config": arm_config(args, world),
         "roofline": {"bound": "hbm", "kernel": "fine_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": (achieved / peak) if achieved else None, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": bytes_per_launch,
@@ -693,7 +761,6 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--config", choices=sorted(CONFIGS), default="c2")
     ap.add_argument("--cpu-steps", type=int, default=4)
-    ap.add_argument("--ref-steps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-fp32", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
@@ -708,7 +775,7 @@ def main():
     ap.add_argument("--c5-requests", type=int, default=200)
     ap.add_argument("--c5-fp64-requests", type=int, default=24,
                     help="first requests of each stream served alone by the FP32 loop and one at a time in FP64")
-    ap.add_argument("--c5-rates", type=float, nargs="+", default=[2.0, 10.0, 50.0])
+    ap.add_argument("--c5-rates", type=float, nargs="+", default=[10.0])
     ap.add_argument("--longrun-cases", nargs="*", default=["c2", "c3n", "c3r", "c3p"],
                     help="channels run long for the FP32-vs-FP64 statistics (none: skip)")
     ap.add_argument("--longrun-warmup", type=int, default=10000)

@@ -23,11 +23,12 @@
  * [ftemp | f] in global C order (i, j, k, a); lbf-uin / lbf-lin hold the
  * [n | p | pp] interface history (i, j, 23); force holds force[0].
  *
- * usage: ref_harness INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY] [FIELDS]
+ * usage: ref_harness INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY] [FIELDS] [WARMUP]
  * (INDIR "-" starts from rest instead of reading restart files; CNTR_OUT < 0
  *  skips the restart output, for timing; FIELDS = 1 also writes the
  *  reference's vel-* / den-* field files of the final state with its own
- *  vel_print, as main does at :1342)
+ *  vel_print, as main does at :1342; WARMUP > 0 starts the clock after that
+ *  many of the NSTEPS steps, so harness_seconds covers NSTEPS - WARMUP steps)
  * The step loop time (MPI_Wtime, as main's t2-t4) is printed as
  *   "harness_seconds <s>".
  */
@@ -125,7 +126,7 @@ static void write_history(const char *path, DP *n, DP *p, DP *pp, int xdc, int y
 }
 
 int main(int argc, char **argv) {
-  if (argc < 7) die("usage: INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY]", NULL);
+  if (argc < 7) die("usage: INDIR CNTR_IN OUTDIR CNTR_OUT NSTEPS cfr|const [G] [STATS_EVERY] [FIELDS] [WARMUP]", NULL);
   const char *indir = argv[1], *outdir = argv[3];
   int cin = atoi(argv[2]), cout = atoi(argv[4]);
   long nsteps = atol(argv[5]);
@@ -134,6 +135,8 @@ int main(int argc, char **argv) {
   double gconst = argc > 7 ? strtod(argv[7], NULL) : 0.0;
   long stats_every = argc > 8 ? atol(argv[8]) : 0;
   int fields = argc > 9 ? atoi(argv[9]) : 0;
+  long warmup = argc > 10 ? atol(argv[10]) : 0;
+  if (warmup < 0 || warmup >= nsteps) warmup = 0;
 
   int dims[2] = {XDIM, YDIM}, period[2] = {1, 1};
   MPI_Init(&argc, &argv);
@@ -272,6 +275,7 @@ cold_start:
   DP Gx = 0.;
   double t4 = MPI_Wtime();
   for (long ss = 0; ss < nsteps; ss++) {
+    if (ss == warmup && warmup > 0) t4 = MPI_Wtime();
     V = encalc2(xdc, ydc, zdc, xdf, ydf, zdf, GR, V, pd, TM, ss, ubulk);
     if (!cfr) V.force[0] = gconst;
     V = wshearstr(xdf, ydf, zdf, zdc, GR, V, pd, tauf, TM, ss);
