@@ -373,6 +373,113 @@ constexpr int kAllCornerGroups = DNS_ALL_CORNER_GROUPS;
 static_assert(kAllCornerGroups >= 1 && kAllCornerGroups <= 8, "field groups of b_icorner_all");
 __host__ __device__ constexpr int all_corner_field(int g) { return 23 * g / kAllCornerGroups; }
 constexpr int kCornerFieldsMax = (23 + kAllCornerGroups - 1) / kAllCornerGroups;
+// DNS_CORNER_PHASED 1: every field of the group in each barrier phase (three
+// phases per substep); 0: one field at a time (three phases per field and
+// substep).
+#ifndef DNS_CORNER_PHASED
+#define DNS_CORNER_PHASED 1
+#endif
+#if DNS_CORNER_PHASED
+struct CornerAllSmem {
+  float N[kCornerFieldsMax][kCQY][kCQX];  // level n of the group's fields, tile and halo
+  float V[kCornerFieldsMax][kCQY][kCQX];  // substep t's values
+  float DY[kCornerFieldsMax][CTY][kCQX];  // their y derivatives on the tile's rows
+};
+
+template <int G>
+__device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &I, const Dyn &D, int tx, int ty,
+                                                  int w, const CornerTimes &ct) {
+  constexpr int F0 = all_corner_field(G), F1 = all_corner_field(G + 1), NF = F1 - F0;
+  static_assert(NF <= kCornerFieldsMax, "group size");
+  constexpr int kDY = NF * CTY * kCQX, kDX = NF * CTY * CTX;
+  const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
+  const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
+  const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
+  const int k = w == 0 ? 1 : I.nzc - 2;
+  const size_t pstride = (size_t)I.nzc * plane;
+  const float *fc = I.fc[D.cc ^ 1] + (size_t)k * plane;  // the coarse state just streamed
+  // ring after this step's rotation: level n in the old pp slot, p in old n, pp in old p
+  float *hn = I.hist + (size_t)D.hpp * hs + ((size_t)w * 23 + F0) * plane;
+  const float *hp = I.hist + (size_t)D.hn * hs + ((size_t)w * 23 + F0) * plane;
+  const float *hpp = I.hist + (size_t)D.hp * hs + ((size_t)w * 23 + F0) * plane;
+  int off[kCNV];
+#pragma unroll
+  for (int s = 0; s < kCNV; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    off[s] = q < kCQX * kCQY ? wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx) : -1;
+  }
+#pragma unroll
+  for (int s = 0; s < kCNV; s++) {
+    const int q = threadIdx.x + s * kThreads;
+    if (off[s] < 0) continue;
+    float d[19];
+    load19f(fc, (size_t)off[s], pstride, d);
+    const Mac32 m = macro_f32(d);
+    const int qi = q % kCQX - 2, qj = q / kCQX - 2;
+    const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < CTY && i0 + qi < nx && j0 + qj < ny;
+#pragma unroll
+    for (int f = 0; f < NF; f++) {
+      const int fg = F0 + f;
+      const float v = fg == 0 ? m.drho
+                      : fg == 1 ? m.u0
+                      : fg == 2 ? m.u1
+                      : fg == 3 ? m.u2 : d[fg - 4] - deq_f32(fg - 4, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
+      C.N[f][q / kCQX][q % kCQX] = v;
+      if (own) hn[(size_t)f * plane + off[s]] = v;
+    }
+  }
+  for (int t = 0; t < ct.gr; t++) {
+    const TimeW tw = ct.w[t];
+    // Hermite-in-time values of every field of the group on the tile and halo
+    // (each thread combines the level-n values it wrote itself); levels p and
+    // pp are read only where their weights are not zero (not in the last
+    // substep, which is level n alone)
+    const bool lv = tw.ap != 0.f || tw.app != 0.f;
+#pragma unroll 2
+    for (int s = 0; s < kCNV; s++) {
+      const int q = threadIdx.x + s * kThreads;
+      if (q >= kCQX * kCQY) continue;
+      const int o = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
+      float a[NF], b[NF];
+#pragma unroll
+      for (int f = 0; f < NF; f++) {
+        a[f] = lv ? __ldg(hp + (size_t)f * plane + o) : 0.f;
+        b[f] = lv ? __ldg(hpp + (size_t)f * plane + o) : 0.f;
+      }
+#pragma unroll
+      for (int f = 0; f < NF; f++)
+        C.V[f][q / kCQX][q % kCQX] = tw.an * C.N[f][q / kCQX][q % kCQX] + tw.ap * a[f] + tw.app * b[f];
+    }
+    __syncthreads();
+#pragma unroll 3
+    for (int s = 0; s < (kDY + kThreads - 1) / kThreads; s++) {
+      const int e = threadIdx.x + s * kThreads;
+      if (e < kDY) {
+        const int f = e / (CTY * kCQX), r = (e / kCQX) % CTY, pi = e % kCQX;
+        C.DY[f][r][pi] = c2o3 * (C.V[f][r + 3][pi] - C.V[f][r + 1][pi]) - c1o12 * (C.V[f][r + 4][pi] - C.V[f][r][pi]);
+      }
+    }
+    __syncthreads();
+    float4 *out = I.corner + (size_t)t * hs + ((size_t)w * 23 + F0) * plane;
+#pragma unroll 2
+    for (int s = 0; s < (kDX + kThreads - 1) / kThreads; s++) {
+      const int e = threadIdx.x + s * kThreads;
+      if (e < kDX) {
+        const int f = e / (CTY * CTX), r = (e / CTX) % CTY, c = e % CTX;
+        if (i0 + c < nx && j0 + r < ny) {
+          const float dx = c2o3 * (C.V[f][r + 2][c + 3] - C.V[f][r + 2][c + 1]) -
+                           c1o12 * (C.V[f][r + 2][c + 4] - C.V[f][r + 2][c]);
+          const float dxy =
+              c2o3 * (C.DY[f][r][c + 3] - C.DY[f][r][c + 1]) - c1o12 * (C.DY[f][r][c + 4] - C.DY[f][r][c]);
+          out[(size_t)f * plane + (size_t)(j0 + r) * nx + i0 + c] =
+              make_float4(C.V[f][r + 2][c + 2], dx, C.DY[f][r][c + 2], dxy);
+        }
+      }
+    }
+    __syncthreads();  // V and DY are rewritten for the next substep or item
+  }
+}
+#else
 struct CornerAllSmem {
   IfCornerSmem S;
   float N[kCornerFieldsMax][kCQX * kCQY];  // level n of the group's fields, tile and halo
@@ -459,6 +566,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     }
   }
 }
+#endif
 
 __global__ void __launch_bounds__(kThreads) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
                                                           CornerTimes ct) {
