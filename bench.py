@@ -347,6 +347,18 @@ def bench_batched(pkg, torch, args, peak, rank=0, world=1, dist=None, device=0):
     insts = [everything[q] for q in mine]
     every = 20
     b = pkg.Batch(device)
+    tuned = {}
+    if args.autotune:
+        # the engine's tuner on each distinct grid shape; admissions of that
+        # shape then take the tuned tile
+        t0 = time.perf_counter()
+        for x in insts:
+            p = x.params(pkg)
+            p.device = device
+            key = (p.xdv, p.ydv, p.zdv, p.zds, p.gratio)
+            if key not in tuned:
+                tuned[key] = b.autotune(p, steps=5)
+        tune_s = time.perf_counter() - t0
     ids = []
     for x in insts:
         p = x.params(pkg)
@@ -367,10 +379,12 @@ def bench_batched(pkg, torch, args, peak, rank=0, world=1, dist=None, device=0):
     failed = int(sum_over_ranks(torch, dist, sum(1 for i in ids if b.info(i).status != 0)))
     stats32 = [b.stats(i)[0] if b.info(i).status == 0 else None for i in ids]
     b.close()
+    tiles = ({"tuned_shapes": len(tuned), "tuning_seconds": tune_s,
+              "tiles": {"x".join(map(str, k)): list(v[0]) for k, v in tuned.items()}} if tuned else "default")
     if args.no_c4_reference:
         return {"value": value, "unit": "MLUPS", "instances": len(everything), "gpus": world, "steps": steps,
                 "ms_per_step": ms / steps, "updates_per_step": U, "failed_instances": failed,
-                "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak}
+                "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak, "tile": tiles}
     # the same channels one after another in FP64 (device time of each whole
     # run), every rank its own shard, and the per-instance comparison
     seq_ms, errs, f64_failed = 0.0, {name: [] for name in W.STAT_NAMES.values()}, 0
@@ -393,7 +407,7 @@ def bench_batched(pkg, torch, args, peak, rank=0, world=1, dist=None, device=0):
         "value": value, "unit": "MLUPS", "dtype": "f32 (deviation storage, FP64 reductions)",
         "instances": len(everything), "gpus": world, "steps": steps, "warmup": args.warmup, "ms_per_step": ms / steps,
         "updates_per_step": U, "device_bytes": held, "failed_instances": failed,
-        "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak,
+        "whole_step_hbm_frac": (work * 152 / (ms * 1e-3) / 1e9) / peak, "tile": tiles,
         "re_tau_drawn_range": [min(x.re_tau for x in insts), max(x.re_tau for x in insts)],
         "re_tau_run_range": [min(x.re_tau_run for x in insts), max(x.re_tau_run for x in insts)],
         "gas_fraction_range": [min(x.gas_fraction for x in insts), max(x.gas_fraction for x in insts)],
@@ -767,7 +781,8 @@ def main():
     ap.add_argument("--no-served", action="store_true")
     ap.add_argument("--no-budget", action="store_true")
     ap.add_argument("--autotune", action=argparse.BooleanOptionalAction, default=False,
-                    help="autotune the FP32 leg's tile (the engine's own tuner) before timing it")
+                    help="autotune the tiles of the FP32 and batched legs (the engine's own tuner, "
+                         "per grid shape) before timing them")
     ap.add_argument("--c4-instances", type=int, default=96)
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--no-c4-reference", action="store_true",

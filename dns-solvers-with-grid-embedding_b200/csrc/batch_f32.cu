@@ -363,7 +363,7 @@ struct CornerTimes {
   int gr;
   TimeW w[4];  // substeps 1..gr
 };
-constexpr int kCQX = CTX + 4, kCQY = CTY + 4, kCNV = (kCQX * kCQY + kThreads - 1) / kThreads;
+constexpr int kCQX = CTX + 4, kCQY = CTY + 4;
 // work items per (tile, wall) of b_icorner_all: field groups (each also forms
 // the level-n moments of its tile and halo)
 #ifndef DNS_ALL_CORNER_GROUPS
@@ -380,18 +380,29 @@ constexpr int kCornerFieldsMax = (23 + kAllCornerGroups - 1) / kAllCornerGroups;
 #define DNS_CORNER_PHASED 1
 #endif
 #if DNS_CORNER_PHASED
-struct CornerAllSmem {
+// threads per block of b_icorner_all: the halo's population loads of one item
+// are spread over more threads, so that more of them are in flight at once
+#ifndef DNS_CORNER_THREADS
+#define DNS_CORNER_THREADS 256
+#endif
+constexpr int kCornerThreads = DNS_CORNER_THREADS;
+constexpr int kCNVP = (kCQX * kCQY + kCornerThreads - 1) / kCornerThreads;
+static_assert(kCQX % 4 == 0 && CTX % 4 == 0, "four-wide shared-memory rows");
+struct __align__(16) CornerAllSmem {
   float N[kCornerFieldsMax][kCQY][kCQX];  // level n of the group's fields, tile and halo
   float V[kCornerFieldsMax][kCQY][kCQX];  // substep t's values
   float DY[kCornerFieldsMax][CTY][kCQX];  // their y derivatives on the tile's rows
 };
+
+__device__ __forceinline__ float4 ld4s(const float *p) { return *reinterpret_cast<const float4 *>(p); }
 
 template <int G>
 __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &I, const Dyn &D, int tx, int ty,
                                                   int w, const CornerTimes &ct) {
   constexpr int F0 = all_corner_field(G), F1 = all_corner_field(G + 1), NF = F1 - F0;
   static_assert(NF <= kCornerFieldsMax, "group size");
-  constexpr int kDY = NF * CTY * kCQX, kDX = NF * CTY * CTX;
+  // four-wide groups: y derivatives over the halo's columns, x derivatives over the tile's
+  constexpr int kDY = NF * CTY * (kCQX / 4), kDX = NF * CTY * (CTX / 4);
   const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
   const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
   const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
@@ -402,18 +413,14 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
   float *hn = I.hist + (size_t)D.hpp * hs + ((size_t)w * 23 + F0) * plane;
   const float *hp = I.hist + (size_t)D.hn * hs + ((size_t)w * 23 + F0) * plane;
   const float *hpp = I.hist + (size_t)D.hp * hs + ((size_t)w * 23 + F0) * plane;
-  int off[kCNV];
+  const int t0 = threadIdx.x;
 #pragma unroll
-  for (int s = 0; s < kCNV; s++) {
-    const int q = threadIdx.x + s * kThreads;
-    off[s] = q < kCQX * kCQY ? wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx) : -1;
-  }
-#pragma unroll
-  for (int s = 0; s < kCNV; s++) {
-    const int q = threadIdx.x + s * kThreads;
-    if (off[s] < 0) continue;
+  for (int s = 0; s < kCNVP; s++) {
+    const int q = t0 + s * kCornerThreads;
+    if (q >= kCQX * kCQY) continue;
+    const int off = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
     float d[19];
-    load19f(fc, (size_t)off[s], pstride, d);
+    load19f(fc, (size_t)off, pstride, d);
     const Mac32 m = macro_f32(d);
     const int qi = q % kCQX - 2, qj = q / kCQX - 2;
     const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < CTY && i0 + qi < nx && j0 + qj < ny;
@@ -425,7 +432,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
                       : fg == 2 ? m.u1
                       : fg == 3 ? m.u2 : d[fg - 4] - deq_f32(fg - 4, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
       C.N[f][q / kCQX][q % kCQX] = v;
-      if (own) hn[(size_t)f * plane + off[s]] = v;
+      if (own) hn[(size_t)f * plane + off] = v;
     }
   }
   for (int t = 0; t < ct.gr; t++) {
@@ -435,44 +442,57 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     // pp are read only where their weights are not zero (not in the last
     // substep, which is level n alone)
     const bool lv = tw.ap != 0.f || tw.app != 0.f;
-#pragma unroll 2
-    for (int s = 0; s < kCNV; s++) {
-      const int q = threadIdx.x + s * kThreads;
-      if (q >= kCQX * kCQY) continue;
-      const int o = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
-      float a[NF], b[NF];
 #pragma unroll
-      for (int f = 0; f < NF; f++) {
-        a[f] = lv ? __ldg(hp + (size_t)f * plane + o) : 0.f;
-        b[f] = lv ? __ldg(hpp + (size_t)f * plane + o) : 0.f;
+    for (int s = 0; s < kCNVP; s++) {
+      const int q = t0 + s * kCornerThreads;
+      if (q >= kCQX * kCQY) continue;
+      float a[NF], b[NF];
+      if (lv) {
+        const int o = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
+#pragma unroll
+        for (int f = 0; f < NF; f++) {
+          a[f] = __ldg(hp + (size_t)f * plane + o);
+          b[f] = __ldg(hpp + (size_t)f * plane + o);
+        }
+      } else {
+#pragma unroll
+        for (int f = 0; f < NF; f++) a[f] = b[f] = 0.f;
       }
 #pragma unroll
       for (int f = 0; f < NF; f++)
         C.V[f][q / kCQX][q % kCQX] = tw.an * C.N[f][q / kCQX][q % kCQX] + tw.ap * a[f] + tw.app * b[f];
     }
     __syncthreads();
-#pragma unroll 3
-    for (int s = 0; s < (kDY + kThreads - 1) / kThreads; s++) {
-      const int e = threadIdx.x + s * kThreads;
+#pragma unroll 2
+    for (int s = 0; s < (kDY + kCornerThreads - 1) / kCornerThreads; s++) {
+      const int e = t0 + s * kCornerThreads;
       if (e < kDY) {
-        const int f = e / (CTY * kCQX), r = (e / kCQX) % CTY, pi = e % kCQX;
-        C.DY[f][r][pi] = c2o3 * (C.V[f][r + 3][pi] - C.V[f][r + 1][pi]) - c1o12 * (C.V[f][r + 4][pi] - C.V[f][r][pi]);
+        const int f = e / (CTY * (kCQX / 4)), r = (e / (kCQX / 4)) % CTY, c = 4 * (e % (kCQX / 4));
+        const float4 v0 = ld4s(&C.V[f][r][c]), v1 = ld4s(&C.V[f][r + 1][c]), v3 = ld4s(&C.V[f][r + 3][c]),
+                     v4 = ld4s(&C.V[f][r + 4][c]);
+        *reinterpret_cast<float4 *>(&C.DY[f][r][c]) =
+            make_float4(c2o3 * (v3.x - v1.x) - c1o12 * (v4.x - v0.x), c2o3 * (v3.y - v1.y) - c1o12 * (v4.y - v0.y),
+                        c2o3 * (v3.z - v1.z) - c1o12 * (v4.z - v0.z), c2o3 * (v3.w - v1.w) - c1o12 * (v4.w - v0.w));
       }
     }
     __syncthreads();
     float4 *out = I.corner + (size_t)t * hs + ((size_t)w * 23 + F0) * plane;
 #pragma unroll 2
-    for (int s = 0; s < (kDX + kThreads - 1) / kThreads; s++) {
-      const int e = threadIdx.x + s * kThreads;
+    for (int s = 0; s < (kDX + kCornerThreads - 1) / kCornerThreads; s++) {
+      const int e = t0 + s * kCornerThreads;
       if (e < kDX) {
-        const int f = e / (CTY * CTX), r = (e / CTX) % CTY, c = e % CTX;
-        if (i0 + c < nx && j0 + r < ny) {
-          const float dx = c2o3 * (C.V[f][r + 2][c + 3] - C.V[f][r + 2][c + 1]) -
-                           c1o12 * (C.V[f][r + 2][c + 4] - C.V[f][r + 2][c]);
-          const float dxy =
-              c2o3 * (C.DY[f][r][c + 3] - C.DY[f][r][c + 1]) - c1o12 * (C.DY[f][r][c + 4] - C.DY[f][r][c]);
-          out[(size_t)f * plane + (size_t)(j0 + r) * nx + i0 + c] =
-              make_float4(C.V[f][r + 2][c + 2], dx, C.DY[f][r][c + 2], dxy);
+        const int f = e / (CTY * (CTX / 4)), r = (e / (CTX / 4)) % CTY, c0 = 4 * (e % (CTX / 4));
+        const float4 xa = ld4s(&C.V[f][r + 2][c0]), xb = ld4s(&C.V[f][r + 2][c0 + 4]);
+        const float4 ya = ld4s(&C.DY[f][r][c0]), yb = ld4s(&C.DY[f][r][c0 + 4]);
+        const float x[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
+        const float y[8] = {ya.x, ya.y, ya.z, ya.w, yb.x, yb.y, yb.z, yb.w};
+        if (j0 + r < ny) {
+          float4 *o = out + (size_t)f * plane + (size_t)(j0 + r) * nx + i0 + c0;
+#pragma unroll
+          for (int n = 0; n < 4; n++)
+            if (i0 + c0 + n < nx)
+              o[n] = make_float4(x[n + 2], c2o3 * (x[n + 3] - x[n + 1]) - c1o12 * (x[n + 4] - x[n]), y[n + 2],
+                                 c2o3 * (y[n + 3] - y[n + 1]) - c1o12 * (y[n + 4] - y[n]));
         }
       }
     }
@@ -480,6 +500,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
   }
 }
 #else
+constexpr int kCNV = (kCQX * kCQY + kThreads - 1) / kThreads;
 struct CornerAllSmem {
   IfCornerSmem S;
   float N[kCornerFieldsMax][kCQX * kCQY];  // level n of the group's fields, tile and halo
@@ -568,7 +589,10 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
 }
 #endif
 
-__global__ void __launch_bounds__(kThreads) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
+#if !DNS_CORNER_PHASED
+constexpr int kCornerThreads = kThreads;
+#endif
+__global__ void __launch_bounds__(kCornerThreads) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
                                                           CornerTimes ct) {
   __shared__ CornerAllSmem C;
   const int n = M->n;
@@ -813,11 +837,11 @@ __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, D
 }
 
 template <class K>
-int occupancy_grid(K kernel, int *grid) {
+int occupancy_grid(K kernel, int *grid, int threads = kThreads) {
   int dev = 0, sms = 0, per = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return -1;
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return -1;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, kThreads, 0) != cudaSuccess) return -1;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, kernel, threads, 0) != cudaSuccess) return -1;
   *grid = sms * (per > 0 ? per : 1);
   return 0;
 }
@@ -844,7 +868,7 @@ int query_grids(int gr, Grids *g) {
   rc |= occupancy_grid(b_sfinal, &g->sfinal);
   rc |= occupancy_grid(b_coarse, &g->coarse);
   rc |= occupancy_grid(b_fine<3>, &g->fine);
-  rc |= occupancy_grid(b_icorner_all, &g->icorner);
+  rc |= occupancy_grid(b_icorner_all, &g->icorner, kCornerThreads);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
   else rc |= occupancy_grid(b_ieval<4>, &g->ieval);
@@ -900,7 +924,7 @@ void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned 
   CornerTimes ct{};
   ct.gr = gr;
   for (int t = 0; t < gr && t < 4; t++) ct.w[t] = time_weights(t + 1, gr);
-  b_icorner_all<<<g.icorner, kThreads, 0, s>>>(m, dyn, ct);
+  b_icorner_all<<<g.icorner, kCornerThreads, 0, s>>>(m, dyn, ct);
   for (int sub = 1; sub <= gr; sub++) {
     const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);
     if (sub > 1) cudaStreamWaitEvent(aux, ev[5 + sub - 2], 0);
