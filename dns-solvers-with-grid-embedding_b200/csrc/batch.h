@@ -92,7 +92,6 @@ constexpr int kCornerTX = 32, kCornerTY = 8;
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
   int stats, sfinal, coarse, fine, icorner, ieval, inject, final_;
-  int fine_eval;  // fine substep and interface evaluation in one launch (GR = 2)
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)

@@ -669,12 +669,24 @@ extern "C" int dns_batch_log(dns_batch *b, int id, long long first, long long n,
 // shape: the fine tile first (the fine kernels carry most of the traffic),
 // then the coarse tile; each candidate is timed
 // over `steps` steps with CUDA events after two warm-up steps.
-static int time_tile(int device, const dns_params &p, const dns_tile &t, int steps, double *ms) {
+// Copies of a shape that the tuner times together: enough for about 32 M node
+// updates a step (the load of a full batch), at most 64 and 8 GB.  A lone
+// small channel leaves most of the GPU idle and would favour narrow tiles
+// that lose in a full batch.
+static int tune_copies(const dns_geometry &g, size_t bytes_each) {
+  const double per = (double)g.updates_per_step;
+  int c = (int)((32e6 + per - 1.) / per);
+  if (c > 64) c = 64;
+  if (bytes_each > 0 && (double)c * (double)bytes_each > 8e9) c = (int)(8e9 / (double)bytes_each);
+  return c < 1 ? 1 : c;
+}
+
+static int time_tile(int device, const dns_params &p, const dns_tile &t, int steps, int copies, double *ms) {
   dns_batch *sb = nullptr;
   int rc = dns_batch_create(device, &sb);
   if (rc) return rc;
   int id = -1;
-  rc = dns_batch_add(sb, &p, &t, 1, 0.05, 0.005, steps + 2, 0, &id);
+  for (int c = 0; c < copies && !rc; c++) rc = dns_batch_add(sb, &p, &t, 1 + c, 0.05, 0.005, steps + 2, 0, &id);
   if (!rc) rc = dns_batch_run(sb, 2, nullptr);
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (!rc) {
@@ -702,14 +714,17 @@ extern "C" int dns_batch_autotune(dns_batch *b, const dns_params *shape, int ste
   if (rc) return rc;
   dns_tile cur;
   dns_batch_tile_for(b, &q, &cur);
+  Inst I0;
+  shape_inst(I0, q, g, cur);
+  const int copies = tune_copies(g, layout_of(I0).total);
   double cur_ms = 0.;
-  if ((rc = time_tile(b->device, q, cur, steps, &cur_ms))) return rc;
+  if ((rc = time_tile(b->device, q, cur, steps, copies, &cur_ms))) return rc;
   auto consider = [&](const dns_tile &t) -> int {
     if (!tile_ok(t)) return DNS_OK;
     double m = 0.;
-    int r2 = time_tile(b->device, q, t, steps, &m);
+    int r2 = time_tile(b->device, q, t, steps, copies, &m);
     if (r2) return r2;
-    if (m < cur_ms) {
+    if (m < 0.99 * cur_ms) {  // a candidate must beat the current best by 1%
       cur_ms = m;
       cur = t;
     }

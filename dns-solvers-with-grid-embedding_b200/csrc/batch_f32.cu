@@ -672,44 +672,6 @@ __global__ void __launch_bounds__(kThreads) b_ieval(const Mix *__restrict__ M, c
   }
 }
 
-// ------------------------------------------------------------------ fine substep + interface evaluation
-// The fine stream-collide of substep sub and the same substep's interface
-// evaluation in one persistent launch (GR = 2).  They write disjoint planes of
-// the destination lattice (the fine items drop their pushes onto the interface
-// plane, which the evaluation writes) and neither reads what the other
-// writes, so their items can run side by side: the evaluation items
-// (latency-bound) are spread evenly through the fine items (bandwidth-bound),
-// item slot w of K = F + E being evaluation item e where w = floor(e K / E).
-#ifndef DNS_FUSE_EVAL
-#define DNS_FUSE_EVAL 1
-#endif
-template <int MODE, int GR>
-__global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
-    b_fine_eval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state, int sub,
-                TimeW tw) {
-  __shared__ IfEvalSmem<GR> S;
-  __shared__ IfParams32 P;
-  const int n = M->n;
-  const int *stf = M->start[PH_FINE], *ste = M->start[PH_IEVAL];
-  const long long F = stf[n], E = ste[n], K = F + E;
-  int sf = 0, se = 0;
-  for (long long w = blockIdx.x; w < K; w += gridDim.x) {
-    const long long e = (w * E + K - 1) / K;  // the first evaluation slot at or after w
-    if (e < E && e * K / E == w) {
-      se = owner(ste, n, (int)e, se);
-      const Inst &I = M->inst[se];
-      const Dyn D = dyn[I.slot];
-      if (D.remaining > 0) eval_item<GR>(S, P, I, D, (int)e - ste[se], sub, tw);
-    } else {
-      const int f = (int)(w - ((w + 1) * E + K - 1) / K);  // w less the evaluation slots up to w
-      sf = owner(stf, n, f, sf);
-      const Inst &I = M->inst[sf];
-      const Dyn D = dyn[I.slot];
-      if (D.remaining > 0) fine_item<MODE>(I, D, f - stf[sf], state, sub);
-    }
-  }
-}
-
 // ------------------------------------------------------------------ injection
 __global__ void __launch_bounds__(kThreads) b_inject(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
   const int n = M->n;
@@ -923,7 +885,6 @@ int query_grids(int gr, Grids *g) {
   rc |= occupancy_grid(b_coarse, &g->coarse);
   rc |= occupancy_grid(b_fine<3>, &g->fine);
   rc |= occupancy_grid(b_icorner_all, &g->icorner, kCornerThreads);
-  rc |= occupancy_grid(b_fine_eval<3, 2>, &g->fine_eval);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
   else rc |= occupancy_grid(b_ieval<4>, &g->ieval);
@@ -945,21 +906,6 @@ static void launch_fine(const Mix *m, Dyn *dyn, DevState *state, int mode, int s
     DNS_BFINE(3)
   }
 #undef DNS_BFINE
-}
-
-static void launch_fine_eval(const Mix *m, Dyn *dyn, DevState *state, int mode, int sub, TimeW tw, const Grids &g,
-                             cudaStream_t s) {
-#define DNS_BFE(M)                                                                \
-  case M:                                                                         \
-    b_fine_eval<M, 2><<<g.fine_eval, kThreads, 0, s>>>(m, dyn, state, sub, tw);  \
-    break;
-  switch (mode) {
-    DNS_BFE(0)
-    DNS_BFE(1)
-    DNS_BFE(2)
-    DNS_BFE(3)
-  }
-#undef DNS_BFE
 }
 
 static TimeW time_weights(int sub, int gr) {
@@ -984,24 +930,6 @@ static void launch_eval(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g,
 // eval(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] eval(sub), [9] inject.
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
                  cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats) {
-  if (DNS_FUSE_EVAL && gr == 2) {
-    // one stream: stats, sfinal, coarse, corners, (fine + evaluation) per
-    // substep, inject, final
-    if (stats) {
-      b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
-      b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
-    }
-    b_coarse<<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
-    CornerTimes ct{};
-    ct.gr = gr;
-    for (int t = 0; t < gr; t++) ct.w[t] = time_weights(t + 1, gr);
-    b_icorner_all<<<g.icorner, kCornerThreads, 0, s>>>(m, dyn, ct);
-    for (int sub = 1; sub <= gr; sub++)
-      launch_fine_eval(m, dyn, state, (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0), sub, time_weights(sub, gr), g, s);
-    b_inject<<<g.inject, kThreads, 0, s>>>(m, dyn);
-    b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log, count);
-    return;
-  }
   cudaEventRecord(ev[0], s);
   cudaStreamWaitEvent(aux, ev[0], 0);
   if (stats) {

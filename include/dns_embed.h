@@ -291,9 +291,12 @@ int dns_batch_footprint(const dns_params *p, long long *bytes);
 int dns_batch_tile_for(const dns_batch *b, const dns_params *p, dns_tile *t);
 /* Tuning-table entry for every later instance of the same grid shape. */
 int dns_batch_set_tile(dns_batch *b, const dns_params *shape, const dns_tile *t);
-/* Time `steps` steps of each candidate tile shape on a throw-away instance of
-   this grid shape (in a scratch batch; resident instances are untouched) and
-   store the fastest in the tuning table.  best and ms (per step) may be NULL. */
+/* Time `steps` steps of each candidate tile shape on throw-away instances of
+   this grid shape in a scratch batch (resident instances are untouched): as
+   many copies as make about 32 M node updates a step, at most 64 and 8 GB, so
+   that the GPU is as loaded as in a full batch.  The fastest goes to the
+   tuning table; a candidate replaces the current best only when at least 1%
+   faster.  best and ms (per step of all the copies) may be NULL. */
 int dns_batch_autotune(dns_batch *b, const dns_params *shape, int steps, dns_tile *best, double *ms);
 /* Add a seeded instance (the state dns_init_seeded builds) with a budget of
    `steps` coarse steps; statistics are sampled every sample_every steps of the
