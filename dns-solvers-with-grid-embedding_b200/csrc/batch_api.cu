@@ -66,15 +66,23 @@ bool tile_ok(const dns_tile &t) {
   return width_ok(t.cw) && width_ok(t.fw) && t.cjb >= 1 && t.cjb <= 64 && t.fjb >= 1 && t.fjb <= 64;
 }
 
+// Row iterations per work item (each iteration: 128 / W rows of 4 W nodes).
+// Coarse 4 (2048 nodes an item on a 256-node row); fine 2: the tuner's choice
+// for c2 (1.8% faster than 4: 4096 fine items fill 6.9 waves of the 592
+// resident blocks where 2048 fill 3.5, so less of the last wave idles) and
+// within noise of 4 on mixed batches.
+#ifndef DNS_DEFAULT_CJB
+#define DNS_DEFAULT_CJB 4
+#endif
+#ifndef DNS_DEFAULT_FJB
+#define DNS_DEFAULT_FJB 2
+#endif
 dns_tile default_tile(const dns_geometry &g) {
   dns_tile t;
-  // four row iterations per work item: on B200 the persistent loop's per-item
-  // set-up and block reduction are amortised over 512 nodes (measured: 4
-  // beats 2 by 4% and is within noise of 8 and 16 on mixed batches)
   t.cw = pick_width(g.nx / 4);
-  t.cjb = 4;
+  t.cjb = DNS_DEFAULT_CJB;
   t.fw = pick_width(g.nxf / 4);
-  t.fjb = 4;
+  t.fjb = DNS_DEFAULT_FJB;
   return t;
 }
 
