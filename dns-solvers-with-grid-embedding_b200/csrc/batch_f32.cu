@@ -208,18 +208,11 @@ __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
 // transfer); wall-adjacent planes send their five wall-bound populations
 // through the bounce-back / specular rule.  MODE bits as the single-channel
 // form: 1 flow-rate partials (last substep), 2 wall-shear sums (first).
-// rev: bulk planes in the opposite order.  Even substeps take them reversed,
-// so that they start on the planes the previous substep wrote last, which the
-// 126 MB L2 still holds (the interface kernels between the two touch little).
-#ifndef DNS_FINE_REVERSE
-#define DNS_FINE_REVERSE 1
-#endif
-__device__ __forceinline__ int fine_plane(int q, int zds, bool rev) {
+__device__ __forceinline__ int fine_plane(int q, int zds) {
   if (q == 0) return 0;
   if (q == 1) return 2 * zds - 1;
   if (q < 6) return zds - 2 + (q - 2);
-  int b = q - 6;
-  if (rev) b = 2 * zds - 7 - b;
+  const int b = q - 6;
   return b < zds - 3 ? b + 1 : zds + 2 + (b - (zds - 3));
 }
 
@@ -232,7 +225,7 @@ __device__ __forceinline__ void fine_item(const Inst &I, const Dyn &D, int local
     const int gxy = I.fgx * I.fgy;
     const int qp = local / gxy, rem = local - qp * gxy, by = rem / I.fgx, bx = rem - by * I.fgx;
     const int zds = I.zds, zdf = I.zdf, gr = I.gr, nx = I.nxf, ny = I.nyf;
-    const int p = fine_plane(qp, zds, DNS_FINE_REVERSE && (sub & 1) == 0);
+    const int p = fine_plane(qp, zds);
     const bool upper = p >= zds;
     const int k = upper ? p - zds : p + 1;
     const int lw = log2i(I.fw), tx = threadIdx.x & (I.fw - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;

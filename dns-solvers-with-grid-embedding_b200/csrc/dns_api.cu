@@ -1058,17 +1058,13 @@ static void L_extract(dns_handle *h, int cbuf, int slot, cudaStream_t st) {
   else
     launch_extract_f64(h->fc[cbuf], h->hist + slot * hslot_elems(h), h->d, h->shape, st);
 }
-#ifndef DNS_FINE_REVERSE
-#define DNS_FINE_REVERSE 1
-#endif
-static void L_fine(dns_handle *h, int src, int dst, int it, bool stats, cudaStream_t st) {
-  const bool first = it == 1, last = it == h->d.gr;
+static void L_fine(dns_handle *h, int src, int dst, bool first, bool last, bool stats, cudaStream_t st) {
   if (is_f32(h))
     launch_fine_f32(F(h->ff[src]), F(h->ff[dst]), h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials,
                     h->pl, first, last, stats, st);
   else
     launch_fine_f64(h->ff[src], h->ff[dst], h->wflag, h->d, h->shape, h->g.omega_f, h->state, h->partials, h->pl,
-                    first, last, stats, DNS_FINE_REVERSE && it % 2 == 0, st);
+                    first, last, stats, st);
 }
 static void L_iface(dns_handle *h, int fbuf, int it, cudaStream_t st) {
   const size_t hs = hslot_elems(h);
@@ -1228,7 +1224,7 @@ static void issue_step_overlapped(dns_handle *h, DevLog *log_row, bool sample) {
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - cur;
     if (it > 1) cudaStreamWaitEvent(T, h->ev_if[it - 2], 0);
-    L_fine(h, cur, nf, it, sample && it == 1, T);
+    L_fine(h, cur, nf, it == 1, it == d.gr, sample && it == 1, T);
     cudaEventRecord(h->ev_fine[it - 1], T);
     if (it > 1) cudaStreamWaitEvent(S, h->ev_fine[it - 2], 0);
     L_iface(h, nf, it, S);
@@ -1258,7 +1254,7 @@ static void issue_step(dns_handle *h, DevLog *log_row, bool sample) {
   PROFILED(h, 1, L_extract(h, nc, h->hn, h->stream));
   for (int it = 1; it <= d.gr; it++) {
     const int nf = 1 - h->cur_f;
-    PROFILED(h, 2, L_fine(h, h->cur_f, nf, it, sample && it == 1, h->stream));
+    PROFILED(h, 2, L_fine(h, h->cur_f, nf, it == 1, it == d.gr, sample && it == 1, h->stream));
     PROFILED(h, 3, L_iface(h, nf, it, h->stream));
     h->cur_f = nf;
   }

@@ -87,11 +87,9 @@ void launch_coarse_f64(const double *src, double *dst, const Dims &d, const Laun
                        cudaStream_t stream);
 void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const LaunchShape &s,
                         cudaStream_t stream);
-// rev: planes in reverse dispatch order (even substeps: L2 reuse of the odd
-// substep's last planes)
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
-                     bool last, bool stats, bool rev, cudaStream_t stream);
+                     bool last, bool stats, cudaStream_t stream);
 // two launches: macroscopic fields into mac[2 walls][4][nyf][nxf], then one
 // block per (tile, wall, population) into the interface planes of fdst
 void launch_interface_f64(const double *hn, const double *hp, const double *hpp, double *mac, double *fdst,

@@ -186,15 +186,11 @@ template <int MODE>
 __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const double *__restrict__ src, double *__restrict__ dst,
                                                           const int8_t *__restrict__ wf, Dims d, int jb, double om,
                                                           const DevState *st, double *__restrict__ part,
-                                                          double *__restrict__ wpart, double *__restrict__ spart,
-                                                          int rev) {
+                                                          double *__restrict__ wpart, double *__restrict__ spart) {
   const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
   const int P = 2 * zds;
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  // rev: planes in the opposite order of the blocks' dispatch, so that an
-  // even substep starts on the planes the odd one wrote last, which the L2
-  // still holds (partials stay indexed by plane: same sums, same order)
-  const int p = rev ? P - 1 - (int)blockIdx.z : (int)blockIdx.z;
+  const int p = blockIdx.z;
   const bool upper = p >= zds;
   const int k = upper ? p - zds : p + 1;  // reference k inside the block
   const int kwall = upper ? zdf - 1 : 0;
@@ -269,7 +265,7 @@ __global__ void __launch_bounds__(kMaxThreads, DNS_MINB_FINE) fine_kernel(const 
       }
     }
   }
-  const size_t blk = ((size_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  const size_t blk = ((size_t)blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce<2>(acc, part + blk * 2);
   if ((MODE & 2) && wall_sum_plane) block_reduce<2>(wacc, wpart + blk * 2);
   if (MODE & 4) block_reduce_stat(sacc, spart + blk * kStatPart);
@@ -1007,12 +1003,12 @@ void launch_extract_f64(const double *fc, double *hist_n, const Dims &d, const L
 
 void launch_fine_f64(const double *src, double *dst, const int8_t *wflag, const Dims &d, const LaunchShape &s,
                      double om, const DevState *st, double *partials, const PartialLayout &pl, bool first,
-                     bool last, bool stats, bool rev, cudaStream_t stream) {
+                     bool last, bool stats, cudaStream_t stream) {
   dim3 grid(s.fgx, s.fgy, 2 * d.zds), block(s.bx);
   const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
   double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
 #define FINE_CASE(M) \
-  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps, rev ? 1 : 0); break;
+  case M: fine_kernel<M><<<grid, block, 0, stream>>>(src, dst, wflag, d, s.jb, om, st, pf, pw, ps); break;
   switch (mode) {
     FINE_CASE(0) FINE_CASE(1) FINE_CASE(2) FINE_CASE(3) FINE_CASE(4) FINE_CASE(5) FINE_CASE(6) FINE_CASE(7)
   }
