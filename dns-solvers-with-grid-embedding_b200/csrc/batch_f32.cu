@@ -745,7 +745,7 @@ constexpr int kFinComp = 18;
 __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, Dyn *__restrict__ dyn,
                                                    DevState *__restrict__ state, DevLog *__restrict__ log,
                                                    unsigned int *__restrict__ count) {
-  __shared__ double sh[kFinComp][kThreads];
+  __shared__ double sh[kFinComp][kThreads / 32 > kFinChunks ? kThreads / 32 : kFinChunks];
   __shared__ bool last;
   const int n = M->n;
   const int *st = M->start[PH_FINAL];
@@ -760,35 +760,54 @@ __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, D
       continue;
     }
     const int c = w - st[s];
+    // the nine partial regions (coarse, fine, injection, six wall planes) as
+    // one run of (U, D) pairs; chunk c takes a fixed slice of it, so that a
+    // thread's loads are issued together whatever region they fall in
+    const int zds = I.zds, zdf = I.zdf;
+    const long nc = (long)I.nzc * I.cgy * I.cgx, nf = (long)2 * I.zds * I.fgy * I.fgx;
+    const long ni = (long)2 * I.ny * I.egx, wn = (long)I.fgy * I.fgx;
+    const int planes[6] = {0, 1, 2, zds + zdf - 2, zds + zdf - 3, zds + zdf - 4};
+    long long base[9];
+    long cnt[9];
+    base[0] = I.pc, cnt[0] = nc;
+    base[1] = I.pf, cnt[1] = nf;
+    base[2] = I.pi, cnt[2] = ni;
+#pragma unroll
+    for (int q = 0; q < 6; q++) base[3 + q] = I.pw + (long long)planes[q] * wn * 2, cnt[3 + q] = wn;
+    const long T = nc + nf + ni + 6 * wn;
+    const long lo = T * c / kFinChunks, hi = T * (c + 1) / kFinChunks;
     double v[kFinComp];
 #pragma unroll
     for (int q = 0; q < kFinComp; q++) v[q] = 0.;
-    const long nc = (long)I.nzc * I.cgy * I.cgx, nf = (long)2 * I.zds * I.fgy * I.fgx;
-    const long ni = (long)2 * I.ny * I.egx, wn = (long)I.fgy * I.fgx;
     const double *P = I.part;
-    auto chunk = [&](long long off, long cnt, int q0) {
-      const long lo = cnt * c / kFinChunks, hi = cnt * (c + 1) / kFinChunks;
-      for (long q = lo + threadIdx.x; q < hi; q += kThreads) {
-        v[q0] += P[off + q * 2];
-        v[q0 + 1] += P[off + q * 2 + 1];
-      }
-    };
-    chunk(I.pc, nc, 0);
-    chunk(I.pf, nf, 2);
-    chunk(I.pi, ni, 4);
-    const int zds = I.zds, zdf = I.zdf;
-    const int planes[6] = {0, 1, 2, zds + zdf - 2, zds + zdf - 3, zds + zdf - 4};
+    for (long q = lo + threadIdx.x; q < hi; q += kThreads) {
+      long r0 = q;
+      int rr = 0;
+      while (rr < 8 && r0 >= cnt[rr]) r0 -= cnt[rr++];
+      const double u = P[base[rr] + r0 * 2], d = P[base[rr] + r0 * 2 + 1];
 #pragma unroll
-    for (int q = 0; q < 6; q++) chunk(I.pw + (long long)planes[q] * wn * 2, wn, 6 + 2 * q);
-#pragma unroll
-    for (int q = 0; q < kFinComp; q++) sh[q][threadIdx.x] = v[q];
-    __syncthreads();
-    for (int o = kThreads / 2; o > 0; o >>= 1) {
-      if (threadIdx.x < o)
-#pragma unroll
-        for (int q = 0; q < kFinComp; q++) sh[q][threadIdx.x] += sh[q][threadIdx.x + o];
-      __syncthreads();
+      for (int r = 0; r < 9; r++)
+        if (r == rr) {
+          v[2 * r] += u;
+          v[2 * r + 1] += d;
+        }
     }
+    // warp sums, then the warps' sums in warp order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int q = 0; q < kFinComp; q++) {
+      double x = v[q];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (lane == 0) sh[q][warp] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < kFinComp) {
+      double a = 0.;
+      for (int q = 0; q < kThreads / 32; q++) a += sh[threadIdx.x][q];
+      sh[threadIdx.x][0] = a;
+    }
+    __syncthreads();
     double *l2 = I.part + I.pl2;
     if (threadIdx.x == 0) {
       for (int q = 0; q < kFinComp; q++) l2[c * kFinComp + q] = sh[q][0];
@@ -798,18 +817,16 @@ __global__ void __launch_bounds__(kThreads) b_final(const Mix *__restrict__ M, D
     __syncthreads();
     if (last) {
       __threadfence();
-      // the chunk rows are loaded by the whole block at once (into the free
-      // reduction buffer), then summed in chunk order by one thread each
-      static_assert(kFinChunks * kFinComp <= kFinComp * kThreads, "staging fits");
-      double *flat = &sh[0][0];
+      // the chunk rows are loaded by the whole block at once, then summed in
+      // chunk order by one thread each
       {
         const volatile double *L = l2;
-        for (int q = threadIdx.x; q < kFinChunks * kFinComp; q += kThreads) flat[q] = L[q];
+        for (int q = threadIdx.x; q < kFinChunks * kFinComp; q += kThreads) sh[q % kFinComp][q / kFinComp] = L[q];
       }
       __syncthreads();
       double a = 0.;
       if (threadIdx.x < kFinComp)
-        for (int q = 0; q < kFinChunks; q++) a += flat[q * kFinComp + threadIdx.x];
+        for (int q = 0; q < kFinChunks; q++) a += sh[threadIdx.x][q];
       __syncthreads();
       if (threadIdx.x < kFinComp) sh[threadIdx.x][0] = a;
       __syncthreads();
