@@ -49,22 +49,12 @@ __device__ __forceinline__ QuadPos quad_pos(int tx, int W, int gx0, int nx, bool
   return q;
 }
 
-// Cache hints of the streamed population arrays (each value is read once
-// and written once per substep): DNS_F32_LOAD_HINT 1 loads with evict-first
-// (ld.global.cs), DNS_F32_STORE_HINT 1 stores with evict-first (st.global.cs).
-#ifndef DNS_F32_LOAD_HINT
-#define DNS_F32_LOAD_HINT 0
-#endif
-#ifndef DNS_F32_STORE_HINT
-#define DNS_F32_STORE_HINT 0
-#endif
 __device__ __forceinline__ void quad_load(const float *__restrict__ src, size_t idx0, size_t pstride, bool ok,
                                           float (&q)[19][4]) {
 #pragma unroll
   for (int a = 0; a < 19; a++) {
     float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 *pa = reinterpret_cast<const float4 *>(src + (size_t)a * pstride + idx0);
-    if (ok) v = DNS_F32_LOAD_HINT ? __ldcs(pa) : __ldg(pa);
+    if (ok) v = __ldg(reinterpret_cast<const float4 *>(src + (size_t)a * pstride + idx0));
     q[a][0] = v.x;
     q[a][1] = v.y;
     q[a][2] = v.z;
@@ -115,10 +105,7 @@ __device__ __forceinline__ void quad_collide(float (&q)[19][4], float om, float 
 }
 
 __device__ __forceinline__ void st4(float *p, float a, float b, float c, float d) {
-  if (DNS_F32_STORE_HINT)
-    __stcs(reinterpret_cast<float4 *>(p), make_float4(a, b, c, d));
-  else
-    *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
+  *reinterpret_cast<float4 *>(p) = make_float4(a, b, c, d);
 }
 
 // Store population a's four post-collision values, pushed by e_x(a) along
