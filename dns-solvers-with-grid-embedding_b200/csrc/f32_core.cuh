@@ -607,12 +607,133 @@ __device__ __forceinline__ void if_column32(const float4 (&C)[IfTile<GR>::TY + 1
   }
 }
 
+// GR = 2, both fine columns of cell column cx (sub-positions 0 and 1) at
+// sub-row JJ of the NR cell rows cy0, cy0 + 2, ...: v[r][0] / v[r][1] (the
+// arithmetic of if_col2 for II = 0 and II = 1).
+#ifndef DNS_EVAL_PAIRS
+#define DNS_EVAL_PAIRS 1
+#endif
+template <int JJ, int NR, int CH, int CW>
+__device__ __forceinline__ void if_pair2(const float4 (&C)[CH][CW], int cx, int cy0, float (&v)[NR][2]) {
+  auto xpass = [&](int r, float &p0, float &q0, float &p1, float &q1) {
+    const float4 c0 = C[r][cx], c1 = C[r][cx + 1];
+    p0 = c0.x;
+    q0 = c0.z;
+    p1 = 0.5f * (c0.x + c1.x) + 0.125f * (c0.y - c1.y);
+    q1 = 0.5f * (c0.z + c1.z) + 0.125f * (c0.w - c1.w);
+  };
+#pragma unroll
+  for (int r = 0; r < NR; r++) {
+    const int cy = cy0 + 2 * r;
+    float pa0, qa0, pa1, qa1;
+    xpass(cy, pa0, qa0, pa1, qa1);
+    if (JJ == 0) {
+      v[r][0] = pa0;
+      v[r][1] = pa1;
+    } else {
+      float pb0, qb0, pb1, qb1;
+      xpass(cy + 1, pb0, qb0, pb1, qb1);
+      v[r][0] = 0.5f * (pa0 + pb0) + 0.125f * (qa0 - qb0);
+      v[r][1] = 0.5f * (pa1 + pb1) + 0.125f * (qa1 - qb1);
+    }
+  }
+}
+
+// GR = 2 form of iface_eval_tile32: a thread takes both fine columns of one
+// cell column and the fine rows w, w + 4, ... of its warp w, so that a warp
+// stores 32 consecutive column pairs (256 contiguous bytes) per row.
+__device__ __forceinline__ void iface_eval_tile32_gr2(IfEvalSmem<2> &S, const IfParams32 &P, int tx, int ty, int w,
+                                                      int a0, int a1) {
+  constexpr int TX = IfTile<2>::TX, TY = IfTile<2>::TY, NR = TY / 2;  // rows per thread
+  constexpr int CW = TX + 1, CH = TY + 1, NC = CW * CH, NCS = (NC + kThreads - 1) / kThreads;
+  static_assert(kThreads == 128 && TX == 32, "four warps of 32 cell columns");
+  const int i0 = tx * TX, j0 = ty * TY;
+  const int t = threadIdx.x, cx = t & 31, wp = t >> 5;
+  const int jj = wp & 1, cy0 = wp >> 1;  // fine rows 2 (cy0 + 2 r) + jj
+  const bool colok = i0 + cx < P.nx;
+  const size_t plane = (size_t)P.ny * P.nx;
+  int goff[NCS];
+#pragma unroll
+  for (int s = 0; s < NCS; s++) {
+    const int c = t + s * kThreads;
+    goff[s] = c < NC ? wrapf(j0 + c / CW, P.ny) * P.nx + wrapf(i0 + c % CW, P.nx) : -1;
+  }
+  const int nf = 4 + (a1 - a0);
+  auto issue = [&](int k) {
+    if (k < nf) {
+      const int f = k < 4 ? k : 4 + a0 + (k - 4);
+      const float4 *src = P.corner + ((size_t)w * 23 + f) * plane;
+      float4 *dst = &S.C[k % kEvalStages][0][0];
+#pragma unroll
+      for (int s = 0; s < NCS; s++)
+        if (goff[s] >= 0) cp_async16(dst + t + s * kThreads, src + goff[s]);
+    }
+    cp_async_commit();
+  };
+  auto column = [&](int k, float (&v)[NR][2]) {
+    if (jj == 0)
+      if_pair2<0, NR, CH, CW>(S.C[k % kEvalStages], cx, cy0, v);
+    else
+      if_pair2<1, NR, CH, CW>(S.C[k % kEvalStages], cx, cy0, v);
+  };
+#pragma unroll
+  for (int k = 0; k < kEvalStages - 1; k++) issue(k);
+  float mac[4][NR][2];
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    cp_async_wait<kEvalStages - 2>();
+    __syncthreads();
+    issue(k + kEvalStages - 1);
+    column(k, mac[k]);
+  }
+  float usq[NR][2];
+#pragma unroll
+  for (int r = 0; r < NR; r++)
+#pragma unroll
+    for (int h = 0; h < 2; h++)
+      usq[r][h] = mac[1][r][h] * mac[1][r][h] + mac[2][r][h] * mac[2][r][h] + mac[3][r][h] * mac[3][r][h];
+  const size_t fplane = (size_t)P.nyf * P.nxf, fstride = (size_t)2 * P.zds * fplane;
+  const int pf = w == 0 ? P.zds - 1 : P.zds;
+  float *out = P.fdst + (size_t)pf * fplane;
+  for (int k = 4; k < nf; k++) {
+    cp_async_wait<kEvalStages - 2>();
+    __syncthreads();
+    issue(k + kEvalStages - 1);
+    const int a = a0 + (k - 4);
+    float fv[NR][2];
+    column(k, fv);
+    const float ex = c_pop[a][0], ey = c_pop[a][1], ez = c_pop[a][2], wa = c_pop[a][3];
+    float *oa = out + (size_t)a * fstride;
+#pragma unroll
+    for (int r = 0; r < NR; r++) {
+      const int cy = cy0 + 2 * r;
+      if (colok && j0 + cy < P.ny) {
+        float o[2];
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const float dr = mac[0][r][h], eu = ex * mac[1][r][h] + ey * mac[2][r][h] + ez * mac[3][r][h];
+          const float deq = wa * (dr + (1.f + dr) * (3.f * eu + 4.5f * eu * eu - 1.5f * usq[r][h]));
+          o[h] = deq + P.fac * fv[r][h];
+        }
+        *reinterpret_cast<float2 *>(oa + (size_t)((j0 + cy) * 2 + jj) * P.nxf + (i0 + cx) * 2) =
+            make_float2(o[0], o[1]);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // the ring may be reused by the next item
+}
+
 // One (tile, wall) and populations [a0, a1) (the macroscopic fields always):
 // the corner tiles of successive fields stream into shared memory through a
 // cp.async ring while earlier ones are evaluated.  blockDim.x == kThreads.
 template <int GR>
 __device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfParams32 &P, int tx, int ty, int w,
                                                   int a0, int a1) {
+  if constexpr (GR == 2 && DNS_EVAL_PAIRS) {
+    iface_eval_tile32_gr2(S, P, tx, ty, w, a0, a1);
+    return;
+  }
   constexpr int TX = IfTile<GR>::TX, TY = IfTile<GR>::TY, NR = GR * TY / 2;
   constexpr int CW = TX + 1, CH = TY + 1, NC = CW * CH, NCS = (NC + kThreads - 1) / kThreads;
   const int i0 = tx * TX, j0 = ty * TY;
