@@ -601,7 +601,10 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
 #if !DNS_CORNER_PHASED
 constexpr int kCornerThreads = kThreads;
 #endif
-__global__ void __launch_bounds__(kCornerThreads) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
+#ifndef DNS_CORNER_MINB
+#define DNS_CORNER_MINB 1
+#endif
+__global__ void __launch_bounds__(kCornerThreads, DNS_CORNER_MINB) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
                                                           CornerTimes ct) {
   __shared__ CornerAllSmem C;
   const int n = M->n;

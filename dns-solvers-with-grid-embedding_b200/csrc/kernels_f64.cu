@@ -412,11 +412,19 @@ __global__ void __launch_bounds__(TPX *TPY) interface_macro_kernel(const double 
     if (ic < nx && jc < ny) {
       double cf[16];
       iface_coeffs(S, cx, cy, cf);
+      if constexpr (GR == 2) {
+        // both fine columns of the cell in one 16-byte store
 #pragma unroll
-      for (int ii = 0; ii < GR; ii++)
+        for (int jj = 0; jj < 2; jj++)
+          *reinterpret_cast<double2 *>(o + (size_t)(jc * 2 + jj) * nxf + ic * 2) =
+              make_double2(iface_eval<2>(cf, 0, jj), iface_eval<2>(cf, 1, jj));
+      } else {
 #pragma unroll
-        for (int jj = 0; jj < GR; jj++)
-          o[(size_t)(jc * GR + jj) * nxf + ic * GR + ii] = iface_eval<GR>(cf, ii, jj);
+        for (int ii = 0; ii < GR; ii++)
+#pragma unroll
+          for (int jj = 0; jj < GR; jj++)
+            o[(size_t)(jc * GR + jj) * nxf + ic * GR + ii] = iface_eval<GR>(cf, ii, jj);
+      }
     }
   }
 }
@@ -450,17 +458,40 @@ __global__ void __launch_bounds__(TPX *TPY) interface_pop_kernel(const double *_
     if (ic < nx && jc < ny) {
       double cf[16];
       iface_coeffs(S, cx, cy, cf);
+      if constexpr (GR == 2) {
+        // both fine columns of the cell: 16-byte loads of the fields and one
+        // 16-byte store (the same arithmetic per node)
 #pragma unroll
-      for (int ii = 0; ii < GR; ii++)
+        for (int jj = 0; jj < 2; jj++) {
+          const size_t q0 = (size_t)(jc * 2 + jj) * nxf + ic * 2;
+          const double2 r2 = *reinterpret_cast<const double2 *>(m + q0);
+          const double2 x2 = *reinterpret_cast<const double2 *>(m + fplane + q0);
+          const double2 y2 = *reinterpret_cast<const double2 *>(m + 2 * fplane + q0);
+          const double2 z2 = *reinterpret_cast<const double2 *>(m + 3 * fplane + q0);
+          double o2[2];
 #pragma unroll
-        for (int jj = 0; jj < GR; jj++) {
-          const size_t qn = (size_t)(jc * GR + jj) * nxf + ic * GR + ii;
-          const double rho = m[qn], u0 = m[fplane + qn], u1 = m[2 * fplane + qn], u2 = m[3 * fplane + qn];
-          const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
-          const double val = iface_eval<GR>(cf, ii, jj);
-          const double feq = feq_f64(wa * rho, proj_f64(a, u0, u1, u2), t15v);
-          out[qn] = feq + ia.fac * val;
+          for (int ii = 0; ii < 2; ii++) {
+            const double rho = ii ? r2.y : r2.x, u0 = ii ? x2.y : x2.x, u1 = ii ? y2.y : y2.x, u2 = ii ? z2.y : z2.x;
+            const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+            const double val = iface_eval<2>(cf, ii, jj);
+            const double feq = feq_f64(wa * rho, proj_f64(a, u0, u1, u2), t15v);
+            o2[ii] = feq + ia.fac * val;
+          }
+          *reinterpret_cast<double2 *>(out + q0) = make_double2(o2[0], o2[1]);
         }
+      } else {
+#pragma unroll
+        for (int ii = 0; ii < GR; ii++)
+#pragma unroll
+          for (int jj = 0; jj < GR; jj++) {
+            const size_t qn = (size_t)(jc * GR + jj) * nxf + ic * GR + ii;
+            const double rho = m[qn], u0 = m[fplane + qn], u1 = m[2 * fplane + qn], u2 = m[3 * fplane + qn];
+            const double t15v = 1.5 * (u0 * u0 + u1 * u1 + u2 * u2);
+            const double val = iface_eval<GR>(cf, ii, jj);
+            const double feq = feq_f64(wa * rho, proj_f64(a, u0, u1, u2), t15v);
+            out[qn] = feq + ia.fac * val;
+          }
+      }
     }
   }
 }
