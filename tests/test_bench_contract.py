@@ -34,6 +34,15 @@ def test_reference_arm_prints_the_contract_line():
     cb = d["cpu_baseline"]
     assert cb["kind"] == "reference" and cb["cores"] >= 1 and cb["value"] == d["value"] and cb["sample"]
     assert d["e2e"] == {"value": d["value"], "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
+    # the same workload description as the main line, and the step counts it ran
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_mod", ROOT / "bench.py")
+    bench = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(bench)
+    args = type("A", (), {"config": "c1"})()
+    assert d["config"] == bench.arm_config(args, 1)
+    assert d["steps"] == 1 and d["warmup"] == 3  # W is raised to the contract's minimum of 3
+    assert "after 3 untimed" in cb["sample"]
 
 
 def test_reference_arm_runs_on_rank_zero_only():
