@@ -601,8 +601,10 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
 #if !DNS_CORNER_PHASED
 constexpr int kCornerThreads = kThreads;
 #endif
+// resident blocks of b_icorner_all per SM: 4 caps it at 64 registers (no
+// spills), 592 blocks for c2's 768 items where 80 registers gave 444
 #ifndef DNS_CORNER_MINB
-#define DNS_CORNER_MINB 1
+#define DNS_CORNER_MINB 4
 #endif
 __global__ void __launch_bounds__(kCornerThreads, DNS_CORNER_MINB) b_icorner_all(const Mix *__restrict__ M, const Dyn *__restrict__ dyn,
                                                           CornerTimes ct) {
