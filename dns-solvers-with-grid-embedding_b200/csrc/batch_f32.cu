@@ -656,8 +656,11 @@ __device__ __forceinline__ void eval_item(IfEvalSmem<GR> &S, IfParams32 &P, cons
   iface_eval_tile32<GR>(S, P, tx, ty, wall, 19 * g / kEvalPopGroups, 19 * (g + 1) / kEvalPopGroups);
 }
 
+#ifndef DNS_EVAL_MINB
+#define DNS_EVAL_MINB 1
+#endif
 template <int GR>
-__global__ void __launch_bounds__(kThreads) b_ieval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
+__global__ void __launch_bounds__(kThreads, DNS_EVAL_MINB) b_ieval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,
                                                     TimeW tw) {
   __shared__ IfEvalSmem<GR> S;
   __shared__ IfParams32 P;
