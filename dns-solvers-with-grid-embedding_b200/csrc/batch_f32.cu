@@ -657,7 +657,7 @@ __device__ __forceinline__ void eval_item(IfEvalSmem<GR> &S, IfParams32 &P, cons
 }
 
 #ifndef DNS_EVAL_MINB
-#define DNS_EVAL_MINB 1
+#define DNS_EVAL_MINB 5
 #endif
 template <int GR>
 __global__ void __launch_bounds__(kThreads, DNS_EVAL_MINB) b_ieval(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, int sub,

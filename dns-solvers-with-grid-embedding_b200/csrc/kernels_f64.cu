@@ -738,19 +738,26 @@ __global__ void __launch_bounds__(kFin2Threads) finalize2_kernel(DevState *st, D
   double v[kFin2Comp];
 #pragma unroll
   for (int c = 0; c < kFin2Comp; c++) v[c] = 0.;
-  // this block's fixed chunk of every region; each thread strides through it
-  auto acc = [&](const double *p, long n, int c0) {
-    const long lo = n * b / nb, hi = n * (b + 1) / nb;
-    for (long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
-      v[c0] += p[q * 2];
-      v[c0 + 1] += p[q * 2 + 1];
-    }
-  };
-  acc(part_c, a.nc, 0);
-  acc(part_f, a.nf, 2);
-  acc(part_i, a.ni, 4);
+  // the nine regions (coarse, fine, injection, six wall planes) as one run of
+  // (U, D) pairs; this block takes a fixed slice of it, so that a thread's
+  // loads are issued together whatever region they fall in
+  const double *base[9] = {part_c, part_f, part_i, part_w + a.wb[0] * 2, part_w + a.wb[1] * 2,
+                           part_w + a.wb[2] * 2, part_w + a.wb[3] * 2, part_w + a.wb[4] * 2, part_w + a.wb[5] * 2};
+  const long cnt[9] = {a.nc, a.nf, a.ni, a.wn, a.wn, a.wn, a.wn, a.wn, a.wn};
+  const long T = a.nc + a.nf + a.ni + 6 * a.wn;
+  const long lo = T * b / nb, hi = T * (b + 1) / nb;
+  for (long q = lo + threadIdx.x; q < hi; q += blockDim.x) {
+    long r0 = q;
+    int rr = 0;
+    while (rr < 8 && r0 >= cnt[rr]) r0 -= cnt[rr++];
+    const double u = base[rr][r0 * 2], dd = base[rr][r0 * 2 + 1];
 #pragma unroll
-  for (int q = 0; q < 6; q++) acc(part_w + a.wb[q] * 2, a.wn, 6 + 2 * q);
+    for (int r = 0; r < 9; r++)
+      if (r == rr) {
+        v[2 * r] += u;
+        v[2 * r + 1] += dd;
+      }
+  }
   block_reduce_n<kFin2Comp, kFin2Threads>(v, sh);
   if (threadIdx.x == 0) {
     for (int c = 0; c < kFin2Comp; c++) level2[b * kFin2Comp + c] = sh[c];
