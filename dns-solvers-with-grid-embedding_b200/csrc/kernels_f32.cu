@@ -5,6 +5,17 @@
 #include "f32_core.cuh"
 #include "kernels.h"
 #include "lattice.cuh"
+#include "quad_f32.cuh"
+
+// DNS_F32_QUAD_SINGLE 1: the single-channel stream-collide uses the
+// four-node kernels where the x extent allows (0: one node per thread).
+#ifndef DNS_F32_QUAD_SINGLE
+#define DNS_F32_QUAD_SINGLE 1
+#endif
+// rows per block of the four-node kernels: the scalar shape's jb
+#ifndef DNS_QUAD_JB
+#define DNS_QUAD_JB 2
+#endif
 
 namespace dns {
 
@@ -131,6 +142,155 @@ __global__ void __launch_bounds__(kThreads, KIND ? DNS_F32_BULK_MINB : 0) fine_f
     else
       fine_wall_f32<MODE, true>(fa, i, j, idx0, d, om, Gf, wf, dst, pstride, wz, wall_sum_plane, wall_rho_plane,
                                 acc, wacc, sacc);
+  }
+  const size_t blk = ((size_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  if (MODE & 1) block_reduce32<2>(acc, part + blk * 2);
+  if ((MODE & 2) && wall_sum_plane) block_reduce32<2>(wacc, wpart + blk * 2);
+  if (MODE & 4) block_reduce_stat(sacc, spart + blk * kStatPart);
+}
+
+// ------------------------------------------------------------------ four nodes per thread
+// The stream-collide of one channel with the batched engine's four-node
+// threads (quad_f32.cuh: 16-byte loads and stores, opposite populations
+// collided in pairs) over the scalar kernels' blocks: 32 x jb threads cover a
+// scalar block's 128 x jb nodes, so every partial sum lands at the same block
+// index and the finalize, statistics and flow-rate paths are unchanged.  Used
+// when the x extent is a multiple of 4 (rows start on 16-byte boundaries);
+// every plane class is one launch.
+constexpr int kQuadRow = 32;  // threads per row: 128 nodes
+
+template <bool STATS>
+__global__ void __launch_bounds__(kQuadRow * DNS_QUAD_JB, 512 / (kQuadRow * DNS_QUAD_JB))
+    coarse_quad_f32(const float *__restrict__ src, float *__restrict__ dst, Dims d, float om,
+                    const DevState *__restrict__ st, double *__restrict__ part, double *__restrict__ spart) {
+  const int nx = d.nx, ny = d.ny, nzc = d.nzc;
+  const int tx = threadIdx.x & (kQuadRow - 1), ty = threadIdx.x / kQuadRow;
+  const int k = blockIdx.z, jr = blockIdx.y * (blockDim.x / kQuadRow) + ty;
+  const bool row_ok = jr < ny;
+  const int j = row_ok ? jr : 0;
+  const size_t pstride = (size_t)nzc * ny * nx;
+  const float G = (float)st->force;
+  const float one[3] = {1.f, 1.f, 1.f};
+  const int plane = ny * nx;
+  double acc[2] = {0., 0.};
+  PlaneStat sacc;
+  sacc.init();
+  const QuadPos P = quad_pos(tx, kQuadRow, blockIdx.x * 4 * kQuadRow, nx, row_ok);
+  const long long rowoff = ((long long)k * ny + j) * nx;
+  float q[19][4];
+  quad_load(src, (size_t)(rowoff + P.x0), pstride, P.ok, q);
+  Mac32 m[4];
+  quad_collide(q, om, G, m);
+  if (STATS && P.ok)
+#pragma unroll
+    for (int c = 0; c < 4; c++) sacc.add(m[c].u0, m[c].u1, m[c].u2, 1.0 + (double)m[c].drho);
+  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+  if (k >= 2 && k <= nzc - 3) {
+    if (P.ok)
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        acc[0] += (double)(m[c].rho * m[c].u0 + m[c].rho * G);
+        acc[1] += (double)m[c].drho;
+      }
+    quad_push<0, 0, false>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+  } else if (k == 0) {
+    quad_push<-2, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+  } else if (k == 1) {
+    quad_push<-1, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+  } else if (k == nzc - 2) {
+    quad_push<1, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+  } else {
+    quad_push<2, 0, true>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, one, acc);
+  }
+  const size_t blk = ((size_t)k * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  block_reduce32<2>(acc, part + blk * 2);
+  if (STATS) block_reduce_stat(sacc, spart + blk * kStatPart);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(kQuadRow * DNS_QUAD_JB, 512 / (kQuadRow * DNS_QUAD_JB))
+    fine_quad_f32(const float *__restrict__ src, float *__restrict__ dst, const int8_t *__restrict__ wf, Dims d,
+                  float om, const DevState *__restrict__ st, double *__restrict__ part, double *__restrict__ wpart,
+                  double *__restrict__ spart) {
+  const int nx = d.nxf, ny = d.nyf, zdf = d.zdf, zds = d.zds, gr = d.gr;
+  const int tx = threadIdx.x & (kQuadRow - 1), ty = threadIdx.x / kQuadRow;
+  const int p = blockIdx.z, jr = blockIdx.y * (blockDim.x / kQuadRow) + ty;
+  const bool row_ok = jr < ny;
+  const int j = row_ok ? jr : 0;
+  const bool upper = p >= zds;
+  const int k = upper ? p - zds : p + 1;
+  const size_t pstride = (size_t)2 * zds * ny * nx;
+  const float Gf = (float)((1. / (double)gr) * st->force);
+  const bool wall_sum_plane =
+      upper ? (k == zdf - 2 || k == zdf - 3 || k == zdf - 4) : (k == 1 || k == 2 || k == 3);
+  const bool wall_rho_plane = upper ? (k == zdf - 4) : (k == 1);
+  const int cls = (!upper && k == 1) ? 1
+                  : (upper && k == zdf - 2) ? 2
+                  : (!upper && k == zdf - 2) ? 3
+                  : (!upper && k == zdf - 1) ? 4
+                  : (upper && k == 1) ? 5
+                  : (upper && k == 0) ? 6 : 0;
+  float wz[3];
+#pragma unroll
+  for (int c = 0; c < 3; c++) {
+    const int kd = k + c - 1;  // destination planes k - 1, k, k + 1 (encalc2.c:33-53, 86-107)
+    wz[c] = !upper ? ((kd >= 1 && kd < zdf - gr) ? 1.f : 0.f)
+                   : ((kd >= gr && kd < zdf - 1) ? (kd == gr ? 0.5f : 1.f) : 0.f);
+  }
+  const bool wuni = wz[0] == wz[1] && wz[1] == wz[2];
+  const int plane = ny * nx;
+  double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
+  PlaneStat sacc;
+  sacc.init();
+  const QuadPos P = quad_pos(tx, kQuadRow, blockIdx.x * 4 * kQuadRow, nx, row_ok);
+  const long long rowoff = ((long long)p * ny + j) * nx;
+  float q[19][4];
+  quad_load(src, (size_t)(rowoff + P.x0), pstride, P.ok, q);
+  Mac32 m[4];
+  quad_collide(q, om, Gf, m);
+  if (P.ok) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      if ((MODE & 2) && wall_sum_plane) wacc[0] += (double)m[c].u0;
+      if ((MODE & 2) && wall_rho_plane) wacc[1] += 1.0 + (double)m[c].drho;
+      if (MODE & 4) sacc.add(m[c].u0, m[c].u1, m[c].u2, 1.0 + (double)m[c].drho);
+    }
+  }
+  const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
+  switch (cls) {
+    case 0:
+      if ((MODE & 1) && wuni) {
+        if (P.ok)
+#pragma unroll
+          for (int c = 0; c < 4; c++) {
+            acc[0] += (double)(wz[1] * (m[c].rho * m[c].u0 + m[c].rho * Gf));
+            acc[1] += (double)(wz[1] * m[c].drho);
+          }
+        quad_push<0, 0, false>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      } else {
+        quad_push<0, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      }
+      break;
+    case 1:
+      quad_push<0, -1, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      quad_wall<false, (MODE & 1) != 0>(q, dst, pstride, rowoff, j, nx, ny, wf, P, wz[1], acc);
+      break;
+    case 2:
+      quad_push<0, 1, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      quad_wall<true, (MODE & 1) != 0>(q, dst, pstride, rowoff, j, nx, ny, wf, P, wz[1], acc);
+      break;
+    case 3:
+      quad_push<1, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      break;
+    case 4:
+      quad_push<2, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      break;
+    case 5:
+      quad_push<-1, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      break;
+    default:
+      quad_push<-2, 0, (MODE & 1) != 0>(q, dst, pstride, rowoff, plane, dym, dyp, P, nx, wz, acc);
+      break;
   }
   const size_t blk = ((size_t)p * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
   if (MODE & 1) block_reduce32<2>(acc, part + blk * 2);
@@ -398,12 +558,25 @@ __global__ void fields_f32_kernel(const float *__restrict__ soa, double *__restr
 }  // namespace
 
 // ====================================================================== host
+// the four-node kernels cover the scalar blocks exactly: 128 nodes of jb rows
+static bool quad_ok(const Dims &d, const LaunchShape &s) {
+  return DNS_F32_QUAD_SINGLE && d.nx % 4 == 0 && s.bx == 4 * kQuadRow && s.jb == DNS_QUAD_JB;
+}
+
 void launch_coarse_f32(const float *src, float *dst, const Dims &d, const LaunchShape &s, double om,
                        const DevState *st, double *partials, const PartialLayout &pl, bool stats,
                        cudaStream_t stream) {
   dim3 gb(s.cgx, s.cgy, d.nzc - 4), ge(s.cgx, s.cgy, 4), block(s.bx);
   double *pc = partials + pl.coarse, *ps = partials + pl.stats_c;
   const float omf = (float)om;
+  if (quad_ok(d, s)) {
+    dim3 g(s.cgx, s.cgy, d.nzc), b(kQuadRow * s.jb);
+    if (stats)
+      coarse_quad_f32<true><<<g, b, 0, stream>>>(src, dst, d, omf, st, pc, ps);
+    else
+      coarse_quad_f32<false><<<g, b, 0, stream>>>(src, dst, d, omf, st, pc, ps);
+    return;
+  }
   if (stats) {
     coarse_f32<true, true><<<gb, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 2);
     coarse_f32<true, false><<<ge, block, 0, stream>>>(src, dst, d, s.jb, omf, st, pc, ps, 0);
@@ -432,6 +605,16 @@ void launch_fine_f32(const float *src, float *dst, const int8_t *wflag, const Di
   const int mode = (last ? 1 : 0) | (first ? 2 : 0) | (stats ? 4 : 0);
   double *pf = partials + pl.fine, *pw = partials + pl.wall, *ps = partials + pl.stats_f;
   const float omf = (float)om;
+  if (quad_ok(d, s)) {
+    dim3 g(s.fgx, s.fgy, 2 * d.zds), b(kQuadRow * s.jb);
+#define FINEQ_CASE(M) \
+  case M: fine_quad_f32<M><<<g, b, 0, stream>>>(src, dst, wflag, d, omf, st, pf, pw, ps); break;
+    switch (mode) {
+      FINEQ_CASE(0) FINEQ_CASE(1) FINEQ_CASE(2) FINEQ_CASE(3) FINEQ_CASE(4) FINEQ_CASE(5) FINEQ_CASE(6) FINEQ_CASE(7)
+    }
+#undef FINEQ_CASE
+    return;
+  }
   dim3 gb(s.fgx, s.fgy, bulk.n), ge(s.fgx, s.fgy, edge.n), ga(s.fgx, s.fgy, adj.n), block(s.bx);
 #define FINE32_CASE(M)                                                                                       \
   case M:                                                                                                    \
