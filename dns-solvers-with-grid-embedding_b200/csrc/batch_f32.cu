@@ -37,10 +37,6 @@ __device__ __forceinline__ bool sampling(const Inst &I, const Dyn &D) {
   return D.remaining > 0 && I.sample_every > 0 && D.step % I.sample_every == 0;
 }
 
-__device__ __forceinline__ void stat_acc(const float (&f)[19], PlaneStat &sacc) {
-  const Mac32 m = macro_f32(f);
-  sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
-}
 
 // ------------------------------------------------------------------ statistics
 // The sampled state's plane sums are formed where the state is read anyway:
