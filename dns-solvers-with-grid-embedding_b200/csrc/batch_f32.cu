@@ -332,7 +332,10 @@ __device__ __forceinline__ void iface_params_of(IfParams32 &P, const Inst &I, co
 // t = 1..GR, the Hermite-in-time value (tinterpolate_hrmt.c), the fourth-order
 // derivatives (derivative.c) and the corner float4s of substep t's array.
 // Every substep's interface depends only on the three history levels, so the
-// whole step's corner data is made right after the coarse kernel.
+// whole step's corner data is made right after the coarse kernel.  Every
+// field of the item's group goes through each barrier phase together: per
+// substep the time combination, the y derivatives and the x derivatives with
+// the store, the derivative phases four-wide in shared memory.
 struct CornerTimes {
   int gr;
   TimeW w[4];  // substeps 1..gr
@@ -347,13 +350,6 @@ constexpr int kAllCornerGroups = DNS_ALL_CORNER_GROUPS;
 static_assert(kAllCornerGroups >= 1 && kAllCornerGroups <= 8, "field groups of b_icorner_all");
 __host__ __device__ constexpr int all_corner_field(int g) { return 23 * g / kAllCornerGroups; }
 constexpr int kCornerFieldsMax = (23 + kAllCornerGroups - 1) / kAllCornerGroups;
-// DNS_CORNER_PHASED 1: every field of the group in each barrier phase (three
-// phases per substep); 0: one field at a time (three phases per field and
-// substep).
-#ifndef DNS_CORNER_PHASED
-#define DNS_CORNER_PHASED 1
-#endif
-#if DNS_CORNER_PHASED
 // threads per block of b_icorner_all: the halo's population loads of one item
 // are spread over more threads, so that more of them are in flight at once
 #ifndef DNS_CORNER_THREADS
@@ -473,99 +469,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     __syncthreads();  // V and DY are rewritten for the next substep or item
   }
 }
-#else
-constexpr int kCNV = (kCQX * kCQY + kThreads - 1) / kThreads;
-struct CornerAllSmem {
-  IfCornerSmem S;
-  float N[kCornerFieldsMax][kCQX * kCQY];  // level n of the group's fields, tile and halo
-};
 
-template <int G>
-__device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &I, const Dyn &D, int tx, int ty,
-                                                  int w, const CornerTimes &ct) {
-  constexpr int F0 = all_corner_field(G), F1 = all_corner_field(G + 1);
-  static_assert(F1 - F0 <= kCornerFieldsMax, "group size");
-  const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
-  const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
-  const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
-  const int k = w == 0 ? 1 : I.nzc - 2;
-  const size_t pstride = (size_t)I.nzc * plane;
-  const float *fc = I.fc[D.cc ^ 1] + (size_t)k * plane;  // the coarse state just streamed
-  // ring after this step's rotation: level n in the old pp slot, p in old n, pp in old p
-  float *hn = I.hist + (size_t)D.hpp * hs + (size_t)w * 23 * plane;
-  const float *hp = I.hist + (size_t)D.hn * hs + (size_t)w * 23 * plane;
-  const float *hpp = I.hist + (size_t)D.hp * hs + (size_t)w * 23 * plane;
-  int off[kCNV];
-#pragma unroll
-  for (int s = 0; s < kCNV; s++) {
-    const int q = threadIdx.x + s * kThreads;
-    off[s] = -1;
-    if (q < kCQX * kCQY) off[s] = wrapf(j0 - 2 + q / kCQX, ny) * nx + wrapf(i0 - 2 + q % kCQX, nx);
-    if (off[s] < 0) continue;
-    float d[19];
-    load19f(fc, (size_t)off[s], pstride, d);
-    const Mac32 m = macro_f32(d);
-    const int qi = q % kCQX - 2, qj = q / kCQX - 2;
-    const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < CTY && i0 + qi < nx && j0 + qj < ny;
-#pragma unroll
-    for (int f = F0; f < F1; f++) {
-      const float v = f == 0 ? m.drho
-                      : f == 1 ? m.u0
-                      : f == 2 ? m.u1
-                      : f == 3 ? m.u2 : d[f - 4] - deq_f32(f - 4, m.drho, m.rho, m.u0, m.u1, m.u2, m.usq);
-      C.N[f - F0][q] = v;
-      if (own) hn[(size_t)f * plane + off[s]] = v;
-    }
-  }
-  __syncthreads();
-  float *V = &C.S.V[0][0];
-  for (int f = F0; f < F1; f++) {
-    float vp[kCNV], vpp[kCNV];
-#pragma unroll
-    for (int s = 0; s < kCNV; s++)
-      if (off[s] >= 0) {
-        vp[s] = __ldg(hp + (size_t)f * plane + off[s]);
-        vpp[s] = __ldg(hpp + (size_t)f * plane + off[s]);
-      }
-    for (int t = 0; t < ct.gr; t++) {
-      const TimeW tw = ct.w[t];
-#pragma unroll
-      for (int s = 0; s < kCNV; s++) {
-        const int q = threadIdx.x + s * kThreads;
-        if (off[s] >= 0) V[q] = tw.an * C.N[f - F0][q] + tw.ap * vp[s] + tw.app * vpp[s];
-      }
-      __syncthreads();
-#pragma unroll
-      for (int s = 0; s < (kCQX * CTY + kThreads - 1) / kThreads; s++) {
-        const int q = threadIdx.x + s * kThreads;
-        if (q < kCQX * CTY) {
-          const int pi = q % kCQX, r = q / kCQX;
-          C.S.DY[r][pi] = c2o3 * (C.S.V[r + 3][pi] - C.S.V[r + 1][pi]) - c1o12 * (C.S.V[r + 4][pi] - C.S.V[r][pi]);
-        }
-      }
-      __syncthreads();
-      float4 *out = I.corner + (size_t)t * 2 * 23 * plane + ((size_t)w * 23 + f) * plane;
-#pragma unroll
-      for (int s = 0; s < CTX * CTY / kThreads; s++) {
-        const int q = threadIdx.x + s * kThreads;
-        const int c = q % CTX, r = q / CTX;
-        if (i0 + c < nx && j0 + r < ny) {
-          const float dx = c2o3 * (C.S.V[r + 2][c + 3] - C.S.V[r + 2][c + 1]) -
-                           c1o12 * (C.S.V[r + 2][c + 4] - C.S.V[r + 2][c]);
-          const float dxy =
-              c2o3 * (C.S.DY[r][c + 3] - C.S.DY[r][c + 1]) - c1o12 * (C.S.DY[r][c + 4] - C.S.DY[r][c]);
-          out[(size_t)(j0 + r) * nx + i0 + c] = make_float4(C.S.V[r + 2][c + 2], dx, C.S.DY[r][c + 2], dxy);
-        }
-      }
-      __syncthreads();  // V and DY are rewritten for the next substep or field
-    }
-  }
-}
-#endif
-
-#if !DNS_CORNER_PHASED
-constexpr int kCornerThreads = kThreads;
-#endif
 // resident blocks of b_icorner_all per SM: 4 caps it at 64 registers (no
 // spills), 592 blocks for c2's 768 items where 80 registers gave 444
 #ifndef DNS_CORNER_MINB

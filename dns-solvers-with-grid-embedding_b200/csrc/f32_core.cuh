@@ -610,9 +610,6 @@ __device__ __forceinline__ void if_column32(const float4 (&C)[IfTile<GR>::TY + 1
 // GR = 2, both fine columns of cell column cx (sub-positions 0 and 1) at
 // sub-row JJ of the NR cell rows cy0, cy0 + 2, ...: v[r][0] / v[r][1] (the
 // arithmetic of if_col2 for II = 0 and II = 1).
-#ifndef DNS_EVAL_PAIRS
-#define DNS_EVAL_PAIRS 1
-#endif
 template <int JJ, int NR, int CH, int CW>
 __device__ __forceinline__ void if_pair2(const float4 (&C)[CH][CW], int cx, int cy0, float (&v)[NR][2]) {
   auto xpass = [&](int r, float &p0, float &q0, float &p1, float &q1) {
@@ -730,7 +727,7 @@ __device__ __forceinline__ void iface_eval_tile32_gr2(IfEvalSmem<2> &S, const If
 template <int GR>
 __device__ __forceinline__ void iface_eval_tile32(IfEvalSmem<GR> &S, const IfParams32 &P, int tx, int ty, int w,
                                                   int a0, int a1) {
-  if constexpr (GR == 2 && DNS_EVAL_PAIRS) {
+  if constexpr (GR == 2) {
     iface_eval_tile32_gr2(S, P, tx, ty, w, a0, a1);
     return;
   }
