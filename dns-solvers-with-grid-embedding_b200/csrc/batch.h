@@ -86,7 +86,10 @@ struct TimeW {
 };
 
 // Interface corner tile (coarse nodes): CTX x CTY of f32_core.cuh.
-constexpr int kCornerTX = 32, kCornerTY = 8;
+#ifndef DNS_CORNER_TY
+#define DNS_CORNER_TY 8
+#endif
+constexpr int kCornerTX = 32, kCornerTY = DNS_CORNER_TY;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {

@@ -17,7 +17,7 @@ namespace {
 
 using namespace f32;
 
-static_assert(CTX == kCornerTX && CTY == kCornerTY, "host and device interface tiles");
+static_assert(CTX == kCornerTX, "host and device interface tiles");
 
 // advance s to the instance owning item w (items are walked in increasing order)
 __device__ __forceinline__ int owner(const int *__restrict__ st, int n, int w, int s) {
@@ -324,7 +324,7 @@ __device__ __forceinline__ void iface_params_of(IfParams32 &P, const Inst &I, co
 
 // Interface corner data of every substep of the step, with the extraction of
 // the new interface history level folded in.  One item: tile (tx, ty) of
-// CTX x CTY coarse interface nodes, wall w, field group G.  The level-n values
+// CTX x kCornerTY coarse interface nodes, wall w, field group G.  The level-n values
 // of the tile and its two-node halo are formed from the coarse state just
 // streamed (xcomputations.c:558-625: [drho, u, f - feq] at k = 1 / zdc - 2) and
 // the tile's own nodes are written to the history (the slot that becomes
@@ -340,7 +340,7 @@ struct CornerTimes {
   int gr;
   TimeW w[4];  // substeps 1..gr
 };
-constexpr int kCQX = CTX + 4, kCQY = CTY + 4;
+constexpr int kCQX = CTX + 4, kCQY = kCornerTY + 4;
 // work items per (tile, wall) of b_icorner_all: field groups (each also forms
 // the level-n moments of its tile and halo)
 #ifndef DNS_ALL_CORNER_GROUPS
@@ -361,7 +361,7 @@ static_assert(kCQX % 4 == 0 && CTX % 4 == 0, "four-wide shared-memory rows");
 struct __align__(16) CornerAllSmem {
   float N[kCornerFieldsMax][kCQY][kCQX];  // level n of the group's fields, tile and halo
   float V[kCornerFieldsMax][kCQY][kCQX];  // substep t's values
-  float DY[kCornerFieldsMax][CTY][kCQX];  // their y derivatives on the tile's rows
+  float DY[kCornerFieldsMax][kCornerTY][kCQX];  // their y derivatives on the tile's rows
 };
 
 __device__ __forceinline__ float4 ld4s(const float *p) { return *reinterpret_cast<const float4 *>(p); }
@@ -372,9 +372,9 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
   constexpr int F0 = all_corner_field(G), F1 = all_corner_field(G + 1), NF = F1 - F0;
   static_assert(NF <= kCornerFieldsMax, "group size");
   // four-wide groups: y derivatives over the halo's columns, x derivatives over the tile's
-  constexpr int kDY = NF * CTY * (kCQX / 4), kDX = NF * CTY * (CTX / 4);
+  constexpr int kDY = NF * kCornerTY * (kCQX / 4), kDX = NF * kCornerTY * (CTX / 4);
   const float c2o3 = 2.f / 3.f, c1o12 = 1.f / 12.f;
-  const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * CTY;
+  const int nx = I.nx, ny = I.ny, i0 = tx * CTX, j0 = ty * kCornerTY;
   const size_t plane = (size_t)ny * nx, hs = (size_t)2 * 23 * plane;
   const int k = w == 0 ? 1 : I.nzc - 2;
   const size_t pstride = (size_t)I.nzc * plane;
@@ -393,7 +393,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     load19f(fc, (size_t)off, pstride, d);
     const Mac32 m = macro_f32(d);
     const int qi = q % kCQX - 2, qj = q / kCQX - 2;
-    const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < CTY && i0 + qi < nx && j0 + qj < ny;
+    const bool own = qi >= 0 && qi < CTX && qj >= 0 && qj < kCornerTY && i0 + qi < nx && j0 + qj < ny;
 #pragma unroll
     for (int f = 0; f < NF; f++) {
       const int fg = F0 + f;
@@ -437,7 +437,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     for (int s = 0; s < (kDY + kCornerThreads - 1) / kCornerThreads; s++) {
       const int e = t0 + s * kCornerThreads;
       if (e < kDY) {
-        const int f = e / (CTY * (kCQX / 4)), r = (e / (kCQX / 4)) % CTY, c = 4 * (e % (kCQX / 4));
+        const int f = e / (kCornerTY * (kCQX / 4)), r = (e / (kCQX / 4)) % kCornerTY, c = 4 * (e % (kCQX / 4));
         const float4 v0 = ld4s(&C.V[f][r][c]), v1 = ld4s(&C.V[f][r + 1][c]), v3 = ld4s(&C.V[f][r + 3][c]),
                      v4 = ld4s(&C.V[f][r + 4][c]);
         *reinterpret_cast<float4 *>(&C.DY[f][r][c]) =
@@ -451,7 +451,7 @@ __device__ __forceinline__ void corner_all_tile32(CornerAllSmem &C, const Inst &
     for (int s = 0; s < (kDX + kCornerThreads - 1) / kCornerThreads; s++) {
       const int e = t0 + s * kCornerThreads;
       if (e < kDX) {
-        const int f = e / (CTY * (CTX / 4)), r = (e / (CTX / 4)) % CTY, c0 = 4 * (e % (CTX / 4));
+        const int f = e / (kCornerTY * (CTX / 4)), r = (e / (CTX / 4)) % kCornerTY, c0 = 4 * (e % (CTX / 4));
         const float4 xa = ld4s(&C.V[f][r + 2][c0]), xb = ld4s(&C.V[f][r + 2][c0 + 4]);
         const float4 ya = ld4s(&C.DY[f][r][c0]), yb = ld4s(&C.DY[f][r][c0 + 4]);
         const float x[8] = {xa.x, xa.y, xa.z, xa.w, xb.x, xb.y, xb.z, xb.w};
