@@ -2,10 +2,10 @@
 // persistent kernels over a per-instance block table (internal to
 // libdnsembed; the C ABI is dns_batch_* in include/dns_embed.h).
 //
-// Every phase of the coarse step (coarse collide-stream, interface history and
-// corner data, fine substeps, interface evaluation, injection, statistics
-// fold, finalize) is one persistent kernel: a grid sized to the machine walks
-// the phase's work items
+// Every phase of the coarse step (statistics, coarse collide-stream, interface
+// history and corner data, fine substeps, interface evaluation, injection,
+// finalize) is one
+// persistent kernel: a grid sized to the machine walks the phase's work items
 // of all resident instances.  Instance s owns items [start[ph][s],
 // start[ph][s+1]); an item is one tile of one instance, decoded against that
 // instance's own sizes and tile shape.  Everything a step needs that changes
@@ -29,7 +29,8 @@ constexpr int kLogRows = 64;    // per-instance log ring (>= steps per graph rep
 constexpr int kFinChunks = 32;  // blocks per instance in the finalize
 
 enum Phase {
-  PH_SFINAL = 0, // per-plane accumulation of the sampled state's sums (coarse 2..zdc-3, every fine plane)
+  PH_STATS = 0,  // plane statistics of the sampled state (coarse 2..zdc-3, every fine plane)
+  PH_SFINAL,     // per-plane accumulation of those sums
   PH_COARSE,     // every coarse plane
   PH_FINE,       // every fine plane of both blocks (wall-adjacent, interface-adjacent, then bulk)
   PH_ICORNER,    // interface history level n and every substep's corner data: tiles x walls x field groups
@@ -93,7 +94,7 @@ constexpr int kCornerTX = 32, kCornerTY = DNS_CORNER_TY;
 
 // Launch helpers (batch_f32.cu).  grid = persistent blocks of each kernel.
 struct Grids {
-  int sfinal, coarse, fine, icorner, ieval, inject, final_;
+  int stats, sfinal, coarse, fine, icorner, ieval, inject, final_;
 };
 int query_grids(int gr, Grids *g);
 // count: one zeroed counter per slot (the finalize resets it)

@@ -37,12 +37,60 @@ __device__ __forceinline__ bool sampling(const Inst &I, const Dyn &D) {
   return D.remaining > 0 && I.sample_every > 0 && D.step % I.sample_every == 0;
 }
 
+__device__ __forceinline__ void stat_acc(const float (&f)[19], PlaneStat &sacc) {
+  const Mac32 m = macro_f32(f);
+  sacc.add(m.u0, m.u1, m.u2, 1.0 + (double)m.drho);
+}
 
 // ------------------------------------------------------------------ statistics
-// The sampled state's plane sums are formed where the state is read anyway:
-// the coarse kernel (planes 2..zdc-3) and the first fine substep (every fine
-// plane) add each node's pre-collision moments when the instance samples this
-// step, into per-block partials that b_sfinal folds into the running rows.
+// Sums of the state at the start of the step (the state the single-channel
+// form samples inside its coarse kernel and first fine substep), four nodes
+// per thread on the tiles of the stream-collide kernels.
+__global__ void __launch_bounds__(kThreads) b_stats(const Mix *__restrict__ M, const Dyn *__restrict__ dyn) {
+  const int n = M->n;
+  const int *st = M->start[PH_STATS];
+  const int total = st[n];
+  int s = 0;
+  for (int w = blockIdx.x; w < total; w += gridDim.x) {
+    s = owner(st, n, w, s);
+    const Inst &I = M->inst[s];
+    const Dyn D = dyn[I.slot];
+    if (!sampling(I, D)) {
+      w = past(w, st[s + 1], gridDim.x);
+      continue;
+    }
+    int local = w - st[s];
+    const int ncs = (I.nzc - 4) * I.cgy * I.cgx;
+    const bool coarse = local < ncs;
+    if (!coarse) local -= ncs;
+    const int W = coarse ? I.cw : I.fw, jb = coarse ? I.cjb : I.fjb;
+    const int gx = coarse ? I.cgx : I.fgx, gy = coarse ? I.cgy : I.fgy;
+    const int nx = coarse ? I.nx : I.nxf, ny = coarse ? I.ny : I.nyf;
+    const int z = local / (gx * gy), rem = local - z * gx * gy, by = rem / gx, bx = rem - by * gx;
+    const int p = coarse ? z + 2 : z;  // coarse plane k, or fine device plane
+    const int lw = log2i(W), tx = threadIdx.x & (W - 1), ty = threadIdx.x >> lw, R = kThreads >> lw;
+    const float *src = coarse ? I.fc[D.cc] : I.ff[D.cf];
+    const size_t pstride = coarse ? (size_t)I.nzc * I.ny * I.nx : (size_t)2 * I.zds * I.nyf * I.nxf;
+    PlaneStat sacc;
+    sacc.init();
+    for (int r = 0; r < jb; r++) {
+      const int j = (by * jb + r) * R + ty;
+      const QuadPos P = quad_pos(tx, W, bx * 4 * W, nx, j < ny);
+      if (!P.ok) continue;  // no shuffles below
+      float q[19][4];
+      quad_load(src, ((size_t)p * ny + j) * nx + P.x0, pstride, true, q);
+#pragma unroll
+      for (int c = 0; c < 4; c++) {
+        float f[19];
+#pragma unroll
+        for (int a = 0; a < 19; a++) f[a] = q[a][c];
+        stat_acc(f, sacc);
+      }
+    }
+    const size_t blk = ((size_t)p * gy + by) * gx + bx;
+    block_reduce_stat(sacc, I.part + (coarse ? I.psc : I.psf) + blk * kStatPart);
+  }
+}
 
 // per composite-profile plane: sum the plane's block partials (fixed order) and
 // add the sample into the instance's running-statistics row (kernels.h layout,
@@ -88,7 +136,6 @@ __global__ void __launch_bounds__(kThreads) b_sfinal(const Mix *__restrict__ M, 
 #ifndef DNS_F32_QUAD_MINB
 #define DNS_F32_QUAD_MINB 4
 #endif
-template <bool STATS>
 __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     b_coarse(const Mix *__restrict__ M, const Dyn *__restrict__ dyn, const DevState *__restrict__ state) {
   const int n = M->n;
@@ -115,9 +162,6 @@ __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     const float one[3] = {1.f, 1.f, 1.f};
     const int plane = ny * nx;
     double acc[2] = {0., 0.};
-    const bool smp = STATS && k >= 2 && k <= nzc - 3 && sampling(I, D);  // block-uniform
-    PlaneStat sacc;
-    if (STATS) sacc.init();
     for (int r = 0; r < I.cjb; r++) {
       const int jr = (by * I.cjb + r) * R + ty;
       const bool row_ok = jr < ny;
@@ -128,9 +172,6 @@ __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
       quad_load(src, (size_t)(rowoff + P.x0), pstride, P.ok, q);
       Mac32 m[4];
       quad_collide(q, om, G, m);
-      if (STATS && smp && P.ok)
-#pragma unroll
-        for (int c = 0; c < 4; c++) sacc.add(m[c].u0, m[c].u1, m[c].u2, 1.0 + (double)m[c].drho);
       const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
       if (k >= 2 && k <= nzc - 3) {
         if (P.ok)
@@ -152,7 +193,6 @@ __global__ void __launch_bounds__(kThreads, DNS_F32_QUAD_MINB)
     }
     const size_t blk = ((size_t)k * I.cgy + by) * I.cgx + bx;
     block_reduce32<2>(acc, I.part + I.pc + blk * 2);
-    if (STATS && smp) block_reduce_stat(sacc, I.part + I.psc + blk * kStatPart);
   }
 }
 
@@ -214,9 +254,6 @@ __device__ __forceinline__ void fine_item(const Inst &I, const Dyn &D, int local
     const bool wuni = wz[0] == wz[1] && wz[1] == wz[2];
     const int plane = ny * nx;
     double acc[2] = {0., 0.}, wacc[2] = {0., 0.};
-    const bool smp = (MODE & 4) && sampling(I, D);  // block-uniform
-    PlaneStat sacc;
-    if (MODE & 4) sacc.init();
     for (int r = 0; r < I.fjb; r++) {
       const int jr = (by * I.fjb + r) * R + ty;
       const bool row_ok = jr < ny;
@@ -232,7 +269,6 @@ __device__ __forceinline__ void fine_item(const Inst &I, const Dyn &D, int local
         for (int c = 0; c < 4; c++) {
           if ((MODE & 2) && wall_sum_plane) wacc[0] += (double)m[c].u0;
           if ((MODE & 2) && wall_rho_plane) wacc[1] += 1.0 + (double)m[c].drho;
-          if ((MODE & 4) && smp) sacc.add(m[c].u0, m[c].u1, m[c].u2, 1.0 + (double)m[c].drho);
         }
       }
       const int dym = j == 0 ? (ny - 1) * nx : -nx, dyp = j == ny - 1 ? -(ny - 1) * nx : nx;
@@ -278,7 +314,6 @@ __device__ __forceinline__ void fine_item(const Inst &I, const Dyn &D, int local
     const size_t blk = ((size_t)p * I.fgy + by) * I.fgx + bx;
     if (MODE & 1) block_reduce32<2>(acc, I.part + I.pf + blk * 2);
     if ((MODE & 2) && wall_sum_plane) block_reduce32<2>(wacc, I.part + I.pw + blk * 2);
-    if ((MODE & 4) && smp) block_reduce_stat(sacc, I.part + I.psf + blk * kStatPart);
   }
 }
 
@@ -760,6 +795,7 @@ int occupancy_grid(K kernel, int *grid, int threads = kThreads) {
 
 void tile_counts(const Inst &I, int c[PH_NPHASE]) {
   const int cb = I.cgx * I.cgy, fb = I.fgx * I.fgy;
+  c[PH_STATS] = (I.nzc - 4) * cb + 2 * I.zds * fb;
   c[PH_SFINAL] = I.nzp;
   c[PH_COARSE] = I.nzc * cb;
   c[PH_FINE] = 2 * I.zds * fb;
@@ -773,9 +809,10 @@ void tile_counts(const Inst &I, int c[PH_NPHASE]) {
 
 int query_grids(int gr, Grids *g) {
   int rc = 0;
+  rc |= occupancy_grid(b_stats, &g->stats);
   rc |= occupancy_grid(b_sfinal, &g->sfinal);
-  rc |= occupancy_grid(b_coarse<true>, &g->coarse);
-  rc |= occupancy_grid(b_fine<7>, &g->fine);
+  rc |= occupancy_grid(b_coarse, &g->coarse);
+  rc |= occupancy_grid(b_fine<3>, &g->fine);
   rc |= occupancy_grid(b_icorner_all, &g->icorner, kCornerThreads);
   if (gr == 2) rc |= occupancy_grid(b_ieval<2>, &g->ieval);
   else if (gr == 3) rc |= occupancy_grid(b_ieval<3>, &g->ieval);
@@ -796,8 +833,6 @@ static void launch_fine(const Mix *m, Dyn *dyn, DevState *state, int mode, int s
     DNS_BFINE(1)
     DNS_BFINE(2)
     DNS_BFINE(3)
-    DNS_BFINE(6)
-    DNS_BFINE(7)
   }
 #undef DNS_BFINE
 }
@@ -817,26 +852,26 @@ static void launch_eval(const Mix *m, Dyn *dyn, int gr, int sub, const Grids &g,
 
 // One coarse step of every resident instance on two streams, with the
 // dependency structure of the single-channel schedule:
-//   s:   coarse, corners (every substep, with the extraction),
-//        eval(1), [fine(1)] eval(2) ..., [inject] sfinal, final
+//   s:   stats, sfinal, coarse, corners (every substep, with the extraction),
+//        eval(1), [fine(1)] eval(2) ..., [inject] final
 //   aux: [start] fine(1), [eval(1)] fine(2) ..., inject
-// The sampled statistics are summed by the coarse kernel and the first fine
-// substep as they read the state.  ev: [0] start, [1..4] fine(sub), [5..8]
-// eval(sub), [9] inject.
+// The statistics read the state fine(2) and eval(2) overwrite; both follow
+// eval(1) on s.  ev: [0] start, [1..4] fine(sub), [5..8] eval(sub), [9] inject.
 void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned int *count, int gr, const Grids &g,
                  cudaStream_t s, cudaStream_t aux, cudaEvent_t *ev, bool stats) {
   cudaEventRecord(ev[0], s);
   cudaStreamWaitEvent(aux, ev[0], 0);
-  if (stats)
-    b_coarse<true><<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
-  else
-    b_coarse<false><<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
+  if (stats) {
+    b_stats<<<g.stats, kThreads, 0, s>>>(m, dyn);
+    b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
+  }
+  b_coarse<<<g.coarse, kThreads, 0, s>>>(m, dyn, state);
   CornerTimes ct{};
   ct.gr = gr;
   for (int t = 0; t < gr && t < 4; t++) ct.w[t] = time_weights(t + 1, gr);
   b_icorner_all<<<g.icorner, kCornerThreads, 0, s>>>(m, dyn, ct);
   for (int sub = 1; sub <= gr; sub++) {
-    const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0) | (stats && sub == 1 ? 4 : 0);
+    const int mode = (sub == gr ? 1 : 0) | (sub == 1 ? 2 : 0);
     if (sub > 1) cudaStreamWaitEvent(aux, ev[5 + sub - 2], 0);
     launch_fine(m, dyn, state, mode, sub, g, aux);
     cudaEventRecord(ev[1 + sub - 1], aux);
@@ -847,9 +882,6 @@ void launch_step(const Mix *m, Dyn *dyn, DevState *state, DevLog *log, unsigned 
   b_inject<<<g.inject, kThreads, 0, aux>>>(m, dyn);
   cudaEventRecord(ev[9], aux);
   cudaStreamWaitEvent(s, ev[9], 0);
-  // the sampled planes' partials are complete (coarse kernel, first fine
-  // substep); folded before the finalize advances the step count they test
-  if (stats) b_sfinal<<<g.sfinal, kThreads, 0, s>>>(m, dyn);
   b_final<<<g.final_, kThreads, 0, s>>>(m, dyn, state, log, count);
 }
 
