@@ -36,6 +36,7 @@ int fail(int code, const std::string &msg) {
   } while (0)
 
 constexpr int kLogCap = 1024;
+constexpr int kXferChunks = 8;  // x runs per level transfer (state import / export)
 constexpr int kProfSteps = 256;  // steps per chunk while profiling (bounds the event pool)
 
 // CUDA-event timing of every launch (dns_set_profiling)
@@ -77,6 +78,8 @@ struct dns_handle {
   unsigned int *fin_counter = nullptr; // finalize's block counter
   cudaStream_t aux = nullptr;          // fine substeps and injection (lowest priority)
   cudaEvent_t ev_start = nullptr, ev_inj = nullptr, ev_fine[4] = {}, ev_if[4] = {};
+  cudaEvent_t ev_xfer[kXferChunks] = {};  // one per x run of a level transfer
+  bool xfer_ok = false;                // the runs overlap on the two streams
   int cur_c = 0, cur_f = 0;
   long ss = 0;                         // coarse steps since load / seed
   int tm = 0;                          // time origin of the log stamps (TSTR or restart counter)
@@ -323,6 +326,8 @@ extern "C" void dns_destroy(dns_handle *h) {
                         &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
   for (cudaEvent_t *e : evs)
     if (*e) cudaEventDestroy(*e);
+  for (cudaEvent_t e : h->ev_xfer)
+    if (e) cudaEventDestroy(e);
   delete h;
 }
 
@@ -391,6 +396,9 @@ extern "C" int dns_create(const dns_params *p, dns_handle **out) {
   cudaEvent_t *evs[] = {&h->ev_start, &h->ev_inj, &h->ev_fine[0], &h->ev_fine[1], &h->ev_fine[2],
                         &h->ev_fine[3], &h->ev_if[0], &h->ev_if[1], &h->ev_if[2], &h->ev_if[3]};
   for (cudaEvent_t *e : evs) ev_ok = ev_ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+  h->xfer_ok = ev_ok;
+  for (cudaEvent_t &e : h->ev_xfer)
+    h->xfer_ok = h->xfer_ok && cudaEventCreateWithFlags(&e, cudaEventDisableTiming) == cudaSuccess;
   if (!ev_ok) {
     dns_destroy(h);
     return fail(DNS_ECUDA, "stream / event creation failed");
@@ -473,47 +481,90 @@ static int staging(dns_handle *h, int level, double **out) {
 // <-> reference AoS doubles on the host, through the device staging buffer:
 // the transpose and the wall plane (from / into wall_dev) are device kernels,
 // the host sees one copy of the whole level and one synchronisation.
-static int export_level(dns_handle *h, int level, double *out) {
+// A level moves in kXferChunks runs of x indices (contiguous on the AoS side):
+// the transpose of one run overlaps the host copy of another, the copies on
+// the second stream back to back.
+static void transpose_level(dns_handle *h, int level, double *stage, bool to_aos, int i0, int i1, cudaStream_t st) {
   const dns_geometry &g = h->g;
   const int zds = h->p.zds;
+  const bool f32 = is_f32(h);
+  if (level == 0) {
+    if (to_aos) {
+      if (f32) launch_dev_to_aos_f32(F(h->fc[h->cur_c]), stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, st, i0, i1);
+      else launch_soa_to_aos(h->fc[h->cur_c], stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, st, i0, i1);
+    } else {
+      if (f32) launch_aos_to_dev_f32(stage, F(h->fc[h->cur_c]), g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, st, i0, i1);
+      else launch_aos_to_soa(stage, h->fc[h->cur_c], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, st, i0, i1);
+    }
+    return;
+  }
+  // lower block: device planes 0..zds-1 are k = 1..zdf-1; upper: zds.. are k = 0..zdf-2
+  const int p0 = level == 1 ? 0 : zds, k0 = level == 1 ? 1 : 0;
+  if (to_aos) {
+    if (f32) launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, st, i0, i1);
+    else launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, st, i0, i1);
+  } else {
+    if (f32) launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, st, i0, i1);
+    else launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, st, i0, i1);
+  }
+}
+
+static int export_level(dns_handle *h, int level, double *out) {
+  const dns_geometry &g = h->g;
   double *stage = nullptr;
   int rc = staging(h, level, &stage);
   if (rc) return rc;
-  const bool f32 = is_f32(h);
-  if (level == 0) {
-    if (f32) launch_dev_to_aos_f32(F(h->fc[h->cur_c]), stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-    else launch_soa_to_aos(h->fc[h->cur_c], stage, g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-  } else {
-    // lower block: device planes 0..zds-1 are k = 1..zdf-1; upper: zds.. are k = 0..zdf-2
-    const int p0 = level == 1 ? 0 : zds, k0 = level == 1 ? 1 : 0, kw = level == 1 ? 0 : g.zdf - 1;
-    if (f32) launch_dev_to_aos_f32(F(h->ff[h->cur_f]), stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
-    else launch_soa_to_aos(h->ff[h->cur_f], stage, g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+  const int nxl = level == 0 ? g.nx : g.nxf;
+  const size_t col = level_doubles(g, level) / (size_t)nxl;  // AoS doubles per x index
+  if (level > 0)
     launch_wall_plane(stage, h->wall_dev + (size_t)(level - 1) * g.nxf * g.nyf * 19, (long long)g.nxf * g.nyf,
-                      g.zdf, kw, true, h->stream);
+                      g.zdf, level == 1 ? 0 : g.zdf - 1, true, h->stream);
+  const int C = h->xfer_ok ? kXferChunks : 1;
+  cudaStream_t cs = C > 1 ? h->aux : h->stream;
+  for (int c = 0; c < C; c++) {
+    const int i0 = (int)((long long)nxl * c / C), i1 = (int)((long long)nxl * (c + 1) / C);
+    if (i1 <= i0) continue;
+    transpose_level(h, level, stage, true, i0, i1, h->stream);
+    if (C > 1) {
+      CUDA_TRY(cudaEventRecord(h->ev_xfer[c], h->stream));
+      CUDA_TRY(cudaStreamWaitEvent(cs, h->ev_xfer[c], 0));
+    }
+    CUDA_TRY(cudaMemcpyAsync(out + (size_t)i0 * col, stage + (size_t)i0 * col, (size_t)(i1 - i0) * col * 8,
+                             cudaMemcpyDeviceToHost, cs));
   }
   CUDA_TRY(cudaGetLastError());
-  CUDA_TRY(cudaMemcpyAsync(out, stage, level_doubles(g, level) * 8, cudaMemcpyDeviceToHost, h->stream));
+  CUDA_TRY(cudaStreamSynchronize(cs));
   CUDA_TRY(cudaStreamSynchronize(h->stream));
   return DNS_OK;
 }
 
 static int import_level(dns_handle *h, int level, const double *in) {
   const dns_geometry &g = h->g;
-  const int zds = h->p.zds;
   double *stage = nullptr;
   int rc = staging(h, level, &stage);
   if (rc) return rc;
-  const bool f32 = is_f32(h);
-  CUDA_TRY(cudaMemcpyAsync(stage, in, level_doubles(g, level) * 8, cudaMemcpyHostToDevice, h->stream));
-  if (level == 0) {
-    if (f32) launch_aos_to_dev_f32(stage, F(h->fc[h->cur_c]), g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-    else launch_aos_to_soa(stage, h->fc[h->cur_c], g.nx, g.ny, g.nzc, 0, g.nzc, g.nzc, 0, h->stream);
-  } else {
-    const int p0 = level == 1 ? 0 : zds, k0 = level == 1 ? 1 : 0, kw = level == 1 ? 0 : g.zdf - 1;
-    if (f32) launch_aos_to_dev_f32(stage, F(h->ff[h->cur_f]), g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
-    else launch_aos_to_soa(stage, h->ff[h->cur_f], g.nxf, g.nyf, 2 * zds, p0, zds, g.zdf, k0, h->stream);
+  const int nxl = level == 0 ? g.nx : g.nxf;
+  const size_t col = level_doubles(g, level) / (size_t)nxl;
+  const int C = h->xfer_ok ? kXferChunks : 1;
+  cudaStream_t cs = C > 1 ? h->aux : h->stream;
+  if (C > 1) {  // the copies follow whatever the handle's stream has queued
+    CUDA_TRY(cudaEventRecord(h->ev_start, h->stream));
+    CUDA_TRY(cudaStreamWaitEvent(cs, h->ev_start, 0));
+  }
+  for (int c = 0; c < C; c++) {
+    const int i0 = (int)((long long)nxl * c / C), i1 = (int)((long long)nxl * (c + 1) / C);
+    if (i1 <= i0) continue;
+    CUDA_TRY(cudaMemcpyAsync(stage + (size_t)i0 * col, in + (size_t)i0 * col, (size_t)(i1 - i0) * col * 8,
+                             cudaMemcpyHostToDevice, cs));
+    if (C > 1) {
+      CUDA_TRY(cudaEventRecord(h->ev_xfer[c], cs));
+      CUDA_TRY(cudaStreamWaitEvent(h->stream, h->ev_xfer[c], 0));
+    }
+    transpose_level(h, level, stage, false, i0, i1, h->stream);
+  }
+  if (level > 0) {
     launch_wall_plane(stage, h->wall_dev + (size_t)(level - 1) * g.nxf * g.nyf * 19, (long long)g.nxf * g.nyf,
-                      g.zdf, kw, false, h->stream);
+                      g.zdf, level == 1 ? 0 : g.zdf - 1, false, h->stream);
     h->wall_host_stale = true;
     h->wall_gen++;
   }

@@ -164,10 +164,12 @@ int tke_budget_planar(const dns_params &p, const dns_geometry &g, const double *
 // (to_aos) or from the compact wall array [nodes][19]
 void launch_wall_plane(double *aos, double *wall, long long nodes, int nz, int kw, bool to_aos, cudaStream_t stream);
 // layout transposes between the device SoA state and the reference AoS order
+// [i0, i1): the x indices to move (i1 < 0: all); the AoS side is i-major, so
+// an x range is one contiguous run of it
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
-                       int k0_aos, cudaStream_t stream);
+                       int k0_aos, cudaStream_t stream, int i0 = 0, int i1 = -1);
 void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, int p0, int np, int nz_aos,
-                       int k0_aos, cudaStream_t stream);
+                       int k0_aos, cudaStream_t stream, int i0 = 0, int i1 = -1);
 
 // --- FP32 deviation-storage kernels (kernels_f32.cu); same layouts in float ---
 void launch_coarse_f32(const float *src, float *dst, const Dims &d, const LaunchShape &s, double om,
@@ -189,8 +191,8 @@ void launch_seed_f32(float *fc, float *ff, float *hist3, const Dims &d, uint64_t
                      cudaStream_t stream);
 // device float deviations <-> reference AoS doubles (f = w + d)
 void launch_dev_to_aos_f32(const float *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos,
-                           int k0_aos, cudaStream_t stream);
+                           int k0_aos, cudaStream_t stream, int i0 = 0, int i1 = -1);
 void launch_aos_to_dev_f32(const double *aos, float *soa, int nx, int ny, int P, int p0, int np, int nz_aos,
-                           int k0_aos, cudaStream_t stream);
+                           int k0_aos, cudaStream_t stream, int i0 = 0, int i1 = -1);
 
 }  // namespace dns

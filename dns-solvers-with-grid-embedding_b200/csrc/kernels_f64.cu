@@ -916,9 +916,9 @@ __global__ void __launch_bounds__(kMaxThreads) seed_kernel(double *fc, double *f
 
 // ------------------------------------------------------------------ transposes
 __global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__restrict__ aos, int nx, int ny, int P,
-                                  int p0, int nz_aos, int k0_aos) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
-  if (i >= nx) return;
+                                  int p0, int nz_aos, int k0_aos, int i0, int i1) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= i1) return;
   const size_t stride = (size_t)P * ny * nx;
   const size_t s = ((size_t)(p0 + q) * ny + j) * nx + i;
   double *o = aos + (((size_t)i * ny + j) * nz_aos + k0_aos + q) * 19;
@@ -926,9 +926,9 @@ __global__ void soa_to_aos_kernel(const double *__restrict__ soa, double *__rest
 }
 
 __global__ void aos_to_soa_kernel(const double *__restrict__ aos, double *__restrict__ soa, int nx, int ny, int P,
-                                  int p0, int nz_aos, int k0_aos) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
-  if (i >= nx) return;
+                                  int p0, int nz_aos, int k0_aos, int i0, int i1) {
+  const int i = i0 + blockIdx.x * blockDim.x + threadIdx.x, j = blockIdx.y, q = blockIdx.z;
+  if (i >= i1) return;
   const size_t stride = (size_t)P * ny * nx;
   const size_t s = ((size_t)(p0 + q) * ny + j) * nx + i;
   const double *o = aos + (((size_t)i * ny + j) * nz_aos + k0_aos + q) * 19;
@@ -1202,15 +1202,19 @@ void launch_seed_f64(double *fc, double *ff, double *hist3, const Dims &d, uint6
 }
 
 void launch_soa_to_aos(const double *soa, double *aos, int nx, int ny, int P, int p0, int np, int nz_aos, int k0_aos,
-                       cudaStream_t stream) {
-  dim3 grid((nx + 127) / 128, ny, np), block(128);
-  soa_to_aos_kernel<<<grid, block, 0, stream>>>(soa, aos, nx, ny, P, p0, nz_aos, k0_aos);
+                       cudaStream_t stream, int i0, int i1) {
+  if (i1 < 0) i1 = nx;
+  if (i1 <= i0) return;
+  dim3 grid((i1 - i0 + 127) / 128, ny, np), block(128);
+  soa_to_aos_kernel<<<grid, block, 0, stream>>>(soa, aos, nx, ny, P, p0, nz_aos, k0_aos, i0, i1);
 }
 
 void launch_aos_to_soa(const double *aos, double *soa, int nx, int ny, int P, int p0, int np, int nz_aos, int k0_aos,
-                       cudaStream_t stream) {
-  dim3 grid((nx + 127) / 128, ny, np), block(128);
-  aos_to_soa_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos);
+                       cudaStream_t stream, int i0, int i1) {
+  if (i1 < 0) i1 = nx;
+  if (i1 <= i0) return;
+  dim3 grid((i1 - i0 + 127) / 128, ny, np), block(128);
+  aos_to_soa_kernel<<<grid, block, 0, stream>>>(aos, soa, nx, ny, P, p0, nz_aos, k0_aos, i0, i1);
 }
 
 void launch_wall_plane(double *aos, double *wall, long long nodes, int nz, int kw, bool to_aos, cudaStream_t stream) {
