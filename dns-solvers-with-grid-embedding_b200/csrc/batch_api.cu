@@ -180,9 +180,7 @@ struct dns_batch {
   unsigned int *dcount = nullptr;         // finalize counters, one per slot
   Dyn *hdyn[2] = {nullptr, nullptr};      // pinned snapshots
   DevLog *hlog[2] = {nullptr, nullptr};
-  Grids occ{};    // persistent grids: the blocks the machine holds at once
-  Grids grids{};  // the grids the captured graphs launch (see sized_grids)
-  long long cap_items[PH_NPHASE] = {};  // work items of the mix the graphs were captured for
+  Grids grids{};
   // [with statistics phases][kGroup steps, 1 step]; the statistics launches
   // are left out while no resident instance samples
   cudaGraphExec_t gexec[2][2] = {{nullptr, nullptr}, {nullptr, nullptr}};
@@ -338,8 +336,7 @@ extern "C" int dns_batch_add(dns_batch *b, const dns_params *p, const dns_tile *
   if (!tile_ok(t)) return fail_with(DNS_EINVAL, "bad tile shape");
   BTRY(cudaSetDevice(b->device));
   if (b->gr == 0) {
-    if (query_grids(g.gr, &b->occ)) return fail_with(DNS_ECUDA, "occupancy query failed");
-    b->grids = b->occ;
+    if (query_grids(g.gr, &b->grids)) return fail_with(DNS_ECUDA, "occupancy query failed");
     b->gr = g.gr;
   }
   Record r;
@@ -464,35 +461,6 @@ static int upload_mix(dns_batch *b) {
   return DNS_OK;
 }
 
-// Grids of the stream-collide and interface phases: one block per work item
-// of the current mix (at least the persistent grid), so that blocks retire
-// during a launch and the next launch's blocks fill the machine as they do,
-// as ordinary grids do; the kernels loop over items either way, so a grid
-// captured for one mix stays correct for any other.  The graphs are
-// re-captured when the mix's item counts move by more than a quarter.
-#ifndef DNS_ITEM_GRIDS
-#define DNS_ITEM_GRIDS 1
-#endif
-static bool sized_grids(dns_batch *b) {
-  if (!DNS_ITEM_GRIDS) return false;
-  const Mix &M = *b->hmix;
-  const int ph[4] = {PH_COARSE, PH_FINE, PH_ICORNER, PH_IEVAL};
-  bool moved = false;
-  for (int q : ph) {
-    const long long now = M.start[q][M.n], was = b->cap_items[q];
-    if (4 * now > 5 * was || 4 * now < 3 * was || was == 0) moved = true;
-  }
-  if (!moved) return false;
-  for (int q : ph) b->cap_items[q] = M.start[q][M.n];
-  auto at_least = [](int occ, long long items) { return (int)std::max<long long>(occ, std::min<long long>(items, 1 << 30)); };
-  b->grids = b->occ;
-  b->grids.coarse = at_least(b->occ.coarse, M.start[PH_COARSE][M.n]);
-  b->grids.fine = at_least(b->occ.fine, M.start[PH_FINE][M.n]);
-  b->grids.icorner = at_least(b->occ.icorner, M.start[PH_ICORNER][M.n]);
-  b->grids.ieval = at_least(b->occ.ieval, M.start[PH_IEVAL][M.n]);
-  return true;
-}
-
 static int capture(dns_batch *b, int steps, bool stats, cudaGraphExec_t *out) {
   cudaGraph_t graph = nullptr;
   BTRY(cudaStreamBeginCapture(b->s, cudaStreamCaptureModeThreadLocal));
@@ -547,13 +515,6 @@ extern "C" int dns_batch_run(dns_batch *b, long long nsteps, int *active) {
     }
   if (live > 0 && nsteps > 0) {
     if (b->dirty && (rc = upload_mix(b))) return rc;
-    if (sized_grids(b))  // new grids: every captured graph is stale
-      for (auto &row : b->gexec)
-        for (cudaGraphExec_t &g : row)
-          if (g) {
-            BTRY(cudaGraphExecDestroy(g));
-            g = nullptr;
-          }
     cudaGraphExec_t *gx = b->gexec[sampling ? 1 : 0];
     if (!gx[0] && (rc = capture(b, kGroup, sampling, &gx[0]))) return rc;
     if (!gx[1] && (rc = capture(b, 1, sampling, &gx[1]))) return rc;
