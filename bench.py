@@ -811,12 +811,15 @@ def main():
     ap.add_argument("--c4-steps", type=int, default=2000)
     ap.add_argument("--no-c4-reference", action="store_true",
                     help="skip the batched channels' FP64 runs (throughput only)")
-    ap.add_argument("--c5-requests", type=int, default=200)
+    ap.add_argument("--c5-requests", type=int, default=100)
     ap.add_argument("--c5-fp64-requests", type=int, default=24,
                     help="first requests of each stream served alone by the FP32 loop and one at a time in FP64")
     ap.add_argument("--c5-rates", type=float, nargs="+", default=[10.0])
-    ap.add_argument("--longrun-cases", nargs="*", default=["c2", "c3n", "c3r", "c3p"],
-                    help="channels run long for the FP32-vs-FP64 statistics (none: skip)")
+    # the default run keeps to a few minutes: config 2's long run (about 40 s);
+    # config 3's three cases (about 75 s each) with --longrun-cases c2 c3n c3r c3p
+    ap.add_argument("--longrun-cases", nargs="*", default=["c2"],
+                    help="channels run long for the FP32-vs-FP64 statistics (none: skip; config 3: c3n c3r c3p, "
+                         "c3n being the no-slip companion of the drag reduction)")
     ap.add_argument("--longrun-warmup", type=int, default=10000)
     ap.add_argument("--longrun-steps", type=int, default=20000, help="sampled steps after the warm-up")
     ap.add_argument("--longrun-c3-steps", type=int, default=15000,
